@@ -1,0 +1,539 @@
+// C++ host runtime of the B200 solvers behind the C ABI of include/gpgmp_c.h.
+//
+// gpgmp_solver mirrors gpgmp::Solver and its two subclasses
+// (exec/src/gpgmp/src/Solver.h:15-239, HomogeneousSolver.cpp:79-235,
+// InhomogeneousSolver.cpp:7-503): the host keeps the per-species diffusion
+// clocks exactly as the reference does, in float, and launches one kernel per
+// reaction window / diffusion sweep covering every realisation.  Nothing waits
+// for the device unless the caller asks for results (or for the reference's
+// finish-after-every-launch behaviour, GPGMP_CREATE_SYNC_EACH_LAUNCH).
+#include <cstring>
+#include <cstdio>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <cuda_runtime.h>
+#include "kernels.h"
+#include "host_common.h"
+
+using namespace gpgmp;
+
+struct gpgmp_solver {
+    gpgmp_model_desc m{};
+    std::vector<float> diffusion;
+    std::vector<gpgmp_reaction> reactions;
+    int R = 1;
+    uint32_t seed = 0;
+    int create_flags = 0;
+    cudaStream_t stream = nullptr;
+    GridDesc g{};
+    size_t area = 0;
+    bool deterministic = false, inhom = false;
+    // stochastic state: two buffers, per-species current index
+    int32_t* d_buf[2] = {nullptr, nullptr};
+    std::vector<int> cur;
+    // deterministic state: whole-state ping-pong
+    float* d_fbuf[2] = {nullptr, nullptr};
+    int fcur = 0;
+    gpgmp_reaction* d_reactions = nullptr;
+    int32_t* d_status = nullptr;
+    float* d_diff = nullptr;
+    float *d_Dx = nullptr, *d_Dy = nullptr, *d_rx = nullptr, *d_ry = nullptr;
+    uint32_t* d_minkey = nullptr;
+    float* d_lambda = nullptr;
+    void* d_stage = nullptr;          // gather buffer for snapshots / readback
+    // diffusion clocks (HomogeneousSolver.h m_dt / m_nextDiffusionTime,
+    // InhomogeneousSolver.h m_nextDiffusionTimeX/Y, m_smallestDtX/Y, m_diffusionDtX/Y)
+    std::vector<float> dt, next;
+    std::vector<float> nextX, nextY, smallX, smallY, ddX, ddY;
+    float pi = 0.f, pmove = 0.f, h = 1.f, det_dt = 0.f;
+};
+
+namespace {
+
+#define CK(expr)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+int after_launch(gpgmp_solver* h, cudaError_t e) {
+    if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    if (h->create_flags & GPGMP_CREATE_SYNC_EACH_LAUNCH) {
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "sync: %s", cudaGetErrorString(e));
+    }
+    return GPGMP_OK;
+}
+
+Planes planes_of(gpgmp_solver* h) {
+    Planes p{};
+    for (int s = 0; s < h->g.S; ++s) p.p[s] = h->d_buf[h->cur[s]];
+    return p;
+}
+
+// Gathers the per-species planes into one contiguous [R][S][area] device buffer.
+int gather_state(gpgmp_solver* h, void* dst) {
+    const size_t plane_bytes = h->area * sizeof(int32_t);
+    bool uniform = true;
+    for (int s = 0; s < h->g.S; ++s) uniform = uniform && h->cur[s] == h->cur[0];
+    if (uniform) {
+        CK(cudaMemcpyAsync(dst, h->d_buf[h->cur[0]], plane_bytes * h->g.S * h->R, cudaMemcpyDeviceToDevice, h->stream));
+        return GPGMP_OK;
+    }
+    CK(cudaMemcpy2DAsync(dst, plane_bytes, h->d_buf[0], plane_bytes, plane_bytes, (size_t)h->g.S * h->R,
+                         cudaMemcpyDeviceToDevice, h->stream));
+    for (int s = 0; s < h->g.S; ++s) {
+        if (h->cur[s] == 0) continue;
+        // species s of every realisation: R planes with a pitch of S planes
+        CK(cudaMemcpy2DAsync((char*)dst + s * plane_bytes, plane_bytes * h->g.S,
+                             (const char*)h->d_buf[1] + s * plane_bytes, plane_bytes * h->g.S, plane_bytes, h->R,
+                             cudaMemcpyDeviceToDevice, h->stream));
+    }
+    return GPGMP_OK;
+}
+
+// Makes buffer 0 hold every plane (so the state is one contiguous array).
+int normalize(gpgmp_solver* h) {
+    if (h->deterministic) {
+        if (h->fcur == 1) {
+            CK(cudaMemcpyAsync(h->d_fbuf[0], h->d_fbuf[1], h->area * h->g.S * h->R * sizeof(float),
+                               cudaMemcpyDeviceToDevice, h->stream));
+            h->fcur = 0;
+        }
+        return GPGMP_OK;
+    }
+    const size_t plane_bytes = h->area * sizeof(int32_t);
+    for (int s = 0; s < h->g.S; ++s) {
+        if (h->cur[s] == 0) continue;
+        CK(cudaMemcpy2DAsync((char*)h->d_buf[0] + s * plane_bytes, plane_bytes * h->g.S,
+                             (const char*)h->d_buf[1] + s * plane_bytes, plane_bytes * h->g.S, plane_bytes, h->R,
+                             cudaMemcpyDeviceToDevice, h->stream));
+        h->cur[s] = 0;
+    }
+    return GPGMP_OK;
+}
+
+void free_all(gpgmp_solver* h) {
+    void* ptrs[] = {h->d_buf[0], h->d_buf[1], h->d_fbuf[0], h->d_fbuf[1], h->d_reactions, h->d_status, h->d_diff,
+                    h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+int validate(const gpgmp_model_desc* m, int R) {
+    if (!m) return set_error(GPGMP_ERR_INVALID, "model is NULL");
+    if (m->width <= 0 || m->height <= 0) return set_error(GPGMP_ERR_INVALID, "grid %dx%d", m->width, m->height);
+    if (m->num_species <= 0 || m->num_species > kMaxSpecies)
+        return set_error(GPGMP_ERR_INVALID, "num_species %d outside 1..%d", m->num_species, kMaxSpecies);
+    if (m->num_reactions < 0 || m->num_reactions > 128)
+        return set_error(GPGMP_ERR_INVALID, "num_reactions %d outside 0..128", m->num_reactions);
+    if (m->num_reactions > 0 && !m->reactions) return set_error(GPGMP_ERR_INVALID, "reactions is NULL");
+    if (!m->diffusion) return set_error(GPGMP_ERR_INVALID, "diffusion is NULL");
+    if (R <= 0) return set_error(GPGMP_ERR_INVALID, "num_realisations %d", R);
+    if ((int64_t)m->width * m->height > (int64_t)1 << 30) return set_error(GPGMP_ERR_INVALID, "grid too large");
+    for (int i = 0; i < m->num_reactions; ++i) {
+        const gpgmp_reaction& r = m->reactions[i];
+        if (r.num_reactants < 0 || r.num_reactants > 3 || r.num_products < 0 || r.num_products > 4)
+            return set_error(GPGMP_ERR_INVALID, "reaction %d: bad reactant/product count", i);
+        for (int j = 0; j < r.num_reactants; ++j)
+            if (r.reactant_species[j] < 0 || r.reactant_species[j] >= m->num_species || r.reactant_stoich[j] < 0)
+                return set_error(GPGMP_ERR_INVALID, "reaction %d: bad reactant %d", i, j);
+        for (int j = 0; j < r.num_products; ++j)
+            if (r.product_species[j] < 0 || r.product_species[j] >= m->num_species || r.product_stoich[j] < 0)
+                return set_error(GPGMP_ERR_INVALID, "reaction %d: bad product %d", i, j);
+    }
+    if (m->solver_type < 0 || m->solver_type > 2) return set_error(GPGMP_ERR_UNSUPPORTED, "solver_type %d", m->solver_type);
+    if (m->solver_type == GPGMP_STOCHASTIC_INHOMOGENEOUS) {
+        if (m->drift_method == GPGMP_DRIFT_FIELD &&
+            (!m->field_dx || !m->field_dy || !m->field_rx || !m->field_ry))
+            return set_error(GPGMP_ERR_INVALID, "field drift method needs all four field arrays");
+        if (m->drift_method < GPGMP_DRIFT_FIELD || m->drift_method > GPGMP_DRIFT_ORNSTEIN_UHLENBECK)
+            return set_error(GPGMP_ERR_UNSUPPORTED, "drift_method %d", m->drift_method);
+        if (m->flags & 1) return set_error(GPGMP_ERR_UNSUPPORTED, "nonlinear diffusivity recompute");
+    }
+    return GPGMP_OK;
+}
+
+// InhomogeneousSolver.cpp:164-212: diffusivity/drift per species, then the first
+// time steps (computeTimestepX/Y read back one float each).
+int inhom_init(gpgmp_solver* h) {
+    const size_t n = h->area * h->g.S;
+    if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
+        CK(cudaMemcpyAsync(h->d_Dx, h->m.field_dx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_Dy, h->m.field_dy, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_rx, h->m.field_rx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_ry, h->m.field_ry, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    } else {
+        for (int s = 0; s < h->g.S; ++s)
+            CK(launch_diffusivity_drift(h->g, s, h->m.drift_method, h->m.drift_params, h->m.physical_length, h->d_Dx,
+                                        h->d_Dy, h->d_rx, h->d_ry, h->stream));
+    }
+    const float dx = h->m.physical_length / (float)h->m.width;
+    for (int s = 0; s < h->g.S; ++s) {
+        uint32_t key[2];
+        CK(launch_timestep((int)h->area, h->d_Dx + s * h->area, h->d_rx + s * h->area, dx, h->d_minkey, h->stream));
+        CK(cudaMemcpyAsync(&key[0], h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(launch_timestep((int)h->area, h->d_Dy + s * h->area, h->d_ry + s * h->area, dx, h->d_minkey, h->stream));
+        CK(cudaMemcpyAsync(&key[1], h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->smallX[s] = key_to_float(key[0]);
+        h->smallY[s] = key_to_float(key[1]);
+        h->ddX[s] = h->smallX[s];
+        h->ddY[s] = h->smallY[s];
+        h->nextX[s] = h->smallX[s];
+        h->nextY[s] = h->smallY[s];
+    }
+    return GPGMP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpgmp_version(void) { return 100; }
+
+int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations, uint32_t seed, int32_t create_flags,
+                        gpgmp_solver** out) {
+    if (!out) return set_error(GPGMP_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = validate(model, num_realisations);
+    if (rc) return rc;
+    auto* h = new gpgmp_solver();
+    h->m = *model;
+    h->R = num_realisations;
+    h->seed = seed;
+    h->create_flags = create_flags;
+    h->diffusion.assign(model->diffusion, model->diffusion + model->num_species);
+    if (model->num_reactions > 0) h->reactions.assign(model->reactions, model->reactions + model->num_reactions);
+    h->m.diffusion = h->diffusion.data();
+    h->m.reactions = h->reactions.empty() ? nullptr : h->reactions.data();
+    h->deterministic = model->solver_type == GPGMP_DETERMINISTIC_RK4;
+    h->inhom = model->solver_type == GPGMP_STOCHASTIC_INHOMOGENEOUS;
+    h->g.W = model->width;
+    h->g.H = model->height;
+    h->g.S = model->num_species;
+    h->g.R = num_realisations;
+    for (int i = 0; i < 4; ++i) h->g.bmask[i] = model->boundary_mask[i];
+    h->area = (size_t)model->width * model->height;
+    h->cur.assign(h->g.S, 0);
+    const int S = h->g.S;
+    const size_t n = h->area * S * (size_t)h->R;
+    h->h = model->physical_length / (float)model->width;
+    auto fail = [&](int code) {
+        free_all(h);
+        delete h;
+        return code;
+    };
+#define CKC(expr)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            int c_ = set_error(e_ == cudaErrorMemoryAllocation ? GPGMP_ERR_NOMEM : GPGMP_ERR_CUDA, "%s: %s", #expr, \
+                               cudaGetErrorString(e_));                                    \
+            return fail(c_);                                                               \
+        }                                                                                  \
+    } while (0)
+    if (h->deterministic) {
+        CKC(cudaMalloc(&h->d_fbuf[0], n * sizeof(float)));
+        CKC(cudaMalloc(&h->d_fbuf[1], n * sizeof(float)));
+        CKC(cudaMemset(h->d_fbuf[0], 0, n * sizeof(float)));
+        CKC(cudaMalloc(&h->d_stage, n * sizeof(float)));
+    } else {
+        CKC(cudaMalloc(&h->d_buf[0], n * sizeof(int32_t)));
+        CKC(cudaMalloc(&h->d_buf[1], n * sizeof(int32_t)));
+        CKC(cudaMemset(h->d_buf[0], 0, n * sizeof(int32_t)));
+        CKC(cudaMalloc(&h->d_stage, n * sizeof(int32_t)));
+    }
+    CKC(cudaMalloc(&h->d_status, sizeof(int32_t) * h->R));
+    CKC(cudaMemset(h->d_status, 0, sizeof(int32_t) * h->R));
+    CKC(cudaMalloc(&h->d_diff, sizeof(float) * S));
+    CKC(cudaMemcpy(h->d_diff, h->diffusion.data(), sizeof(float) * S, cudaMemcpyHostToDevice));
+    CKC(cudaMalloc(&h->d_lambda, sizeof(float) * S));
+    if (!h->reactions.empty()) {
+        CKC(cudaMalloc(&h->d_reactions, sizeof(gpgmp_reaction) * h->reactions.size()));
+        CKC(cudaMemcpy(h->d_reactions, h->reactions.data(), sizeof(gpgmp_reaction) * h->reactions.size(),
+                       cudaMemcpyHostToDevice));
+    }
+    // stay probability and jump probability as the reference's header computes them
+    const float stay = (float)(1.0 - (double)model->p0);
+    h->pi = (float)((1.0 - (double)stay) / 6.0);
+    h->pmove = h->pi * 4.0f;
+    h->dt.assign(S, 0.f);
+    h->next.assign(S, 0.f);
+    if (h->deterministic) {
+        // HomogeneousSolver.cpp:168-192: one common step, the smallest over species
+        float dtd = 0.f;
+        for (int i = 0; i < S; ++i) {
+            float d = h->diffusion[i] > 0 ? (float)1e-2f * h->h * h->h / (4.f * h->diffusion[i]) : model->max_time;
+            if (i == 0 || d < dtd) dtd = d;
+        }
+        h->det_dt = dtd;
+        for (int i = 0; i < S; ++i) { h->dt[i] = dtd; h->next[i] = dtd; }
+    } else if (!h->inhom) {
+        // HomogeneousSolver.cpp:154-166: dt_i = p0 / (2 * 3) * h^2 / D_i
+        for (int i = 0; i < S; ++i) {
+            h->dt[i] = h->diffusion[i] > 0 ? model->p0 / ((float)2. * 3) * h->h * h->h / h->diffusion[i]
+                                           : model->max_time;
+            h->next[i] = h->dt[i];
+        }
+    } else {
+        const size_t nf = h->area * S;
+        CKC(cudaMalloc(&h->d_Dx, nf * sizeof(float)));
+        CKC(cudaMalloc(&h->d_Dy, nf * sizeof(float)));
+        CKC(cudaMalloc(&h->d_rx, nf * sizeof(float)));
+        CKC(cudaMalloc(&h->d_ry, nf * sizeof(float)));
+        CKC(cudaMalloc(&h->d_minkey, sizeof(uint32_t)));
+        h->nextX.assign(S, 0.f); h->nextY.assign(S, 0.f);
+        h->smallX.assign(S, 0.f); h->smallY.assign(S, 0.f);
+        h->ddX.assign(S, 0.f); h->ddY.assign(S, 0.f);
+        int rc2 = inhom_init(h);
+        if (rc2) return fail(rc2);
+        for (int i = 0; i < S; ++i) h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
+    }
+    // the model's field arrays are the caller's; they were copied above if used
+    h->m.field_dx = h->m.field_dy = h->m.field_rx = h->m.field_ry = nullptr;
+#undef CKC
+    *out = h;
+    return GPGMP_OK;
+}
+
+int gpgmp_solver_destroy(gpgmp_solver* h) {
+    if (!h) return GPGMP_OK;
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return GPGMP_OK;
+}
+
+int gpgmp_solver_set_stream(gpgmp_solver* h, void* stream) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    h->stream = (cudaStream_t)stream;
+    return GPGMP_OK;
+}
+
+int gpgmp_set_state(gpgmp_solver* h, const void* host) {
+    if (!h || !host) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    const size_t n = h->area * h->g.S * (size_t)h->R;
+    if (h->deterministic) {
+        CK(cudaMemcpyAsync(h->d_fbuf[0], host, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        h->fcur = 0;
+    } else {
+        CK(cudaMemcpyAsync(h->d_buf[0], host, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        std::fill(h->cur.begin(), h->cur.end(), 0);
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+int gpgmp_get_state(gpgmp_solver* h, void* host) {
+    if (!h || !host) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    const size_t n = h->area * h->g.S * (size_t)h->R;
+    if (h->deterministic) {
+        CK(cudaMemcpyAsync(host, h->d_fbuf[h->fcur], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        int rc = gather_state(h, h->d_stage);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(host, h->d_stage, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+void* gpgmp_device_state(gpgmp_solver* h) {
+    if (!h) return nullptr;
+    if (normalize(h)) return nullptr;
+    return h->deterministic ? (void*)h->d_fbuf[0] : (void*)h->d_buf[0];
+}
+
+int gpgmp_init_poisson(gpgmp_solver* h, const float* lambda) {
+    if (!h || !lambda) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (h->deterministic) return set_error(GPGMP_ERR_UNSUPPORTED, "Poisson initial state is for stochastic solvers");
+    CK(cudaMemcpyAsync(h->d_lambda, lambda, sizeof(float) * h->g.S, cudaMemcpyHostToDevice, h->stream));
+    std::fill(h->cur.begin(), h->cur.end(), 0);
+    return after_launch(h, launch_init_poisson(h->g, planes_of(h), h->seed, h->d_lambda, h->stream));
+}
+
+int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
+    if (!h || !seed) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (h->deterministic) {
+        return after_launch(h, launch_rk4(h->g, h->d_fbuf[h->fcur], h->d_reactions, (int)h->reactions.size(), deltat,
+                                          h->stream));
+    }
+    int rc = after_launch(h, launch_ssa(h->g, planes_of(h), h->d_reactions, (int)h->reactions.size(), h->seed,
+                                        (uint32_t)*seed, deltat, h->d_status, h->stream));
+    (*seed)++;
+    return rc;
+}
+
+int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
+    if (!h || !seed) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (i < 0 || i >= h->g.S) return set_error(GPGMP_ERR_INVALID, "species %d", i);
+    const size_t plane_stride = 0;
+    (void)plane_stride;
+    if (h->deterministic) {
+        int rc = after_launch(h, launch_det_diffuse(h->g, h->d_fbuf[h->fcur], h->d_fbuf[1 - h->fcur], h->d_diff,
+                                                    h->dt[i], h->h * h->h, h->stream));
+        h->fcur ^= 1;
+        h->next[i] += h->dt[i];
+        return rc;
+    }
+    if (!h->inhom) {
+        const int c = h->cur[i];
+        int rc = after_launch(h, launch_homog_diffuse(h->g, h->d_buf[c], h->d_buf[1 - c], i, h->seed, (uint32_t)*seed,
+                                                      h->pmove, h->stream));
+        if (rc) return rc;
+        h->cur[i] ^= 1;
+        int32_t* base = h->d_buf[h->cur[i]];
+        const int* sm = h->m.source_mask;
+        // HomogeneousSolver.cpp:212-227 (wall 0 takes its count from source_mask[1])
+        const int counts[4] = {sm[1], sm[1], sm[2], sm[3]};
+        for (int b = 0; b < 4; ++b) {
+            if (sm[b] > 0) {
+                rc = after_launch(h, launch_source(h->g, base, i, h->seed, (uint32_t)*seed, b, counts[b], h->pi,
+                                                   h->stream));
+                if (rc) return rc;
+            }
+        }
+        h->next[i] += h->dt[i];
+        return GPGMP_OK;
+    }
+    const float dxw = h->m.physical_length / (float)h->m.width;
+    const float dyw = h->m.physical_length / (float)h->m.height;
+    if (h->nextX[i] <= t) {
+        const int c = h->cur[i];
+        int rc = after_launch(h, launch_sweep(h->g, h->d_buf[c], h->d_buf[1 - c], i, 0, h->seed, (uint32_t)*seed,
+                                              h->d_Dx, h->d_rx, h->ddX[i], dxw, h->stream));
+        if (rc) return rc;
+        h->cur[i] ^= 1;
+        (*seed)++;
+        h->nextX[i] += h->smallX[i];
+        h->ddX[i] = h->smallX[i];
+    }
+    if (h->nextY[i] <= t) {
+        const int c = h->cur[i];
+        int rc = after_launch(h, launch_sweep(h->g, h->d_buf[c], h->d_buf[1 - c], i, 1, h->seed, (uint32_t)*seed,
+                                              h->d_Dy, h->d_ry, h->ddY[i], dyw, h->stream));
+        if (rc) return rc;
+        h->cur[i] ^= 1;
+        (*seed)++;
+        h->nextY[i] += h->smallY[i];
+        h->ddY[i] = h->smallY[i];
+    }
+    h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
+    return GPGMP_OK;
+}
+
+int gpgmp_next_diffusion_time(gpgmp_solver* h, float* out) {
+    if (!h || !out) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    for (int i = 0; i < h->g.S; ++i) out[i] = h->next[i];
+    return GPGMP_OK;
+}
+
+int gpgmp_timesteps(gpgmp_solver* h, float* dtx, float* dty) {
+    if (!h || !dtx || !dty) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (!h->inhom) return set_error(GPGMP_ERR_INVALID, "time steps per direction exist for the inhomogeneous solver");
+    for (int i = 0; i < h->g.S; ++i) { dtx[i] = h->smallX[i]; dty[i] = h->smallY[i]; }
+    return GPGMP_OK;
+}
+
+int gpgmp_get_status(gpgmp_solver* h, int32_t* status) {
+    if (!h || !status) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    CK(cudaMemcpyAsync(status, h->d_status, sizeof(int32_t) * h->R, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+int gpgmp_synchronize(gpgmp_solver* h) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+// DiffusionModel::oclSolve (DiffusionModel.cpp:1414-1603).  Step n uses the
+// stream seed 64 n (the reference draws boost::uniform_int + n, :1482); every
+// doReactions and every inhomogeneous sweep advances it by one, as the
+// reference does.  Output events take two passes of the loop (the first only
+// re-arms, :1555-1571), and ties between events go to diffusion.
+int gpgmp_solve(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_snaps, int32_t* nsnap, int64_t* steps) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    const int S = h->g.S;
+    const size_t elem = h->deterministic ? sizeof(float) : sizeof(int32_t);
+    const size_t block = h->area * S * (size_t)h->R * elem;
+    int ns = 0;
+    auto snap = [&](float t) -> int {
+        if (snaps && ns < max_snaps) {
+            char* dst = (char*)snaps + (size_t)ns * block;
+            if (h->deterministic) {
+                CK(cudaMemcpyAsync(dst, h->d_fbuf[h->fcur], block, cudaMemcpyDeviceToHost, h->stream));
+            } else {
+                int rc = gather_state(h, h->d_stage);
+                if (rc) return rc;
+                CK(cudaMemcpyAsync(dst, h->d_stage, block, cudaMemcpyDeviceToHost, h->stream));
+            }
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        if (snap_times && ns < max_snaps) snap_times[ns] = t;
+        ns++;
+        return GPGMP_OK;
+    };
+    const bool stop_on_error = (h->m.flags & GPGMP_FLAG_STOP_ON_ERROR) != 0;
+    std::vector<int32_t> st_host(h->R);
+    int rc = snap(0.f);
+    if (rc) return rc;
+    float simTime = 0.f, outputLast = 0.f;
+    int64_t n = 0;
+    const gpgmp_model_desc& m = h->m;
+    while ((m.max_steps < 0 || n < m.max_steps) && simTime < m.max_time) {
+        int32_t seed = (int32_t)((uint32_t)n * 64u);
+        n++;
+        float mindt = h->next[0];
+        int minspec = 0;
+        for (int i = 1; i < S; ++i)
+            if (h->next[i] < mindt) { mindt = h->next[i]; minspec = i; }
+        int ev = 0;
+        const float mo = outputLast + m.output_interval;
+        if (mo < mindt) { mindt = mo; ev = 1; }
+        const float deltat = mindt - simTime;
+        if (m.num_reactions > 0) {
+            rc = gpgmp_do_reactions(h, deltat, &seed);
+            if (rc) return rc;
+        }
+        if (ev == 0) {
+            bool applied = false;
+            for (int i = 0; i < S; ++i) {
+                if (!(i == minspec || h->next[i] <= mindt)) continue;
+                if (!(h->next[i] > 0)) continue;
+                if (h->deterministic && applied && !(m.flags & GPGMP_FLAG_LITERAL_REDIFFUSION)) {
+                    h->next[i] += h->dt[i];
+                    continue;
+                }
+                rc = gpgmp_diffuse(h, i, mindt, &seed);
+                if (rc) return rc;
+                applied = true;
+            }
+        } else if (simTime >= outputLast + m.output_interval) {
+            rc = snap(mindt);
+            if (rc) return rc;
+            outputLast += m.output_interval;
+        }
+        simTime = mindt;
+        if (stop_on_error && !h->deterministic) {
+            rc = gpgmp_get_status(h, st_host.data());
+            if (rc) return rc;
+            bool any = false;
+            for (int v : st_host) any = any || v != 0;
+            if (any) break;
+        }
+    }
+    rc = snap(simTime);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    if (nsnap) *nsnap = ns;
+    if (steps) *steps = n;
+    return GPGMP_OK;
+}
+
+}  // extern "C"

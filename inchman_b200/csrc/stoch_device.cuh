@@ -1,0 +1,134 @@
+// Per-cell device routines of the stochastic solvers, shared by the wide kernels
+// (one launch covers every realisation) and the persistent ensemble kernel.
+//
+// Reference semantics (paths inside the reference project):
+//   ssa_cell      Gillespie.cl:58-99 direct method; hazards Reaction.cpp:119-138;
+//                 reaction picked where the cumulative hazard first exceeds r2,
+//                 which is what the isless/isgreaterequal masks of
+//                 Solver.cpp:865-904 select; the event that crosses the window
+//                 end is discarded (Gillespie.cl:80).
+//   homog_lost    StochasticHomogeneousDiffusion.cl:56-92: each particle moves to
+//                 one of four neighbours with probability (1-Stay)/6 each;
+//                 reflecting walls keep it, absorbing walls lose it.  Here the
+//                 four counts are one multinomial draw (binomial for "moved",
+//                 then an equal four-way split) instead of one uniform per particle.
+//   sweep_probs   StochasticInhomogeneousDriftDiffusion.cl:512-520 (X) and
+//                 :642-650 (Y): ps, p1 (towards +), p2-p1 (towards -).
+//   cell_timestep StochasticInhomogeneousDriftDiffusion.cl:124-151.
+#pragma once
+#include "common.cuh"
+#include "../../include/gpgmp_c.h"
+
+namespace gpgmp {
+
+__device__ __forceinline__ float hazard(const gpgmp_reaction& rc, const int* x, int stride) {
+    float v = rc.rate;
+    for (int j = 0; j < rc.num_reactants; ++j) {
+        const int a = x[rc.reactant_species[j] * stride];
+        v = v * (float)a;
+        for (int k = 1; k < rc.reactant_stoich[j]; ++k) v = v * (float)(a - k);
+    }
+    return v;
+}
+
+// Runs one SSA window on the counts x[s * stride]; returns a GPGMP_SIM_* bit or 0.
+__device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x, int stride, Stream& st,
+                                        float window) {
+    float t = 0.0f;
+    int events = 0;
+    for (;;) {
+        float h0 = 0.0f;
+        for (int r = 0; r < R; ++r) h0 = h0 + hazard(rt[r], x, stride);
+        if (!(h0 > 0.0f)) return 0;
+        const uint32_t a = st.next(), b = st.next();
+        const float r1 = u01_open0(a);
+        const float r2 = u01(b) * h0;
+        const float dtev = -gp_logf(r1) / h0;
+        t = t + dtev;
+        if (!(t < window)) return 0;
+        // second pass: same partial sums, stop at the first one above r2
+        int j = -1;
+        float hc = 0.0f;
+        for (int r = 0; r < R; ++r) {
+            hc = hc + hazard(rt[r], x, stride);
+            if (r2 < hc) { j = r; break; }
+        }
+        if (j >= 0) {
+            const gpgmp_reaction& rc = rt[j];
+            for (int q = 0; q < rc.num_products; ++q)
+                if (x[rc.product_species[q] * stride] > INT32_MAX - rc.product_stoich[q]) return SIM_OVERFLOW;
+            for (int q = 0; q < rc.num_reactants; ++q) x[rc.reactant_species[q] * stride] -= rc.reactant_stoich[q];
+            for (int q = 0; q < rc.num_products; ++q) x[rc.product_species[q] * stride] += rc.product_stoich[q];
+        }
+        if (++events >= SSA_EVENT_CAP) return SIM_EVENT_CAP;
+    }
+}
+
+// Four lost counts (-x, +x, -y, +y) of one cell of n particles.
+__device__ __forceinline__ void homog_lost(int n, float pmove, Stream& st, int x, int y, int W, int H,
+                                           const int* bmask, int l[4]) {
+    l[0] = l[1] = l[2] = l[3] = 0;
+    const int moved = binomial(st, n, pmove);
+    if (moved <= 64) {
+        uint32_t w = 0;
+        for (int i = 0; i < moved; ++i) {
+            if ((i & 15) == 0) w = st.next();
+            const uint32_t d = (w >> (2 * (i & 15))) & 3u;
+            l[0] += d == 0u; l[1] += d == 1u; l[2] += d == 2u; l[3] += d == 3u;
+        }
+    } else {
+        l[0] = binomial(st, moved, 0.25f);
+        l[1] = binomial(st, moved - l[0], 1.0f / 3.0f);
+        l[2] = binomial(st, moved - l[0] - l[1], 0.5f);
+        l[3] = moved - l[0] - l[1] - l[2];
+    }
+    if (x == 0 && bmask[0] == 0) l[0] = 0;
+    if (x == W - 1 && bmask[1] == 0) l[1] = 0;
+    if (y == 0 && bmask[2] == 0) l[2] = 0;
+    if (y == H - 1 && bmask[3] == 0) l[3] = 0;
+}
+
+__device__ __forceinline__ float clamp01(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
+
+__device__ __forceinline__ void sweep_probs(float D, float r, float dt, float dx, float* Pp, float* Pm) {
+    const float denom = 2.0f * D + r * r * dt;
+    const float ps = 1.0f - (dt * denom) / (dx * dx);
+    const float q = 1.0f - ps;
+    float p1 = 0.0f, pm = 0.0f;
+    if (denom > 0.0f) {
+        const float b = (dx * r) / denom;
+        p1 = q * (1.0f + b) * 0.5f;
+        pm = q * (1.0f - b) * 0.5f;
+    }
+    *Pp = clamp01(p1);
+    const float rest = 1.0f - *Pp;
+    *Pm = pm < 0.0f ? 0.0f : (pm > rest ? rest : pm);
+}
+
+// (minus, plus) counts of one cell for a directional sweep.
+__device__ __forceinline__ void sweep_lost(int n, float D, float r, float dt, float dx, Stream& st, bool at_lo,
+                                           bool at_hi, int mask_lo, int mask_hi, int* minus, int* plus) {
+    float Pp, Pm;
+    sweep_probs(D, r, dt, dx, &Pp, &Pm);
+    const float Pt = Pp + Pm;
+    const int moved = binomial(st, n, Pt);
+    int p = Pt > 0.0f ? binomial(st, moved, Pp / Pt) : 0;
+    int m = moved - p;
+    if (at_lo && mask_lo == 0) m = 0;
+    if (at_hi && mask_hi == 0) p = 0;
+    *minus = m;
+    *plus = p;
+}
+
+__device__ __forceinline__ float cell_timestep(float D, float r, float dx) {
+    if (r == 0.0f) return (dx * dx) / (2.0f * D) * (1.0f / 3.0f);
+    if (D == 0.0f) return dx / fabsf(r);
+    const float eps = dx * r / (2.0f * D);
+    const float th = gp_tanhf(eps);
+    const float sh = gp_sinhf(eps);
+    float temp = 1.0f + (-1.0f / (th * eps) + 1.0f / (sh * sh));
+    if (temp <= 0.0f) temp = 1.0f / 3.0f;
+    return dx / r * th * temp;
+}
+
+}  // namespace gpgmp

@@ -1,0 +1,136 @@
+"""Python mirror of the reference's solver interface over the C ABI.
+
+    s = Solver(model, realisations=16, seed=1234)
+    s.init_poisson([100, 100, 0])
+    s.do_reactions(dt, seed)            # Solver::doReactions      (Solver.h:52)
+    s.diffuse(i, t, seed)               # Solver::diffuse          (Solver.h:80)
+    s.get_next_diffusion_time()         # Solver::getNextDiffusionTime (Solver.h:68)
+    s.synchronize_state_from_device()   # Solver::synchronizeStateBufferFromDevice (Solver.h:85)
+    s.solve()                           # DiffusionModel::oclSolve (DiffusionModel.cpp:1414)
+
+HomogeneousSolver / InhomogeneousSolver are the same class chosen by the
+model's solver type, as oclSolve picks them (DiffusionModel.cpp:1425-1440).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .model import DiffusionModel
+
+
+class Solver:
+    def __init__(self, model: DiffusionModel, realisations: int = 1, seed: int = 0, sync_each_launch: bool = False,
+                 stream: Optional[int] = None):
+        self.model = model
+        self.R = int(realisations)
+        self.seed = int(seed) & 0xFFFFFFFF
+        self._desc, self._keep = model.to_desc()
+        h = C.c_void_p()
+        flags = _lib.CREATE_SYNC_EACH_LAUNCH if sync_each_launch else 0
+        _lib.call("gpgmp_solver_create", C.byref(self._desc), self.R, self.seed, flags, C.byref(h))
+        self._h = h
+        self.deterministic = model.solver == _lib.DETERMINISTIC_RK4
+        self.dtype = np.float32 if self.deterministic else np.int32
+        if stream is not None:
+            _lib.call("gpgmp_solver_set_stream", self._h, C.c_void_p(stream))
+
+    @property
+    def shape(self):
+        m = self.model
+        return (self.R, m.num_species, m.height, m.width)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().gpgmp_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state --------------------------------------------------------------------
+    def set_state(self, state: np.ndarray):
+        a = np.ascontiguousarray(state, dtype=self.dtype)
+        if a.size != int(np.prod(self.shape)):
+            raise ValueError(f"state must hold {self.shape} values")
+        _lib.call("gpgmp_set_state", self._h, a.ctypes.data_as(C.c_void_p))
+
+    synchronize_state_to_device = set_state
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=self.dtype)
+        _lib.call("gpgmp_get_state", self._h, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    synchronize_state_from_device = get_state
+
+    def init_poisson(self, lam: Sequence[float]):
+        a = np.ascontiguousarray(lam, dtype=np.float32)
+        _lib.call("gpgmp_init_poisson", self._h, a.ctypes.data_as(C.POINTER(C.c_float)))
+
+    def device_state_ptr(self) -> int:
+        return _lib.lib().gpgmp_device_state(self._h) or 0
+
+    # -- the Solver virtuals ---------------------------------------------------------
+    def do_reactions(self, deltat: float, seed: int) -> int:
+        s = C.c_int32(seed)
+        _lib.call("gpgmp_do_reactions", self._h, C.c_float(deltat), C.byref(s))
+        return s.value
+
+    def diffuse(self, species: int, current_time: float, seed: int) -> int:
+        s = C.c_int32(seed)
+        _lib.call("gpgmp_diffuse", self._h, int(species), C.c_float(current_time), C.byref(s))
+        return s.value
+
+    def get_next_diffusion_time(self) -> np.ndarray:
+        out = np.empty(self.model.num_species, dtype=np.float32)
+        _lib.call("gpgmp_next_diffusion_time", self._h, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def timesteps(self):
+        S = self.model.num_species
+        dx = np.empty(S, dtype=np.float32)
+        dy = np.empty(S, dtype=np.float32)
+        _lib.call("gpgmp_timesteps", self._h, dx.ctypes.data_as(C.POINTER(C.c_float)),
+                  dy.ctypes.data_as(C.POINTER(C.c_float)))
+        return dx, dy
+
+    def status(self) -> np.ndarray:
+        out = np.zeros(self.R, dtype=np.int32)
+        _lib.call("gpgmp_get_status", self._h, out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return out
+
+    def synchronize(self):
+        _lib.call("gpgmp_synchronize", self._h)
+
+    def solve(self, max_snapshots: int = 0, count_only: bool = False):
+        """Runs the oclSolve event loop; returns (snapshots, times, steps)."""
+        if count_only or max_snapshots == 0:
+            ns = C.c_int32(0)
+            steps = C.c_int64(0)
+            _lib.call("gpgmp_solve", self._h, None, None, 0, C.byref(ns), C.byref(steps))
+            return None, None, steps.value
+        snaps = np.zeros((max_snapshots,) + self.shape, dtype=self.dtype)
+        times = np.zeros(max_snapshots, dtype=np.float32)
+        ns = C.c_int32(0)
+        steps = C.c_int64(0)
+        _lib.call("gpgmp_solve", self._h, snaps.ctypes.data_as(C.c_void_p),
+                  times.ctypes.data_as(C.POINTER(C.c_float)), max_snapshots, C.byref(ns), C.byref(steps))
+        n = min(ns.value, max_snapshots)
+        return snaps[:n], times[:n], steps.value
+
+
+HomogeneousSolver = Solver
+InhomogeneousSolver = Solver

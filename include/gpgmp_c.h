@@ -1,0 +1,141 @@
+/*
+ * gpgmp_c.h -- C ABI of the B200 GPGMP solvers.
+ *
+ * This is the drop-in boundary for Inchman's spatial simulation hot path.  The
+ * reference's boundary is the abstract C++ class gpgmp::Solver
+ * (exec/src/gpgmp/src/Solver.h:15-239) with the concrete HomogeneousSolver
+ * (HomogeneousSolver.h:10) and InhomogeneousSolver (InhomogeneousSolver.h:11),
+ * driven by DiffusionModel::oclSolve (DiffusionModel.cpp:1414-1620).  Each
+ * function below names the member it replaces.
+ *
+ * Conventions:
+ *  - every function returns GPGMP_OK (0) or a positive GPGMP_ERR_* code and never
+ *    exits the process (the reference calls exit(1): Kernel.h:254-270,
+ *    DiffusionModel.cpp:550-565); gpgmp_last_error() gives the message of the
+ *    calling thread's last failure;
+ *  - the caller owns host buffers; a handle owns its device memory;
+ *  - a handle issues its work on one CUDA stream (the legacy default stream
+ *    unless gpgmp_solver_set_stream is called); calls are asynchronous on that
+ *    stream, the gpgmp_get_* / gpgmp_synchronize calls wait for it;
+ *  - a handle is not safe to use from two host threads at once.
+ *  - State layout is [realisation][species][y][x] with x fastest, the
+ *    reference's per-run layout (Solver.cpp:476-482) repeated per realisation.
+ */
+#ifndef GPGMP_C_H
+#define GPGMP_C_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPGMP_OK 0
+#define GPGMP_ERR_INVALID 1      /* bad argument or model */
+#define GPGMP_ERR_CUDA 2         /* a CUDA call failed; see gpgmp_last_error() */
+#define GPGMP_ERR_NOMEM 3        /* device allocation failed */
+#define GPGMP_ERR_UNSUPPORTED 4  /* feature outside what this build implements */
+#define GPGMP_ERR_TIMEOUT 5      /* a bounded device wait gave up (sort/scan look-back) */
+
+/* per-realisation simulation status bits (gpgmp_get_status) */
+#define GPGMP_SIM_EVENT_CAP 1    /* a cell hit the SSA event cap inside one window */
+#define GPGMP_SIM_OVERFLOW 2     /* a count would have passed INT32_MAX */
+
+/* SolverType (DiffusionModel.h:46-56) for the solvers this build implements */
+#define GPGMP_STOCHASTIC_HOMOGENEOUS 0
+#define GPGMP_STOCHASTIC_INHOMOGENEOUS 1
+#define GPGMP_DETERMINISTIC_RK4 2
+
+/* drift/diffusivity methods (DiffusionModel.cpp:319-380); FIELD takes per-cell arrays */
+#define GPGMP_DRIFT_FIELD (-1)
+#define GPGMP_DRIFT_HOMOGENEOUS 0          /* params: diffX, diffY, driftX, driftY */
+#define GPGMP_DRIFT_MULTIPLICATIVE_NOISE 1 /* params: sigmaX, sigmaY, muX, muY */
+#define GPGMP_DRIFT_ORNSTEIN_UHLENBECK 2   /* params: diffX, diffY, gammaXX, gammaXY, gammaYX, gammaYY */
+
+/* gpgmp_model_desc.flags */
+#define GPGMP_FLAG_STOP_ON_ERROR 4         /* end a realisation's event loop once its status is set */
+#define GPGMP_FLAG_LITERAL_REDIFFUSION 8   /* deterministic: repeat the stencil per due species (reference) */
+
+/* gpgmp_solver_create flags */
+#define GPGMP_CREATE_SYNC_EACH_LAUNCH 1    /* wait after every launch, as Kernel.h:252-253 does */
+
+/* A mass-action reaction (Reaction.h:31-211): hazard = rate * prod_s A_s (A_s - 1) ...
+ * (Reaction.cpp:119-138, no 1/n! factor). */
+typedef struct gpgmp_reaction {
+    float   rate;
+    int32_t num_reactants;
+    int32_t reactant_species[3];
+    int32_t reactant_stoich[3];
+    int32_t num_products;
+    int32_t product_species[4];
+    int32_t product_stoich[4];
+} gpgmp_reaction;
+
+/* The model fields the hot path reads (DiffusionModel.h, Species.h:23,
+ * Compartment.h:29-43; initial states are the caller's, as generateInitialStates
+ * fills them host-side, DiffusionModel.cpp:568-723). */
+typedef struct gpgmp_model_desc {
+    int32_t width, height, num_species, num_reactions;
+    float   physical_length;      /* L: cell width h = L / width */
+    float   p0;                   /* redistribution fraction, default 0.1 (DiffusionModel.cpp:150) */
+    float   max_time, output_interval;
+    int32_t max_steps;            /* < 0: unlimited */
+    int32_t boundary_mask[4];     /* x-, x+, y-, y+ : 0 reflecting, 1 absorbing (DiffusionModel.cpp:233-242) */
+    int32_t source_mask[4];       /* > 0: source wall (HomogeneousSolver.cpp:210-227) */
+    int32_t solver_type;          /* GPGMP_STOCHASTIC_* / GPGMP_DETERMINISTIC_RK4 */
+    int32_t drift_method;         /* GPGMP_DRIFT_* (inhomogeneous solver) */
+    int32_t flags;                /* GPGMP_FLAG_* */
+    float   drift_params[8];
+    const float* diffusion;           /* [num_species] diffusion constants */
+    const gpgmp_reaction* reactions;  /* [num_reactions] */
+    const float* field_dx;            /* GPGMP_DRIFT_FIELD: [S][H][W] diffusivity x */
+    const float* field_dy;            /* [S][H][W] diffusivity y */
+    const float* field_rx;            /* [S][H][W] drift x */
+    const float* field_ry;            /* [S][H][W] drift y */
+} gpgmp_model_desc;
+
+typedef struct gpgmp_solver gpgmp_solver;
+
+const char* gpgmp_last_error(void);
+int gpgmp_version(void);
+
+/* Solver(DiffusionModel&, runState, detState, SolverType, ...) -- Solver.h:33-36,
+ * HomogeneousSolver.h / InhomogeneousSolver.h:28-33.  num_realisations copies of
+ * the model run side by side; seed keys every random stream. */
+int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations, uint32_t seed,
+                        int32_t create_flags, gpgmp_solver** out);
+/* ~Solver() -- Solver.cpp:174-206 */
+int gpgmp_solver_destroy(gpgmp_solver* h);
+/* bind the handle to a CUDA stream (cudaStream_t passed as void*) */
+int gpgmp_solver_set_stream(gpgmp_solver* h, void* stream);
+/* synchronizeStateBufferToDevice / FromDevice -- Solver.h:85-93, Solver.cpp:297-315.
+ * Stochastic solvers take int32 counts, the deterministic solver float. */
+int gpgmp_set_state(gpgmp_solver* h, const void* host_state);
+int gpgmp_get_state(gpgmp_solver* h, void* host_state);
+/* device-side initial state: Poisson(lambda[s]) per cell and species */
+int gpgmp_init_poisson(gpgmp_solver* h, const float* lambda_per_species);
+/* doReactions(Real deltat, int& seed) -- Solver.h:52, Solver.cpp:207-267 */
+int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed);
+/* diffuse(int speciesIndex, Real currentTime, int& seed) -- Solver.h:80,
+ * HomogeneousSolver.cpp:203-235, InhomogeneousSolver.cpp:254-427 */
+int gpgmp_diffuse(gpgmp_solver* h, int32_t species, float current_time, int32_t* seed);
+/* getNextDiffusionTime() -- Solver.h:68, InhomogeneousSolver.cpp:238-252 */
+int gpgmp_next_diffusion_time(gpgmp_solver* h, float* out_per_species);
+/* DiffusionModel::oclSolve's event loop (DiffusionModel.cpp:1414-1603) run in C++
+ * over this solver.  Snapshots: the initial state, one per output interval, the
+ * final state; snapshots has room for max_snapshots states (NULL to count only). */
+int gpgmp_solve(gpgmp_solver* h, void* snapshots, float* snapshot_times, int32_t max_snapshots,
+                int32_t* num_snapshots, int64_t* steps);
+/* per-realisation GPGMP_SIM_* bits; the reference's debug error buffer
+ * (Gillespie.cl:86-98, Solver.cpp:274-295) turned into a status word */
+int gpgmp_get_status(gpgmp_solver* h, int32_t* status_per_realisation);
+int gpgmp_synchronize(gpgmp_solver* h);
+/* the device state buffer (for zero-copy views); valid until destroy */
+void* gpgmp_device_state(gpgmp_solver* h);
+/* computeTimestepX/Y + reduceBlocks + readback -- InhomogeneousSolver.cpp:468-500 */
+int gpgmp_timesteps(gpgmp_solver* h, float* dt_x, float* dt_y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,115 @@
+/*
+ * oracle/gpgmp_oracle.h -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * The oracle is a CPU restatement of the reference's hot path (GPGMP, the
+ * simulation engine of Inchman) and a CPU replay of this project's CUDA
+ * algorithms.  Only tests/, the smoke check and bench.py's CPU baseline use it;
+ * the product never links it.
+ *
+ * Two families of functions:
+ *   orc_ref_*  restate the reference's OpenCL kernels and host logic literally
+ *              (Threefry-2x32 keyed per cell, one uniform per particle, C
+ *              promotion rules for the kernels' double literals).  Pinned
+ *              bit-exactly against the reference's own kernel sources compiled
+ *              for the CPU (oracle/_ref).
+ *   orc_rep_*  replay the CUDA kernels of this project (Philox-4x32 streams,
+ *              binomial jump counts) with the same IEEE single-precision
+ *              operations, so that seeded GPU runs compare bit for bit.
+ *
+ * The model description has the same memory layout as gpgmp_model_desc in
+ * include/gpgmp_c.h, so one ctypes structure drives both.
+ */
+#ifndef GPGMP_ORACLE_H
+#define GPGMP_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_reaction {
+    float   rate;
+    int32_t num_reactants;
+    int32_t reactant_species[3];
+    int32_t reactant_stoich[3];
+    int32_t num_products;
+    int32_t product_species[4];
+    int32_t product_stoich[4];
+} orc_reaction;
+
+typedef struct orc_model {
+    int32_t width, height, num_species, num_reactions;
+    float   physical_length, p0, max_time, output_interval;
+    int32_t max_steps;
+    int32_t boundary_mask[4];   /* x-, x+, y-, y+ : 0 reflecting, 1 absorbing */
+    int32_t source_mask[4];
+    int32_t solver_type;        /* 0 stochastic homogeneous, 1 stochastic inhomogeneous, 2 deterministic RK4 */
+    int32_t drift_method;       /* -1 field arrays, 0 homogeneous, 1 multiplicative noise, 2 OU, 3 nonlinear */
+    int32_t flags;              /* bit 0 nonlinear diffusivity (recompute after sweeps), bit 1 compute moments */
+    float   drift_params[8];
+    const float* diffusion;            /* [S] */
+    const orc_reaction* reactions;     /* [R] */
+    const float* field_dx;             /* [S][H][W] or NULL */
+    const float* field_dy;
+    const float* field_rx;
+    const float* field_ry;
+} orc_model;
+
+/* ---- generators and elementary functions ---------------------------------- */
+void orc_threefry2x32_20(const uint32_t ctr[2], const uint32_t key[2], uint32_t out[2]);
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void orc_philox_fill(uint32_t k0, uint32_t k1, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t* out, int n);
+void orc_logf_many(const float* x, float* y, int n);
+void orc_expf_many(const float* x, float* y, int n);
+void orc_sincos2pi_many(const float* u, float* s, float* c, int n);
+void orc_binomial_many(uint32_t k0, uint32_t k1, const int32_t* n, const float* p, int32_t* out, int count);
+void orc_poisson_many(uint32_t k0, uint32_t k1, const float* lam, int32_t* out, int count);
+
+/* ---- reference-exact restatements -------------------------------------------- */
+float orc_ref_stay_probability(const orc_model* m);
+float orc_ref_cell_width(const orc_model* m);
+void orc_ref_homog_diffuse(const orc_model* m, int32_t* state, int species, int32_t seed, int32_t* lost4);
+void orc_ref_source_boundary(const orc_model* m, int32_t* state, int species, int32_t seed, int boundary, int source);
+void orc_ref_gillespie(const orc_model* m, int32_t* state, int32_t seed, float deltat);
+void orc_ref_inhomog_diffuse(const orc_model* m, int32_t* state, int species, int32_t seed, float dt, int sweep_y,
+                             const float* dx, const float* dy, const float* rx, const float* ry, int32_t* lost4);
+float orc_ref_timestep(const orc_model* m, int species, int sweep_y,
+                       const float* dx, const float* dy, const float* rx, const float* ry, float* per_cell);
+void orc_ref_det_diffuse(const orc_model* m, const float* in, float* out, float dt, int in_place);
+void orc_ref_rk4(const orc_model* m, float* state, float deltat);
+int orc_ref_solve(const orc_model* m, int32_t* state, uint32_t seed_base,
+                  int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots, int64_t* steps);
+
+/* ---- replay of the CUDA algorithms --------------------------------------------- */
+void orc_rep_init_poisson(int W, int H, int S, int R, uint32_t seed, const float* lambda_per_species, int32_t* state);
+void orc_rep_ssa(const orc_model* m, int32_t* state, int R, uint32_t seed, uint32_t step_seed, float window,
+                 int32_t* status);
+void orc_rep_homog_diffuse(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, uint32_t step_seed);
+void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int sweep_y,
+                           uint32_t step_seed, float dt, const float* dfield, const float* rfield);
+float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float* dfield, const float* rfield);
+void orc_rep_diffusivity_drift(const orc_model* m, int species, float* dx, float* dy, float* rx, float* ry);
+int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
+                  int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots,
+                  int64_t* steps, int32_t* status);
+
+/* ---- deterministic solver ----------------------------------------------------- */
+void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float dt, float* u, float* v);
+void orc_gs_forward_f64(int N, int steps, double F, double k, double Du, double Dv, double dt, double* u, double* v);
+double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, double Dv, double dt,
+                            const double* u0, const double* v0, const double* ut, const double* vt,
+                            int checkpoint_every, double* grad4);
+int orc_det_solve(const orc_model* m, float* state, float* snapshots, float* snap_times, int max_snapshots,
+                  int* num_snapshots, int64_t* steps);
+
+/* ---- sort, scan, cell offsets, particles -------------------------------------- */
+void orc_sort_pairs_u32(uint32_t* keys, uint32_t* vals, int64_t n);
+void orc_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n);
+void orc_cell_indices_ref(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* left, uint32_t* right);
+void orc_cell_offsets(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count);
+int64_t orc_particles_run(int64_t n, float* px, float* py, uint8_t* species, int grid, float D, float vx, float vy,
+                          float dt, float p_react, uint32_t seed, int step0, int nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
