@@ -156,6 +156,36 @@ __device__ __forceinline__ void gp_sincos2pi(float u, float* sn, float* cs) {
     *cs = c_;
 }
 
+
+// double-precision exp, same construction as gp_expf (two-part ln 2 with 21 trailing
+// zero bits in the high part, Taylor series to r^13)
+__device__ __forceinline__ double gp_exp_d(double x) {
+    if (x != x) return x;
+    if (x > 709.0) return INFINITY;
+    if (x < -745.0) return 0.0;
+    double kd = rint(x * 1.4426950408889634);
+    double r = fma(-kd, 0.6931471803691238, x);
+    r = fma(-kd, 1.9082149292705877e-10, r);
+    double p = fma(r, 1.0 / 6227020800.0, 1.0 / 479001600.0);
+    p = fma(r, p, 1.0 / 39916800.0);
+    p = fma(r, p, 1.0 / 3628800.0);
+    p = fma(r, p, 1.0 / 362880.0);
+    p = fma(r, p, 1.0 / 40320.0);
+    p = fma(r, p, 1.0 / 5040.0);
+    p = fma(r, p, 1.0 / 720.0);
+    p = fma(r, p, 1.0 / 120.0);
+    p = fma(r, p, 1.0 / 24.0);
+    p = fma(r, p, 1.0 / 6.0);
+    p = fma(r, p, 0.5);
+    p = fma(r, p, 1.0);
+    p = fma(r, p, 1.0);
+    int k = (int)kd;
+    int k1 = k / 2, k2 = k - k1;
+    double s1 = __longlong_as_double((long long)(k1 + 1023) << 52);
+    double s2 = __longlong_as_double((long long)(k2 + 1023) << 52);
+    return (p * s1) * s2;
+}
+
 __device__ __forceinline__ float gp_tanhf(float e) {
     float a = e < 0.0f ? -e : e;
     float t = gp_expf(-2.0f * a);

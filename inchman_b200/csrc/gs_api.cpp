@@ -1,0 +1,197 @@
+// C ABI of the Gray-Scott forward and adjoint solvers (gray_scott.cu).
+//
+// The adjoint uses two-level checkpointing: the forward pass keeps the state every
+// checkpoint_every steps; the backward pass walks the segments last to first,
+// recomputes the segment's states from its checkpoint into the work buffer
+// (one forward launch), then runs the transposed steps over them (one adjoint
+// launch).  Memory: ceil(steps/c) + c states; time: about two forward solves plus
+// the adjoint steps.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+#include "gs_kernels.h"
+#include "host_common.h"
+#include "../../include/gpgmp_c.h"
+
+using namespace gpgmp;
+
+namespace {
+
+#define CK(expr)                                                                                              \
+    do {                                                                                                      \
+        cudaError_t e_ = (expr);                                                                              \
+        if (e_ != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_));    \
+    } while (0)
+
+int check(const gpgmp_gs_params* p, int elem_bytes) {
+    if (!p) return set_error(GPGMP_ERR_INVALID, "params is NULL");
+    if (p->n <= 2 || p->steps < 0) return set_error(GPGMP_ERR_INVALID, "n %d steps %d", p->n, p->steps);
+    int cl = p->cluster > 0 ? p->cluster : gs_cluster_size(p->n, elem_bytes);
+    if (cl <= 0 || cl > 16 || p->n % cl)
+        return set_error(GPGMP_ERR_UNSUPPORTED, "lattice %d does not fit one thread-block cluster", p->n);
+    if ((size_t)elem_bytes * 4 * (size_t)(p->n / cl + 2) * p->n > 227 * 1024)
+        return set_error(GPGMP_ERR_UNSUPPORTED, "lattice %d needs more shared memory per CTA than a B200 has", p->n);
+    return GPGMP_OK;
+}
+
+GSParams to_params(const gpgmp_gs_params* p) {
+    GSParams g;
+    g.n = p->n; g.steps = p->steps;
+    g.F = p->F; g.k = p->k; g.Du = p->Du; g.Dv = p->Dv; g.vx = p->vx; g.vy = p->vy; g.dt = p->dt;
+    g.cluster = p->cluster;
+    return g;
+}
+
+int ck_every(const gpgmp_gs_params* p) { return p->checkpoint_every > 0 ? p->checkpoint_every : 100; }
+
+template <typename T>
+int forward(const gpgmp_gs_params* p, const T* u0, const T* v0, T* u, T* v, T* ckpt, void* stream) {
+    int rc = check(p, sizeof(T));
+    if (rc) return rc;
+    GSParams g = to_params(p);
+    CK(gs_forward<T>(g, u0, v0, u, v, ckpt, ck_every(p), (cudaStream_t)stream));
+    return GPGMP_OK;
+}
+
+template <typename T>
+int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T* gu, T* gv, double* grad6,
+            void* work, void* stream) {
+    int rc = check(p, sizeof(T));
+    if (rc) return rc;
+    if (!ckpt || !lu || !lv || !gu || !gv || !grad6 || !work) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int c = ck_every(p);
+    const size_t nn = (size_t)p->n * p->n;
+    T* seg = (T*)work;                       // c states, 2 nn each
+    T* lam = seg + (size_t)2 * c * nn;       // two adjoint buffers (u, v) x 2
+    T* la[2] = {lam, lam + 2 * nn};
+    CK(cudaMemsetAsync(grad6, 0, 6 * sizeof(double), st));
+    CK(cudaMemcpyAsync(la[0], lu, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(la[0] + nn, lv, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    const int nseg = (p->steps + c - 1) / c;
+    int cur = 0;
+    GSParams g = to_params(p);
+    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+        const int s0 = sgi * c;
+        const int len = std::min(c, p->steps - s0);
+        const T* cku = ckpt + (size_t)2 * sgi * nn;
+        GSParams gf = g;
+        gf.steps = len;
+        // states before steps 0..len-1 of the segment; the final state lands in the spare slot
+        T* scratch = la[1 - cur];
+        CK(gs_forward<T>(gf, cku, cku + nn, scratch, scratch + nn, seg, 1, st));
+        T* out = la[1 - cur];
+        T* outg = (sgi == 0) ? nullptr : out;
+        if (sgi == 0) {
+            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, gu, gv, grad6, st));
+        } else {
+            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, outg, outg + nn, grad6, st));
+            cur = 1 - cur;
+        }
+    }
+    if (nseg == 0) {
+        CK(cudaMemcpyAsync(gu, lu, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(gv, lv, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    }
+    return GPGMP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpgmp_gs_buffer_sizes(const gpgmp_gs_params* p, int32_t elem_bytes, size_t* ck_bytes, size_t* work_bytes) {
+    if (!p || !ck_bytes || !work_bytes) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (elem_bytes != 4 && elem_bytes != 8) return set_error(GPGMP_ERR_INVALID, "elem_bytes %d", elem_bytes);
+    const int c = ck_every(p);
+    const size_t nn = (size_t)p->n * p->n;
+    const size_t nseg = (size_t)((p->steps + c - 1) / c);
+    *ck_bytes = std::max<size_t>(1, nseg) * 2 * nn * elem_bytes;
+    *work_bytes = ((size_t)2 * c * nn + 4 * nn) * elem_bytes;
+    return GPGMP_OK;
+}
+
+int gpgmp_gs_forward_f32(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v, float* ck,
+                         void* stream) {
+    return forward<float>(p, u0, v0, u, v, ck, stream);
+}
+int gpgmp_gs_forward_f64(const gpgmp_gs_params* p, const double* u0, const double* v0, double* u, double* v,
+                         double* ck, void* stream) {
+    return forward<double>(p, u0, v0, u, v, ck, stream);
+}
+int gpgmp_gs_adjoint_f32(const gpgmp_gs_params* p, const float* ck, const float* lu, const float* lv, float* gu,
+                         float* gv, double* grad6, void* work, void* stream) {
+    return adjoint<float>(p, ck, lu, lv, gu, gv, grad6, work, stream);
+}
+int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* ck, const double* lu, const double* lv, double* gu,
+                         double* gv, double* grad6, void* work, void* stream) {
+    return adjoint<double>(p, ck, lu, lv, gu, gv, grad6, work, stream);
+}
+
+int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v) {
+    int rc = check(p, 4);
+    if (rc) return rc;
+    if (!u0 || !v0 || !u || !v) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    const size_t nn = (size_t)p->n * p->n, bytes = nn * sizeof(float);
+    cudaStream_t st = nullptr;
+    float* d = nullptr;
+    CK(cudaMallocAsync((void**)&d, 4 * bytes, st));
+    CK(cudaMemcpyAsync(d, u0, bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + nn, v0, bytes, cudaMemcpyHostToDevice, st));
+    rc = forward<float>(p, d, d + nn, d + 2 * nn, d + 3 * nn, nullptr, st);
+    if (rc == GPGMP_OK) {
+        CK(cudaMemcpyAsync(u, d + 2 * nn, bytes, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(v, d + 3 * nn, bytes, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaFreeAsync(d, st));
+    CK(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const float* v0, const float* ut,
+                            const float* vt, double* loss, double* grad6) {
+    int rc = check(p, 4);
+    if (rc) return rc;
+    if (!u0 || !v0 || !ut || !vt || !loss || !grad6) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    const size_t nn = (size_t)p->n * p->n, bytes = nn * sizeof(float);
+    size_t ckb = 0, wb = 0;
+    gpgmp_gs_buffer_sizes(p, 4, &ckb, &wb);
+    cudaStream_t st = nullptr;
+    float *d = nullptr, *ck = nullptr, *work = nullptr;
+    double* dg = nullptr;
+    CK(cudaMallocAsync((void**)&d, 8 * bytes, st));
+    CK(cudaMallocAsync((void**)&ck, ckb, st));
+    CK(cudaMallocAsync((void**)&work, wb, st));
+    CK(cudaMallocAsync((void**)&dg, 6 * sizeof(double), st));
+    CK(cudaMemcpyAsync(d, u0, bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + nn, v0, bytes, cudaMemcpyHostToDevice, st));
+    rc = forward<float>(p, d, d + nn, d + 2 * nn, d + 3 * nn, ck, st);
+    if (rc) return rc;
+    std::vector<float> un(nn), vn(nn);
+    CK(cudaMemcpyAsync(un.data(), d + 2 * nn, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(vn.data(), d + 3 * nn, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double L = 0;
+    std::vector<float> lu(nn), lv(nn);
+    for (size_t i = 0; i < nn; ++i) {
+        const double a = (double)un[i] - ut[i], b = (double)vn[i] - vt[i];
+        L += a * a + b * b;
+        lu[i] = (float)(2.0 * a);
+        lv[i] = (float)(2.0 * b);
+    }
+    CK(cudaMemcpyAsync(d + 4 * nn, lu.data(), bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + 5 * nn, lv.data(), bytes, cudaMemcpyHostToDevice, st));
+    rc = adjoint<float>(p, ck, d + 4 * nn, d + 5 * nn, d + 6 * nn, d + 7 * nn, dg, work, st);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(grad6, dg, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(d, st));
+    CK(cudaFreeAsync(ck, st));
+    CK(cudaFreeAsync(work, st));
+    CK(cudaFreeAsync(dg, st));
+    CK(cudaStreamSynchronize(st));
+    *loss = L;
+    return GPGMP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// Launchers of the Gray-Scott cluster kernels (gray_scott.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpgmp {
+
+struct GSParams {
+    int n, steps;
+    double F, k, Du, Dv, vx, vy, dt;
+    int cluster;   // CTAs per cluster, 0 = smallest that fits
+};
+
+// smallest cluster size (1..16) whose shared memory holds an n x n lattice of elem_bytes values
+int gs_cluster_size(int n, int elem_bytes);
+
+// p.steps explicit steps from (u0, v0) into (u, v).  If trace is not NULL it receives
+// the state before every step s with s % trace_every == 0:
+// trace[2 (s / trace_every) n^2 ...] = u_s, the next n^2 values v_s.
+template <typename T>
+cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, T* trace, int trace_every,
+                       cudaStream_t st);
+
+// Adjoint of `len` steps whose input states are states[j] (j = 0..len-1, layout as
+// trace above): lam_out = J^T ... J^T lam_in; adds dt-weighted parameter gradients
+// (F, k, Du, Dv, vx, vy) into grad[0..5].
+template <typename T>
+cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, const T* lu_in, const T* lv_in, T* lu_out,
+                               T* lv_out, double* grad, cudaStream_t st);
+
+}  // namespace gpgmp

@@ -120,15 +120,29 @@ __device__ __forceinline__ void sweep_lost(int n, float D, float r, float dt, fl
     *plus = p;
 }
 
-__device__ __forceinline__ float cell_timestep(float D, float r, float dx) {
-    if (r == 0.0f) return (dx * dx) / (2.0f * D) * (1.0f / 3.0f);
-    if (D == 0.0f) return dx / fabsf(r);
-    const float eps = dx * r / (2.0f * D);
-    const float th = gp_tanhf(eps);
-    const float sh = gp_sinhf(eps);
-    float temp = 1.0f + (-1.0f / (th * eps) + 1.0f / (sh * sh));
-    if (temp <= 0.0f) temp = 1.0f / 3.0f;
-    return dx / r * th * temp;
+// Evaluated in double; below |eps| = 1e-3 tanh and temp come from their series
+// (tanh eps = eps - eps^3/3, temp = 1/3 + 4 eps^2/45) because the closed form
+// cancels there (in float it gives NaN or 0 for small drift).
+__device__ __forceinline__ float cell_timestep(float Df, float rf, float dxf) {
+    const double D = Df, r = rf, dx = dxf;
+    if (r == 0.0) return (float)(dx * dx / (2.0 * D) * (1.0 / 3.0));
+    if (D == 0.0) return (float)(dx / fabs(r));
+    const double eps = dx * r / (2.0 * D);
+    const double a = fabs(eps);
+    double th, temp;
+    if (a < 1e-3) {
+        th = eps - eps * eps * eps / 3.0;
+        temp = 1.0 / 3.0 + 4.0 * eps * eps / 45.0;
+    } else {
+        const double t = gp_exp_d(-2.0 * a);
+        const double tha = (1.0 - t) / (1.0 + t);
+        th = eps < 0.0 ? -tha : tha;
+        const double E = gp_exp_d(a);
+        const double sha = (E - 1.0 / E) * 0.5;
+        temp = 1.0 + (-1.0 / (th * eps) + 1.0 / (sha * sha));
+        if (temp <= 0.0) temp = 1.0 / 3.0;
+    }
+    return (float)(dx / r * th * temp);
 }
 
 }  // namespace gpgmp

@@ -151,7 +151,10 @@ __global__ void k_timestep(int area, const float* __restrict__ D, const float* _
                            uint32_t* min_key) {
     uint32_t best = 0xffffffffu;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < area; c += gridDim.x * blockDim.x)
-        best = min(best, float_key(cell_timestep(D[c], r[c], dx)));
+    {
+        const float ts = cell_timestep(D[c], r[c], dx);
+        if (ts == ts) best = min(best, float_key(ts));   // NaN is skipped, as fminf does
+    }
     for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
     if ((threadIdx.x & 31) == 0) atomicMin(min_key, best);
 }

@@ -135,6 +135,46 @@ void* gpgmp_device_state(gpgmp_solver* h);
 /* computeTimestepX/Y + reduceBlocks + readback -- InhomogeneousSolver.cpp:468-500 */
 int gpgmp_timesteps(gpgmp_solver* h, float* dt_x, float* dt_y);
 
+
+/* ---- deterministic reaction-diffusion: Gray-Scott, forward and adjoint ----------
+ * The reference's deterministic solver (Deterministic.cl:17-238, driven as in
+ * DiffusionModel.cpp:534-548) run on the Gray-Scott network of
+ * exec/src/tests/GrayScottModel.cpp:14-60 with explicit Euler steps on a periodic
+ * n x n lattice, h = 1, plus a constant drift (vx, vy) (the drift stencil of
+ * Deterministic.cl:71-136).  The reference has no adjoint; gpgmp_gs_adjoint_* is the
+ * hand-written discrete adjoint of the same steps.
+ * Device pointers; u and v are n*n row-major arrays.  Checkpoint buffers hold
+ * ceil(steps / checkpoint_every) states, each u then v. */
+typedef struct gpgmp_gs_params {
+    int32_t n;                  /* lattice side; a multiple of the cluster size */
+    int32_t steps;
+    double  F, k, Du, Dv, vx, vy, dt;
+    int32_t checkpoint_every;   /* <= 0: 100 */
+    int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
+} gpgmp_gs_params;
+
+/* bytes of the checkpoint buffer and of the adjoint's work buffer */
+int gpgmp_gs_buffer_sizes(const gpgmp_gs_params* p, int32_t elem_bytes, size_t* checkpoint_bytes,
+                          size_t* work_bytes);
+int gpgmp_gs_forward_f32(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v,
+                         float* checkpoints, void* stream);
+int gpgmp_gs_forward_f64(const gpgmp_gs_params* p, const double* u0, const double* v0, double* u, double* v,
+                         double* checkpoints, void* stream);
+/* lam_u/lam_v: dL/du_N, dL/dv_N in; grad_u0/grad_v0: dL/du_0, dL/dv_0 out;
+ * grad6 (device, 6 doubles): dL/d(F, k, Du, Dv, vx, vy), overwritten. */
+int gpgmp_gs_adjoint_f32(const gpgmp_gs_params* p, const float* checkpoints, const float* lam_u, const float* lam_v,
+                         float* grad_u0, float* grad_v0, double* grad6, void* work, void* stream);
+int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* checkpoints, const double* lam_u,
+                         const double* lam_v, double* grad_u0, double* grad_v0, double* grad6, void* work,
+                         void* stream);
+/* Host buffers in and out: copies (u0, v0) to the device, runs the forward solve,
+ * copies (u, v) back.  Allocates its device buffers from the stream-ordered pool. */
+int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v);
+/* Host buffers: loss L = sum (u_N - ut)^2 + (v_N - vt)^2 and its gradient with
+ * respect to (F, k, Du, Dv, vx, vy) by the adjoint. */
+int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const float* v0, const float* ut,
+                            const float* vt, double* loss, double* grad6);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,11 +93,13 @@ int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
                   int64_t* steps, int32_t* status);
 
 /* ---- deterministic solver ----------------------------------------------------- */
-void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float dt, float* u, float* v);
-void orc_gs_forward_f64(int N, int steps, double F, double k, double Du, double Dv, double dt, double* u, double* v);
-double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, double Dv, double dt,
-                            const double* u0, const double* v0, const double* ut, const double* vt,
-                            int checkpoint_every, double* grad4);
+void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float vx, float vy, float dt,
+                        float* u, float* v);
+void orc_gs_forward_f64(int N, int steps, double F, double k, double Du, double Dv, double vx, double vy, double dt,
+                        double* u, double* v);
+double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, double Dv, double vx, double vy,
+                            double dt, const double* u0, const double* v0, const double* ut, const double* vt,
+                            int checkpoint_every, double* grad6);
 int orc_det_solve(const orc_model* m, float* state, float* snapshots, float* snap_times, int max_snapshots,
                   int* num_snapshots, int64_t* steps);
 

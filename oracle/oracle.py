@@ -66,9 +66,10 @@ def orc():
             "orc_rep_timestep": (f32, [vp, C.c_int, C.c_int, vp, vp]),
             "orc_rep_diffusivity_drift": (None, [vp, C.c_int, vp, vp, vp, vp]),
             "orc_rep_solve": (C.c_int, [vp, vp, C.c_int, u32, vp, vp, C.c_int, P(C.c_int), P(i64), vp]),
-            "orc_gs_forward_f32": (None, [C.c_int, C.c_int, f32, f32, f32, f32, f32, vp, vp]),
-            "orc_gs_forward_f64": (None, [C.c_int, C.c_int, f64, f64, f64, f64, f64, vp, vp]),
-            "orc_gs_loss_grad_f64": (f64, [C.c_int, C.c_int, f64, f64, f64, f64, f64, vp, vp, vp, vp, C.c_int, vp]),
+            "orc_gs_forward_f32": (None, [C.c_int, C.c_int, f32, f32, f32, f32, f32, f32, f32, vp, vp]),
+            "orc_gs_forward_f64": (None, [C.c_int, C.c_int, f64, f64, f64, f64, f64, f64, f64, vp, vp]),
+            "orc_gs_loss_grad_f64": (f64, [C.c_int, C.c_int, f64, f64, f64, f64, f64, f64, f64, vp, vp, vp, vp,
+                                           C.c_int, vp]),
             "orc_det_solve": (C.c_int, [vp, vp, vp, vp, C.c_int, P(C.c_int), P(i64)]),
             "orc_sort_pairs_u32": (None, [vp, vp, i64]),
             "orc_exclusive_scan_u32": (None, [vp, vp, i64]),

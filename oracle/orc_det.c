@@ -4,12 +4,13 @@
  * Deterministic reaction-diffusion oracles:
  *  - Gray-Scott, forward Euler, 5-point periodic Laplacian (h = 1), in float and
  *    double, and the double-precision discrete adjoint of the loss
- *    L = sum (u_N - u*)^2 + (v_N - v*)^2 with respect to (F, k, Du, Dv), with
+ *    L = sum (u_N - u*)^2 + (v_N - v*)^2 with respect to (F, k, Du, Dv, vx, vy), with
  *    checkpoints every `checkpoint_every` steps and per-segment recomputation.
  *    The network is the reference's Gray-Scott model (exec/src/tests/
  *    GrayScottModel.cpp:14-60: U+2V->3V, U->0 at F, V->0 at F+k, 0->U at F),
  *    whose deterministic laws (Reaction.cpp:145-162) give the ODE right-hand side
- *    -u v^2 + F (1 - u), u v^2 - (F + k) v.
+ *    -u v^2 + F (1 - u), u v^2 - (F + k) v; a constant drift (vx, vy) enters by
+ *    central differences (Deterministic.cl:71-136 with constant velocity).
  *  - The reference's deterministic RK4 event loop (DiffusionModel.cpp:1414-1603,
  *    HomogeneousSolver.cpp:168-192 common time step, Deterministic.cl:17-65 and
  *    :179-238), with one diffusion per event unless flags bit 3 asks for the
@@ -22,7 +23,8 @@
 
 #define IDX(x, y, N) ((size_t)(((y) + (N)) % (N)) * (N) + (size_t)(((x) + (N)) % (N)))
 
-void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float dt, float* u, float* v) {
+void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float vx, float vy, float dt,
+                        float* u, float* v) {
     const size_t n = (size_t)N * N;
     float* u2 = (float*)malloc(sizeof(float) * n);
     float* v2 = (float*)malloc(sizeof(float) * n);
@@ -35,8 +37,10 @@ void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, 
                 float lu = u[IDX(x - 1, y, N)] + u[IDX(x + 1, y, N)] + u[IDX(x, y - 1, N)] + u[IDX(x, y + 1, N)] - 4.0f * uc;
                 float lv = v[IDX(x - 1, y, N)] + v[IDX(x + 1, y, N)] + v[IDX(x, y - 1, N)] + v[IDX(x, y + 1, N)] - 4.0f * vc;
                 float uvv = uc * vc * vc;
-                u2[i] = uc + dt * (Du * lu - uvv + F * (1.0f - uc));
-                v2[i] = vc + dt * (Dv * lv + uvv - (F + k) * vc);
+                float au = vx * (u[IDX(x + 1, y, N)] - u[IDX(x - 1, y, N)]) * 0.5f + vy * (u[IDX(x, y + 1, N)] - u[IDX(x, y - 1, N)]) * 0.5f;
+                float av = vx * (v[IDX(x + 1, y, N)] - v[IDX(x - 1, y, N)]) * 0.5f + vy * (v[IDX(x, y + 1, N)] - v[IDX(x, y - 1, N)]) * 0.5f;
+                u2[i] = uc + dt * (Du * lu - au - uvv + F * (1.0f - uc));
+                v2[i] = vc + dt * (Dv * lv - av + uvv - (F + k) * vc);
             }
         memcpy(u, u2, sizeof(float) * n);
         memcpy(v, v2, sizeof(float) * n);
@@ -44,7 +48,7 @@ void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, 
     free(u2); free(v2);
 }
 
-static void gs_step_f64(int N, double F, double k, double Du, double Dv, double dt,
+static void gs_step_f64(int N, double F, double k, double Du, double Dv, double vx, double vy, double dt,
                         const double* u, const double* v, double* u2, double* v2) {
     #pragma omp parallel for schedule(static)
     for (int y = 0; y < N; ++y)
@@ -54,26 +58,29 @@ static void gs_step_f64(int N, double F, double k, double Du, double Dv, double 
             double lu = u[IDX(x - 1, y, N)] + u[IDX(x + 1, y, N)] + u[IDX(x, y - 1, N)] + u[IDX(x, y + 1, N)] - 4.0 * uc;
             double lv = v[IDX(x - 1, y, N)] + v[IDX(x + 1, y, N)] + v[IDX(x, y - 1, N)] + v[IDX(x, y + 1, N)] - 4.0 * vc;
             double uvv = uc * vc * vc;
-            u2[i] = uc + dt * (Du * lu - uvv + F * (1.0 - uc));
-            v2[i] = vc + dt * (Dv * lv + uvv - (F + k) * vc);
+            double au = vx * (u[IDX(x + 1, y, N)] - u[IDX(x - 1, y, N)]) * 0.5 + vy * (u[IDX(x, y + 1, N)] - u[IDX(x, y - 1, N)]) * 0.5;
+            double av = vx * (v[IDX(x + 1, y, N)] - v[IDX(x - 1, y, N)]) * 0.5 + vy * (v[IDX(x, y + 1, N)] - v[IDX(x, y - 1, N)]) * 0.5;
+            u2[i] = uc + dt * (Du * lu - au - uvv + F * (1.0 - uc));
+            v2[i] = vc + dt * (Dv * lv - av + uvv - (F + k) * vc);
         }
 }
 
-void orc_gs_forward_f64(int N, int steps, double F, double k, double Du, double Dv, double dt, double* u, double* v) {
+void orc_gs_forward_f64(int N, int steps, double F, double k, double Du, double Dv, double vx, double vy, double dt,
+                        double* u, double* v) {
     const size_t n = (size_t)N * N;
     double* u2 = (double*)malloc(sizeof(double) * n);
     double* v2 = (double*)malloc(sizeof(double) * n);
     for (int s = 0; s < steps; ++s) {
-        gs_step_f64(N, F, k, Du, Dv, dt, u, v, u2, v2);
+        gs_step_f64(N, F, k, Du, Dv, vx, vy, dt, u, v, u2, v2);
         memcpy(u, u2, sizeof(double) * n);
         memcpy(v, v2, sizeof(double) * n);
     }
     free(u2); free(v2);
 }
 
-double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, double Dv, double dt,
-                            const double* u0, const double* v0, const double* ut, const double* vt,
-                            int ck, double* grad4) {
+double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, double Dv, double vx, double vy,
+                            double dt, const double* u0, const double* v0, const double* ut, const double* vt,
+                            int ck, double* grad6) {
     const size_t n = (size_t)N * N;
     if (ck <= 0) ck = steps;
     const int nseg = (steps + ck - 1) / ck;
@@ -93,7 +100,7 @@ double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, dou
             memcpy(cu + (size_t)(s / ck) * n, su, sizeof(double) * n);
             memcpy(cv + (size_t)(s / ck) * n, sv, sizeof(double) * n);
         }
-        gs_step_f64(N, F, k, Du, Dv, dt, su, sv, su + n, sv + n);
+        gs_step_f64(N, F, k, Du, Dv, vx, vy, dt, su, sv, su + n, sv + n);
         memcpy(su, su + n, sizeof(double) * n);
         memcpy(sv, sv + n, sizeof(double) * n);
     }
@@ -104,20 +111,20 @@ double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, dou
         lu[i] = 2.0 * du;
         lv[i] = 2.0 * dv;
     }
-    double gF = 0, gk = 0, gDu = 0, gDv = 0;
+    double gF = 0, gk = 0, gDu = 0, gDv = 0, gvx = 0, gvy = 0;
     for (int seg = nseg - 1; seg >= 0; --seg) {
         int s0 = seg * ck, s1 = s0 + ck < steps ? s0 + ck : steps;
         int len = s1 - s0;
         memcpy(su, cu + (size_t)seg * n, sizeof(double) * n);
         memcpy(sv, cv + (size_t)seg * n, sizeof(double) * n);
         for (int j = 0; j < len - 1; ++j)
-            gs_step_f64(N, F, k, Du, Dv, dt, su + (size_t)j * n, sv + (size_t)j * n,
+            gs_step_f64(N, F, k, Du, Dv, vx, vy, dt, su + (size_t)j * n, sv + (size_t)j * n,
                         su + (size_t)(j + 1) * n, sv + (size_t)(j + 1) * n);
         for (int j = len - 1; j >= 0; --j) {
             const double* u = su + (size_t)j * n;
             const double* v = sv + (size_t)j * n;
-            double aF = 0, ak = 0, aDu = 0, aDv = 0;
-            #pragma omp parallel for schedule(static) reduction(+:aF, ak, aDu, aDv)
+            double aF = 0, ak = 0, aDu = 0, aDv = 0, avx = 0, avy = 0;
+            #pragma omp parallel for schedule(static) reduction(+:aF, ak, aDu, aDv, avx, avy)
             for (int y = 0; y < N; ++y)
                 for (int x = 0; x < N; ++x) {
                     size_t i = (size_t)y * N + x;
@@ -127,20 +134,30 @@ double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, dou
                     double a = lu[i], b = lv[i];
                     double lapa = lu[IDX(x - 1, y, N)] + lu[IDX(x + 1, y, N)] + lu[IDX(x, y - 1, N)] + lu[IDX(x, y + 1, N)] - 4.0 * a;
                     double lapb = lv[IDX(x - 1, y, N)] + lv[IDX(x + 1, y, N)] + lv[IDX(x, y - 1, N)] + lv[IDX(x, y + 1, N)] - 4.0 * b;
-                    lu2[i] = a + dt * (Du * lapa + a * (-vc * vc - F) + b * (vc * vc));
-                    lv2[i] = b + dt * (Dv * lapb + a * (-2.0 * uc * vc) + b * (2.0 * uc * vc - (F + k)));
+                    double dxa = (lu[IDX(x + 1, y, N)] - lu[IDX(x - 1, y, N)]) * 0.5;
+                    double dya = (lu[IDX(x, y + 1, N)] - lu[IDX(x, y - 1, N)]) * 0.5;
+                    double dxb = (lv[IDX(x + 1, y, N)] - lv[IDX(x - 1, y, N)]) * 0.5;
+                    double dyb = (lv[IDX(x, y + 1, N)] - lv[IDX(x, y - 1, N)]) * 0.5;
+                    double dxu = (u[IDX(x + 1, y, N)] - u[IDX(x - 1, y, N)]) * 0.5;
+                    double dyu = (u[IDX(x, y + 1, N)] - u[IDX(x, y - 1, N)]) * 0.5;
+                    double dxv = (v[IDX(x + 1, y, N)] - v[IDX(x - 1, y, N)]) * 0.5;
+                    double dyv = (v[IDX(x, y + 1, N)] - v[IDX(x, y - 1, N)]) * 0.5;
+                    lu2[i] = a + dt * (Du * lapa + vx * dxa + vy * dya + a * (-vc * vc - F) + b * (vc * vc));
+                    lv2[i] = b + dt * (Dv * lapb + vx * dxb + vy * dyb + a * (-2.0 * uc * vc) + b * (2.0 * uc * vc - (F + k)));
                     aF += dt * (a * (1.0 - uc) - b * vc);
                     ak += dt * (-b * vc);
                     aDu += dt * a * lapu;
                     aDv += dt * b * lapv;
+                    avx += dt * (-a * dxu - b * dxv);
+                    avy += dt * (-a * dyu - b * dyv);
                 }
-            gF += aF; gk += ak; gDu += aDu; gDv += aDv;
+            gF += aF; gk += ak; gDu += aDu; gDv += aDv; gvx += avx; gvy += avy;
             double* t;
             t = lu; lu = lu2; lu2 = t;
             t = lv; lv = lv2; lv2 = t;
         }
     }
-    grad4[0] = gF; grad4[1] = gk; grad4[2] = gDu; grad4[3] = gDv;
+    grad6[0] = gF; grad6[1] = gk; grad6[2] = gDu; grad6[3] = gDv; grad6[4] = gvx; grad6[5] = gvy;
     free(cu); free(cv); free(su); free(sv); free(lu); free(lv); free(lu2); free(lv2);
     return loss;
 }

@@ -123,6 +123,69 @@ static inline float orc_sinhf(float e) {
     return (E - 1.0f / E) * 0.5f;
 }
 
+
+/* double-precision exp, same construction as orc_expf: Cody-Waite reduction with a
+ * two-part ln 2 (high part with 21 trailing zero bits), Taylor series to r^13 */
+#define ORC_LN2_HI_D 0.6931471803691238
+#define ORC_LN2_LO_D 1.9082149292705877e-10
+static inline double orc_exp_d(double x) {
+    if (x != x) return x;
+    if (x > 709.0) return INFINITY;
+    if (x < -745.0) return 0.0;
+    double kd = rint(x * 1.4426950408889634);
+    double r = fma(-kd, ORC_LN2_HI_D, x);
+    r = fma(-kd, ORC_LN2_LO_D, r);
+    double p = fma(r, 1.0 / 6227020800.0, 1.0 / 479001600.0);
+    p = fma(r, p, 1.0 / 39916800.0);
+    p = fma(r, p, 1.0 / 3628800.0);
+    p = fma(r, p, 1.0 / 362880.0);
+    p = fma(r, p, 1.0 / 40320.0);
+    p = fma(r, p, 1.0 / 5040.0);
+    p = fma(r, p, 1.0 / 720.0);
+    p = fma(r, p, 1.0 / 120.0);
+    p = fma(r, p, 1.0 / 24.0);
+    p = fma(r, p, 1.0 / 6.0);
+    p = fma(r, p, 0.5);
+    p = fma(r, p, 1.0);
+    p = fma(r, p, 1.0);
+    int k = (int)kd;
+    int k1 = k / 2, k2 = k - k1;
+    uint64_t b1 = (uint64_t)(k1 + 1023) << 52, b2 = (uint64_t)(k2 + 1023) << 52;
+    double s1, s2;
+    memcpy(&s1, &b1, 8);
+    memcpy(&s2, &b2, 8);
+    return (p * s1) * s2;
+}
+
+/* Per-cell stable time step of a directional drift-diffusion sweep, the reference's
+ * formula (StochasticInhomogeneousDriftDiffusion.cl:124-151) evaluated in double:
+ *   r = 0: h^2/(2D) (1 - 2/3);  D = 0: h/|r|;
+ *   else eps = h r/(2D), temp = 1 - 1/(eps tanh eps) + 1/sinh^2 eps (<= 0 -> 1/3),
+ *        dt = h/r tanh(eps) temp,
+ * with tanh eps = eps - eps^3/3 and temp = 1/3 + 4 eps^2/45 for |eps| < 1e-3, where
+ * the closed form cancels. */
+static inline float orc_cell_timestep(float Df, float rf, float dxf) {
+    const double D = Df, r = rf, dx = dxf;
+    if (r == 0.0) return (float)(dx * dx / (2.0 * D) * (1.0 / 3.0));
+    if (D == 0.0) return (float)(dx / fabs(r));
+    const double eps = dx * r / (2.0 * D);
+    const double a = fabs(eps);
+    double th, temp;
+    if (a < 1e-3) {
+        th = eps - eps * eps * eps / 3.0;
+        temp = 1.0 / 3.0 + 4.0 * eps * eps / 45.0;
+    } else {
+        const double t = orc_exp_d(-2.0 * a);
+        const double tha = (1.0 - t) / (1.0 + t);
+        th = eps < 0.0 ? -tha : tha;
+        const double E = orc_exp_d(a);
+        const double sha = (E - 1.0 / E) * 0.5;
+        temp = 1.0 + (-1.0 / (th * eps) + 1.0 / (sha * sha));
+        if (temp <= 0.0) temp = 1.0 / 3.0;
+    }
+    return (float)(dx / r * th * temp);
+}
+
 /* Binomial(n, p) by chunked inversion. */
 static inline int orc_binomial(orc_stream* st, int n, float p) {
     if (n <= 0 || !(p > 0.0f)) return 0;

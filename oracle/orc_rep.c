@@ -261,6 +261,7 @@ void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t s
 }
 
 float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float* dfield, const float* rfield) {
+    /* StochasticInhomogeneousDriftDiffusion.cl:124-151 per cell, then the minimum (:382-423) */
     const size_t area = (size_t)m->width * m->height;
     const float dx = m->physical_length / (float)m->width;
     const float* Df = dfield + (size_t)species * area;
@@ -268,20 +269,8 @@ float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float
     (void)sweep_y;
     float best = INFINITY;
     for (size_t c = 0; c < area; ++c) {
-        float D = Df[c], r = rf[c], ts;
-        if (r == 0.0f) {
-            ts = (dx * dx) / (2.0f * D) * (1.0f / 3.0f);
-        } else if (D == 0.0f) {
-            ts = dx / fabsf(r);
-        } else {
-            float eps = dx * r / (2.0f * D);
-            float th = orc_tanhf(eps);
-            float sh = orc_sinhf(eps);
-            float temp = 1.0f + (-1.0f / (th * eps) + 1.0f / (sh * sh));
-            if (temp <= 0.0f) temp = 1.0f / 3.0f;
-            ts = dx / r * th * temp;
-        }
-        best = fminf(best, ts);
+        float ts = orc_cell_timestep(Df[c], rf[c], dx);
+        if (ts == ts) best = fminf(best, ts);
     }
     return best;
 }
