@@ -1,0 +1,328 @@
+"""Benchmark of the B200 GPGMP hot path.
+
+Default workload (one JSON line): deterministic Gray-Scott reaction-diffusion,
+256 x 256 periodic lattice, FP32, F=0.04, k=0.06, Du=0.16, Dv=0.08, dt=1, 10,000
+explicit steps (synthetic seeded initial state).  A bench step is one full
+10,000-step forward solve; value = cell-steps/s with the state resident in HBM;
+e2e = the same through the C ABI call with host buffers (copies inside the timed
+region); adjoint_forward_ratio = time of the gradient (adjoint with checkpointing,
+recomputation included) over the time of one forward solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload gray_scott|ssa_plain|ssa_batched|lotka_volterra|ensemble|particles]
+
+Multi-GPU: every rank runs its own replica (the path does not shard: replicas
+only); value = total cell-steps of all ranks / max over ranks of the time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s per B200, batched vs plain at same stats; adjoint/forward time ratio"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, index: int = 0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl != "reference":
+        torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl != "reference" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def flush_l2(buf):
+    buf.add_(1)
+
+
+# ---------------------------------------------------------------------------
+# Gray-Scott (deterministic reaction-diffusion + adjoint)
+# ---------------------------------------------------------------------------
+
+def bench_gray_scott(args, rank, world):
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = gs.GrayScottConfig()
+    n, steps = cfg.n, cfg.steps
+    cell_steps = n * n * steps
+    u0h, v0h = cfg.initial_state(np.float32)
+    dev = torch.device("cuda")
+    u0 = torch.tensor(u0h, device=dev)
+    v0 = torch.tensor(v0h, device=dev)
+    p = cfg.params()
+    l2 = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        gs.forward(u0, v0, p)
+    torch.cuda.synchronize()
+    # ---- device-resident forward: K solves, each timed with events, L2 flushed between
+    times = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush_l2(l2)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            gs.forward(u0, v0, p)
+            b.record(stream)
+            times.append((a, b))
+        torch.cuda.synchronize()
+        barrier(world)
+    per = [a.elapsed_time(b) / 1e3 for a, b in times]
+    t_total = max_over_ranks(sum(per), world)
+    value = cell_steps * args.steps * world / t_total
+    t_launch = sum(per) / len(per)
+    # ---- end to end through the C ABI with pinned host buffers
+    pu = torch.from_numpy(u0h).pin_memory()
+    pv = torch.from_numpy(v0h).pin_memory()
+    ou = torch.empty_like(pu).pin_memory()
+    ov = torch.empty_like(pv).pin_memory()
+    nu, nv, nou, nov = pu.numpy(), pv.numpy(), ou.numpy(), ov.numpy()
+    import ctypes as C
+    fh = gs._fn("gpgmp_gs_forward_host")
+    for _ in range(max(1, args.warmup)):
+        fh(C.byref(p), nu.ctypes.data_as(C.c_void_p), nv.ctypes.data_as(C.c_void_p), nou.ctypes.data_as(C.c_void_p),
+           nov.ctypes.data_as(C.c_void_p))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = fh(C.byref(p), nu.ctypes.data_as(C.c_void_p), nv.ctypes.data_as(C.c_void_p),
+                nou.ctypes.data_as(C.c_void_p), nov.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("gpgmp_gs_forward_host failed")
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = cell_steps * args.steps * world / t_e2e
+    # ---- adjoint / forward ratio (gradient of the snapshot loss)
+    ckb, _ = gs.buffer_sizes(p, 4)
+    ck = torch.empty(ckb // 4, dtype=torch.float32, device=dev)
+    ut, vt = gs.forward(u0, v0, gs.GrayScottConfig(F=0.042).params())
+    GS = gs.GrayScott()
+    th = torch.tensor(cfg.theta(), dtype=torch.float64, device=dev, requires_grad=True)
+
+    def grad_once():
+        u, v = GS.apply(u0, v0, th, steps, cfg.dt, cfg.checkpoint_every)
+        loss = ((u - ut) ** 2 + (v - vt) ** 2).sum()
+        loss.backward()
+        return loss
+
+    for _ in range(2):
+        grad_once()
+    torch.cuda.synchronize()
+    ga, gb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nrep = max(1, min(args.steps, 5))
+    ga.record(stream)
+    for _ in range(nrep):
+        grad_once()
+    gb.record(stream)
+    torch.cuda.synchronize()
+    t_grad = ga.elapsed_time(gb) / 1e3 / nrep
+    # forward + backward over forward-only time
+    ratio = t_grad / t_launch
+    peak, peak_kind = load_peaks()
+    alg_bytes = 16.0 * cell_steps
+    achieved = alg_bytes / t_launch / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "gray_scott_forward_256x256.md")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                traffic = float(ln.split(":")[1])
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_total / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": "gray_scott_256x256_periodic_fp32_10000_steps", "lattice": [n, n],
+                   "explicit_steps_per_bench_step": steps, "cell_steps_per_bench_step": cell_steps,
+                   "F": cfg.F, "k": cfg.k, "Du": cfg.Du, "Dv": cfg.Dv, "dt": cfg.dt,
+                   "l2": "flushed between timed iterations (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "adjoint_forward_ratio": ratio,
+        "gradient_ms": t_grad * 1e3,
+        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * n * n * 4,
+                "d2h_bytes_per_step": 2 * n * n * 4},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "note": "16 B/cell-step algorithmic; the lattice stays in cluster shared memory"},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline_gray_scott(cfg)
+    return line
+
+
+def cpu_baseline_gray_scott(cfg, steps=None):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    n = cfg.n
+    u0, v0 = cfg.initial_state(np.float32)
+    cores = os.cpu_count() or 1
+    k = steps or 200
+    u, v = u0.copy(), v0.copy()
+    t0 = time.perf_counter()
+    oracle.orc().orc_gs_forward_f32(n, k, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt, oracle.ptr(u),
+                                    oracle.ptr(v))
+    t = time.perf_counter() - t0
+    if t < 5.0 and steps is None:
+        k = int(min(20000, max(200, k * 10.0 / max(t, 1e-3))))
+        u, v = u0.copy(), v0.copy()
+        t0 = time.perf_counter()
+        oracle.orc().orc_gs_forward_f32(n, k, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt, oracle.ptr(u),
+                                        oracle.ptr(v))
+        t = time.perf_counter() - t0
+    return {"value": n * n * k / t, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{k} explicit steps of the 256x256 lattice (OpenMP, {cores} threads)"}
+
+
+def reference_gray_scott(args, rank, world):
+    """The reference's CPU implementation of the path: the oracle restatement (the
+    reference's deterministic reaction kernels need generated code, so the reference
+    itself does not build for this network), all host threads."""
+    from inchman_b200.gray_scott import GrayScottConfig
+    cfg = GrayScottConfig()
+    sample = 100
+    for _ in range(args.warmup):
+        cpu_baseline_gray_scott(cfg, steps=10)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_baseline_gray_scott(cfg, steps=sample)
+    t = time.perf_counter() - t0
+    v = cfg.n * cfg.n * sample * args.steps / t
+    cores = os.cpu_count() or 1
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "gray_scott_256x256_periodic_fp32_10000_steps",
+                       "sample_explicit_steps_per_bench_step": sample},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample} explicit steps of the 256x256 lattice per bench step"},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="gray_scott")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3) if args.impl != "reference" else args.warmup
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        if rank == 0:
+            line = reference_gray_scott(args, rank, world)
+            print(json.dumps(line), flush=True)
+        return 0
+    if args.workload == "gray_scott":
+        line = bench_gray_scott(args, rank, world)
+    else:
+        from inchman_b200 import workloads
+        line = workloads.run(args, rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -127,7 +127,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 1) k_gs_adjoint(GSArgs<T> a, const T* __restrict__ states, int len,
                                                            const T* __restrict__ lu_in, const T* __restrict__ lv_in,
                                                            T* __restrict__ lu_out, T* __restrict__ lv_out,
-                                                           double* __restrict__ grad) {
+                                                           double* __restrict__ grad, int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     __shared__ double red[6][kThreads / 32];
@@ -208,8 +208,374 @@ __global__ void __launch_bounds__(kThreads, 1) k_gs_adjoint(GSArgs<T> a, const T
     cl.sync();
 }
 
+
+// ---- fast path: column walk with a split-phase cluster barrier -------------------
+// Block (BX, BY): thread (tx, ty) owns columns tx, tx + BX, ... and the RPT rows
+// 1 + ty RPT .. (ty + 1) RPT of its CTA's slab; walking down a column it keeps the
+// rows above, at and below the cell in registers (three shared loads per cell and
+// field).  Per step: the interior rows (2 .. rp-1, which need no halo) are updated
+// while the cluster barrier of the previous step completes; after the wait the
+// two edge rows are updated reading the neighbouring slabs' edge rows directly from
+// their shared memory (DSMEM); then a block barrier and the arrive for this step.
+// A CTA's edge rows of a buffer are rewritten only after the next wait, which
+// needs every neighbour's arrive, which follows its reads: no read-after-write or
+// write-after-read race across CTAs.
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// Arrive without a fence of its own: threads that wrote data other CTAs will read
+// (the edge rows) release it with cluster_release() first; the rest only signal.
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_release() { asm volatile("fence.acq_rel.cluster;\n" ::: "memory"); }
+
+// Folded constants of one explicit step, applied in increment form (the small
+// update is formed first and added to the cell's value, which keeps float32
+// rounding at the size of the update):
+//   u' = u + du lap u + hx (uL - uR) + hy (uU - uD) + dtF (1 - u) - dt u v^2
+//   v' = v + dv lap v + hx (vL - vR) + hy (vU - vD) - dtFk v     + dt u v^2
+// with du = dt Du, dv = dt Dv, hx = dt vx / 2, hy = dt vy / 2, dtF = dt F,
+// dtFk = dt (F + k).
 template <typename T>
-cudaError_t launch_cluster(const void* fn, int n, int cluster, size_t smem, cudaStream_t st, void** args) {
+struct GSCoef {
+    T du, dv, hx, hy, dt, dtF, dtFk;
+    bool drift;
+    __device__ __forceinline__ explicit GSCoef(const GSArgs<T>& a) {
+        du = a.dt * a.Du;
+        dv = a.dt * a.Dv;
+        hx = a.dt * a.vx * T(0.5);
+        hy = a.dt * a.vy * T(0.5);
+        dt = a.dt;
+        dtF = a.dt * a.F;
+        dtFk = a.dt * (a.F + a.k);
+        drift = a.vx != T(0) || a.vy != T(0);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ void gs_update(const GSCoef<T>& k, T uU, T uC, T uD, T uL, T uR, T vU, T vC, T vD, T vL,
+                                          T vR, T* un, T* vn) {
+    const T uvv = uC * vC * vC;
+    const T lu = fma(T(-4), uC, (uL + uR) + (uU + uD));
+    const T lv = fma(T(-4), vC, (vL + vR) + (vU + vD));
+    T a = fma(k.du, lu, fma(-k.dtF, uC, k.dtF));
+    T b = fma(-k.dtFk, vC, k.dv * lv);
+    if (k.drift) {
+        a = fma(k.hx, uL - uR, fma(k.hy, uU - uD, a));
+        b = fma(k.hx, vL - vR, fma(k.hy, vU - vD, b));
+    }
+    *un = uC + fma(-k.dt, uvv, a);
+    *vn = vC + fma(k.dt, uvv, b);
+}
+
+// Forward kernel with the lattice side N known at compile time.
+template <typename T, int N>
+__global__ void __launch_bounds__(1024, 1) k_gs_forward_cw(GSArgs<T> a, const T* __restrict__ u0,
+                                                          const T* __restrict__ v0, T* __restrict__ uo,
+                                                          T* __restrict__ vo, T* __restrict__ trace,
+                                                          int trace_every) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    cg::cluster_group cl = cg::this_cluster();
+    const int rp = N / (int)cl.num_blocks();
+    const int r0 = (int)cl.block_rank() * rp;
+    constexpr int NN = N * N;
+    const int BX = blockDim.x, BY = blockDim.y;
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int nthr = BX * BY;
+    const int rpt = rp / BY;
+    const int rb = 1 + threadIdx.y * rpt;
+    const int ilo = rb < 2 ? 2 : rb;
+    const int ihi = rb + rpt - 1 > rp - 1 ? rp - 1 : rb + rpt - 1;
+    const unsigned rank = cl.block_rank(), nb = cl.num_blocks();
+    const unsigned up = (rank + nb - 1) % nb, down = (rank + 1) % nb;
+    const GSCoef<T> k(a);
+    const int PL = (rp + 2) * N;                // one plane: [rp + 2][N]; layout [buf][field]
+    for (int i = tid; i < rp * N; i += nthr) {
+        sm[N + i] = u0[r0 * N + i];
+        sm[PL + N + i] = v0[r0 * N + i];
+    }
+    __syncthreads();
+    cluster_arrive();
+    for (int s = 0; s < a.steps; ++s) {
+        const int cur = s & 1;
+        const T* U = sm + (2 * cur) * PL;
+        const T* V = U + PL;
+        T* Un = sm + (2 * (cur ^ 1)) * PL;
+        T* Vn = Un + PL;
+        if (trace && s % trace_every == 0) {
+            T* dst = trace + (size_t)(2 * (s / trace_every)) * NN + r0 * N;
+            for (int i = tid; i < rp * N; i += nthr) {
+                dst[i] = U[N + i];
+                dst[NN + i] = V[N + i];
+            }
+        }
+        if (ilo <= ihi) {
+            for (int c = threadIdx.x; c < N; c += BX) {
+                const int cl_ = (c + N - 1) & (N - 1), cr = (c + 1) & (N - 1);
+                T uU = U[(ilo - 1) * N + c], vU = V[(ilo - 1) * N + c];
+                T uC = U[ilo * N + c], vC = V[ilo * N + c];
+                for (int r = ilo; r <= ihi; ++r) {
+                    const int o = r * N;
+                    const T uD = U[o + N + c], vD = V[o + N + c];
+                    gs_update(k, uU, uC, uD, U[o + cl_], U[o + cr], vU, vC, vD, V[o + cl_], V[o + cr], &Un[o + c],
+                              &Vn[o + c]);
+                    uU = uC; uC = uD;
+                    vU = vC; vC = vD;
+                }
+            }
+        }
+        cluster_wait();
+        {
+            const T* Uu = cl.map_shared_rank(U, up);
+            const T* Vu = cl.map_shared_rank(V, up);
+            const T* Ud = cl.map_shared_rank(U, down);
+            const T* Vd = cl.map_shared_rank(V, down);
+            for (int i = tid; i < 2 * N; i += nthr) {
+                const int e = i / N, c = i & (N - 1);
+                const int r = e == 0 ? 1 : rp;
+                if (e == 1 && rp == 1) continue;
+                const int cl_ = (c + N - 1) & (N - 1), cr = (c + 1) & (N - 1);
+                const int o = r * N;
+                const T uU = r == 1 ? Uu[rp * N + c] : U[o - N + c];
+                const T vU = r == 1 ? Vu[rp * N + c] : V[o - N + c];
+                const T uD = r == rp ? Ud[N + c] : U[o + N + c];
+                const T vD = r == rp ? Vd[N + c] : V[o + N + c];
+                gs_update(k, uU, U[o + c], uD, U[o + cl_], U[o + cr], vU, V[o + c], vD, V[o + cl_], V[o + cr],
+                          &Un[o + c], &Vn[o + c]);
+            }
+        }
+        __syncthreads();
+        cluster_arrive();
+    }
+    cluster_wait();
+    const int fin = a.steps & 1;
+    for (int i = tid; i < rp * N; i += nthr) {
+        uo[r0 * N + i] = sm[(2 * fin) * PL + N + i];
+        vo[r0 * N + i] = sm[(2 * fin + 1) * PL + N + i];
+    }
+}
+
+// Adjoint update of one cell (the transpose of gs_update): (aX, bX) the adjoint
+// after the step around the cell, (uX, vX) the step's input state.  Adds the cell's
+// contributions to the parameter gradients, before the dt factor and signs, to t:
+//   t0 += a (1 - u), t1 += b v, t2 += a lap u, t3 += b lap v,
+//   t4 += a (uR - uL) + b (vR - vL), t5 += a (uD - uU) + b (vD - vU)
+// so that dL/dF = dt (t0 - t1), dL/dk = -dt t1, dL/dDu = dt t2, dL/dDv = dt t3,
+// dL/dvx = -dt t4 / 2, dL/dvy = -dt t5 / 2.
+template <typename T>
+__device__ __forceinline__ void gs_adj_update(const GSCoef<T>& k, T aU, T aC, T aD, T aL, T aR, T bU, T bC, T bD,
+                                              T bL, T bR, T uU, T uC, T uD, T uL, T uR, T vU, T vC, T vD, T vL,
+                                              T vR, T* an, T* bn, T t[6]) {
+    const T lap_a = fma(T(-4), aC, (aL + aR) + (aU + aD));
+    const T lap_b = fma(T(-4), bC, (bL + bR) + (bU + bD));
+    const T ba = bC - aC;
+    T x = fma(k.du, lap_a, -k.dtF * aC);
+    T y = fma(k.dv, lap_b, -k.dtFk * bC);
+    if (k.drift) {
+        x = fma(k.hx, aR - aL, fma(k.hy, aD - aU, x));
+        y = fma(k.hx, bR - bL, fma(k.hy, bD - bU, y));
+    }
+    x = fma(k.dt * (vC * vC), ba, x);
+    y = fma((k.dt + k.dt) * (uC * vC), ba, y);
+    *an = aC + x;
+    *bn = bC + y;
+    const T lu = fma(T(-4), uC, (uL + uR) + (uU + uD));
+    const T lv = fma(T(-4), vC, (vL + vR) + (vU + vD));
+    t[0] = fma(aC, T(1) - uC, t[0]);
+    t[1] = fma(bC, vC, t[1]);
+    t[2] = fma(aC, lu, t[2]);
+    t[3] = fma(bC, lv, t[3]);
+    t[4] = fma(aC, uR - uL, fma(bC, vR - vL, t[4]));
+    t[5] = fma(aC, uD - uU, fma(bC, vD - vU, t[5]));
+}
+
+__device__ __forceinline__ void grad_finish(const double g[6], double dt, double out[6]) {
+    out[0] = dt * (g[0] - g[1]);
+    out[1] = -dt * g[1];
+    out[2] = dt * g[2];
+    out[3] = dt * g[3];
+    out[4] = -0.5 * dt * g[4];
+    out[5] = -0.5 * dt * g[5];
+}
+
+// block-reduce the six per-thread gradient sums and add them to grad[0..5]
+__device__ __forceinline__ void grad_reduce(const double g[6], double dt, double* grad, double (*red)[32], int tid,
+                                            int nthr) {
+    double o[6];
+    grad_finish(g, dt, o);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double v = o[q];
+        for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+        if ((tid & 31) == 0) red[q][tid >> 5] = v;
+    }
+    __syncthreads();
+    if (tid < 6) {
+        double v = 0;
+        for (int w = 0; w < nthr / 32; ++w) v += red[tid][w];
+        atomicAdd(&grad[tid], v);
+    }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(512, 1) k_gs_adjoint_cw(GSArgs<T> a, const T* __restrict__ states, int len,
+                                                         const T* __restrict__ lu_in, const T* __restrict__ lv_in,
+                                                         T* __restrict__ lu_out, T* __restrict__ lv_out,
+                                                         double* __restrict__ grad, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    __shared__ double red[6][32];
+    cg::cluster_group cl = cg::this_cluster();
+    const int rp = N / (int)cl.num_blocks();
+    const int r0 = (int)cl.block_rank() * rp;
+    constexpr int NN = N * N;
+    const int BX = blockDim.x, BY = blockDim.y;
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int nthr = BX * BY;
+    const int rpt = rp / BY;
+    const int rb = 1 + threadIdx.y * rpt;
+    const int ilo = rb < 2 ? 2 : rb;
+    const int ihi = rb + rpt - 1 > rp - 1 ? rp - 1 : rb + rpt - 1;
+    const unsigned rank = cl.block_rank(), nb = cl.num_blocks();
+    const unsigned up = (rank + nb - 1) % nb, down = (rank + 1) % nb;
+    const GSCoef<T> k(a);
+    (void)err;
+    const int PL = (rp + 2) * N;
+    for (int i = tid; i < rp * N; i += nthr) {
+        sm[N + i] = lu_in[r0 * N + i];
+        sm[PL + N + i] = lv_in[r0 * N + i];
+    }
+    double g[6] = {0, 0, 0, 0, 0, 0};
+    __syncthreads();
+    cluster_arrive();
+    for (int j = len - 1, s = 0; j >= 0; --j, ++s) {
+        const int cur = s & 1;
+        const T* A = sm + (2 * cur) * PL;
+        const T* B = A + PL;
+        T* An = sm + (2 * (cur ^ 1)) * PL;
+        T* Bn = An + PL;
+        const T* Us = states + (size_t)(2 * j) * NN;
+        const T* Vs = Us + NN;
+        T t[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+        if (ilo <= ihi) {
+            for (int c = threadIdx.x; c < N; c += BX) {
+                const int cl_ = (c + N - 1) & (N - 1), cr = (c + 1) & (N - 1);
+                const int g0 = r0 + ilo - 1;
+                T uU = Us[(g0 - 1) * N + c], vU = Vs[(g0 - 1) * N + c];
+                T uC = Us[g0 * N + c], vC = Vs[g0 * N + c];
+                T aU = A[(ilo - 1) * N + c], bU = B[(ilo - 1) * N + c];
+                T aC = A[ilo * N + c], bC = B[ilo * N + c];
+                for (int r = ilo; r <= ihi; ++r) {
+                    const int o = r * N, go = (r0 + r - 1) * N;
+                    const T uD = Us[go + N + c], vD = Vs[go + N + c];
+                    const T aD = A[o + N + c], bD = B[o + N + c];
+                    gs_adj_update(k, aU, aC, aD, A[o + cl_], A[o + cr], bU, bC, bD, B[o + cl_], B[o + cr], uU, uC, uD,
+                                  Us[go + cl_], Us[go + cr], vU, vC, vD, Vs[go + cl_], Vs[go + cr], &An[o + c],
+                                  &Bn[o + c], t);
+                    uU = uC; uC = uD; vU = vC; vC = vD;
+                    aU = aC; aC = aD; bU = bC; bC = bD;
+                }
+            }
+        }
+        cluster_wait();
+        {
+            const T* Au = cl.map_shared_rank(A, up);
+            const T* Bu = cl.map_shared_rank(B, up);
+            const T* Ad = cl.map_shared_rank(A, down);
+            const T* Bd = cl.map_shared_rank(B, down);
+            for (int i = tid; i < 2 * N; i += nthr) {
+                const int e = i / N, c = i & (N - 1);
+                const int r = e == 0 ? 1 : rp;
+                if (e == 1 && rp == 1) continue;
+                const int cl_ = (c + N - 1) & (N - 1), cr = (c + 1) & (N - 1);
+                const int o = r * N;
+                const int gr = r0 + r - 1;
+                const int gu = (gr + N - 1) & (N - 1), gd = (gr + 1) & (N - 1);
+                const int go = gr * N;
+                const T aU = r == 1 ? Au[rp * N + c] : A[o - N + c];
+                const T bU = r == 1 ? Bu[rp * N + c] : B[o - N + c];
+                const T aD = r == rp ? Ad[N + c] : A[o + N + c];
+                const T bD = r == rp ? Bd[N + c] : B[o + N + c];
+                gs_adj_update(k, aU, A[o + c], aD, A[o + cl_], A[o + cr], bU, B[o + c], bD, B[o + cl_], B[o + cr],
+                              Us[gu * N + c], Us[go + c], Us[gd * N + c], Us[go + cl_], Us[go + cr],
+                              Vs[gu * N + c], Vs[go + c], Vs[gd * N + c], Vs[go + cl_], Vs[go + cr],
+                              &An[o + c], &Bn[o + c], t);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) g[q] += (double)t[q];
+        __syncthreads();
+        cluster_arrive();
+    }
+    cluster_wait();
+    const int fin = len & 1;
+    for (int i = tid; i < rp * N; i += nthr) {
+        lu_out[r0 * N + i] = sm[(2 * fin) * PL + N + i];
+        lv_out[r0 * N + i] = sm[(2 * fin + 1) * PL + N + i];
+    }
+    grad_reduce(g, (double)a.dt, grad, red, tid, nthr);
+}
+
+#include "gs_f32x2.cuh"
+
+template <typename T>
+const void* fwd_kernel(int n) {
+    if (sizeof(T) == 4) {
+        switch (n) {
+            case 64: return (const void*)k_gs_forward_x2<64>;
+            case 128: return (const void*)k_gs_forward_x2<128>;
+            case 256: return (const void*)k_gs_forward_x2<256>;
+            case 512: return (const void*)k_gs_forward_x2<512>;
+            default: return nullptr;
+        }
+    }
+    switch (n) {
+        case 64: return (const void*)k_gs_forward_cw<T, 64>;
+        case 128: return (const void*)k_gs_forward_cw<T, 128>;
+        case 256: return (const void*)k_gs_forward_cw<T, 256>;
+        case 512: return (const void*)k_gs_forward_cw<T, 512>;
+        default: return nullptr;
+    }
+}
+template <typename T>
+const void* adj_kernel(int n) {
+    if (sizeof(T) == 4) {
+        switch (n) {
+            case 64: return (const void*)k_gs_adjoint_x2<64>;
+            case 128: return (const void*)k_gs_adjoint_x2<128>;
+            case 256: return (const void*)k_gs_adjoint_x2<256>;
+            case 512: return (const void*)k_gs_adjoint_x2<512>;
+            default: return nullptr;
+        }
+    }
+    switch (n) {
+        case 64: return (const void*)k_gs_adjoint_cw<T, 64>;
+        case 128: return (const void*)k_gs_adjoint_cw<T, 128>;
+        case 256: return (const void*)k_gs_adjoint_cw<T, 256>;
+        case 512: return (const void*)k_gs_adjoint_cw<T, 512>;
+        default: return nullptr;
+    }
+}
+
+// Block shape of the packed float32 kernels: BX column pairs, rows split evenly.
+dim3 x2_block(int n, int cluster, int max_threads) {
+    const int bx = n / 2 < 256 ? n / 2 : 256;
+    if (bx < 32 || (n / 2) % bx) return dim3(0, 0, 1);
+    const int rp = n / cluster;
+    int by = max_threads / bx;
+    while (by > 1 && rp % by) by >>= 1;
+    if (rp % by) return dim3(0, 0, 1);
+    return dim3(bx, by, 1);
+}
+
+template <typename T>
+cudaError_t launch_cluster(const void* fn, int n, int cluster, size_t smem, cudaStream_t st, void** args,
+                           dim3 block = dim3(kThreads, 1, 1)) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (cluster > 8) {
@@ -218,7 +584,7 @@ cudaError_t launch_cluster(const void* fn, int n, int cluster, size_t smem, cuda
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster, 1, 1);
-    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -237,10 +603,26 @@ size_t smem_bytes(int n, int cluster) {
     return sizeof(T) * 2 * 2 * (size_t)(n / cluster + 2) * n;
 }
 
+// Block shape of the column-walk kernels, or bx = 0 when the lattice does not fit
+// their layout (n a multiple of 32, the CTA's rows split evenly across block rows).
+dim3 cw_block(int n, int cluster, int max_threads = 1024) {
+    if (n % 32 != 0) return dim3(0, 0, 1);
+    const int bx = n < 256 ? n : 256;
+    if (n % bx) return dim3(0, 0, 1);
+    const int rp = n / cluster;
+    int by = max_threads / bx;
+    while (by > 1 && rp % by) by >>= 1;
+    if (rp % by) return dim3(0, 0, 1);
+    return dim3(bx, by, 1);
+}
+
 }  // namespace
 
 int gs_cluster_size(int n, int elem_bytes) {
-    // the smallest cluster (<= 16) that fits the lattice in shared memory
+    // 16 CTAs (16 SMs) when the lattice splits into 16 slabs that fit, else the
+    // smallest cluster that holds the lattice in shared memory
+    if (n % 16 == 0 && (size_t)elem_bytes * 4 * (size_t)(n / 16 + 2) * n <= 200 * 1024 && cw_block(n, 16).x != 0)
+        return 16;
     for (int c : {1, 2, 4, 8, 16}) {
         if (n % c) continue;
         if ((size_t)elem_bytes * 4 * (size_t)(n / c + 2) * n <= 200 * 1024) return c;
@@ -256,16 +638,24 @@ cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, 
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     int every = trace_every > 0 ? trace_every : 1;
     void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every};
+    const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl);
+    const void* fk = fwd_kernel<T>(p.n);
+    if (blk.x != 0 && fk && !p.generic) return launch_cluster<T>(fk, p.n, cl, smem_bytes<T>(p.n, cl), st, args, blk);
     return launch_cluster<T>((const void*)k_gs_forward<T>, p.n, cl, smem_bytes<T>(p.n, cl), st, args);
 }
 
 template <typename T>
 cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, const T* lu_in, const T* lv_in, T* lu_out,
-                               T* lv_out, double* grad, cudaStream_t st) {
+                               T* lv_out, double* grad, int* err, cudaStream_t st) {
     const int cl = p.cluster > 0 ? p.cluster : gs_cluster_size(p.n, (int)sizeof(T));
     if (cl <= 0) return cudaErrorInvalidValue;
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
-    void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad};
+    void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad, &err};
+    const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl, 512);
+    const void* ak = adj_kernel<T>(p.n);
+    // the packed float32 adjoint also holds two state buffers in shared memory
+    const size_t smem = smem_bytes<T>(p.n, cl) * (sizeof(T) == 4 ? 2 : 1);
+    if (blk.x != 0 && ak && !p.generic) return launch_cluster<T>(ak, p.n, cl, smem, st, args, blk);
     return launch_cluster<T>((const void*)k_gs_adjoint<T>, p.n, cl, smem_bytes<T>(p.n, cl), st, args);
 }
 
@@ -274,8 +664,8 @@ template cudaError_t gs_forward<float>(const GSParams&, const float*, const floa
 template cudaError_t gs_forward<double>(const GSParams&, const double*, const double*, double*, double*, double*, int,
                                         cudaStream_t);
 template cudaError_t gs_adjoint_segment<float>(const GSParams&, const float*, int, const float*, const float*, float*,
-                                               float*, double*, cudaStream_t);
+                                               float*, double*, int*, cudaStream_t);
 template cudaError_t gs_adjoint_segment<double>(const GSParams&, const double*, int, const double*, const double*,
-                                                double*, double*, double*, cudaStream_t);
+                                                double*, double*, double*, int*, cudaStream_t);
 
 }  // namespace gpgmp

@@ -40,6 +40,7 @@ GSParams to_params(const gpgmp_gs_params* p) {
     g.n = p->n; g.steps = p->steps;
     g.F = p->F; g.k = p->k; g.Du = p->Du; g.Dv = p->Dv; g.vx = p->vx; g.vy = p->vy; g.dt = p->dt;
     g.cluster = p->cluster;
+    g.generic = p->variant == 1;
     return g;
 }
 
@@ -66,7 +67,9 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
     T* seg = (T*)work;                       // c states, 2 nn each
     T* lam = seg + (size_t)2 * c * nn;       // two adjoint buffers (u, v) x 2
     T* la[2] = {lam, lam + 2 * nn};
+    int* err = (int*)(lam + 4 * nn);         // status word: a bounded in-kernel wait gave up
     CK(cudaMemsetAsync(grad6, 0, 6 * sizeof(double), st));
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
     CK(cudaMemcpyAsync(la[0], lu, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(la[0] + nn, lv, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
     const int nseg = (p->steps + c - 1) / c;
@@ -84,9 +87,9 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
         T* out = la[1 - cur];
         T* outg = (sgi == 0) ? nullptr : out;
         if (sgi == 0) {
-            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, gu, gv, grad6, st));
+            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, gu, gv, grad6, err, st));
         } else {
-            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, outg, outg + nn, grad6, st));
+            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, outg, outg + nn, grad6, err, st));
             cur = 1 - cur;
         }
     }
@@ -108,7 +111,7 @@ int gpgmp_gs_buffer_sizes(const gpgmp_gs_params* p, int32_t elem_bytes, size_t* 
     const size_t nn = (size_t)p->n * p->n;
     const size_t nseg = (size_t)((p->steps + c - 1) / c);
     *ck_bytes = std::max<size_t>(1, nseg) * 2 * nn * elem_bytes;
-    *work_bytes = ((size_t)2 * c * nn + 4 * nn) * elem_bytes;
+    *work_bytes = ((size_t)2 * c * nn + 4 * nn) * elem_bytes + 16;  // + status word
     return GPGMP_OK;
 }
 
@@ -184,12 +187,15 @@ int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const flo
     CK(cudaMemcpyAsync(d + 5 * nn, lv.data(), bytes, cudaMemcpyHostToDevice, st));
     rc = adjoint<float>(p, ck, d + 4 * nn, d + 5 * nn, d + 6 * nn, d + 7 * nn, dg, work, st);
     if (rc) return rc;
+    int err = 0;
     CK(cudaMemcpyAsync(grad6, dg, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, (char*)work + wb - 16, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaFreeAsync(d, st));
     CK(cudaFreeAsync(ck, st));
     CK(cudaFreeAsync(work, st));
     CK(cudaFreeAsync(dg, st));
     CK(cudaStreamSynchronize(st));
+    if (err) return set_error(GPGMP_ERR_TIMEOUT, "a bounded wait for a TMA copy in the adjoint gave up");
     *loss = L;
     return GPGMP_OK;
 }

@@ -8,10 +8,12 @@ namespace gpgmp {
 struct GSParams {
     int n, steps;
     double F, k, Du, Dv, vx, vy, dt;
-    int cluster;   // CTAs per cluster, 0 = smallest that fits
+    int cluster;   // CTAs per cluster, 0 = 16 where the lattice fits, else the smallest that fits
+    int generic;   // 1: use the one-cell-per-iteration kernels instead of the column walk
 };
 
-// smallest cluster size (1..16) whose shared memory holds an n x n lattice of elem_bytes values
+// cluster size (<= 16) for an n x n lattice of elem_bytes values: 16 when the
+// lattice splits evenly into 16 slabs that fit, else the smallest that fits
 int gs_cluster_size(int n, int elem_bytes);
 
 // p.steps explicit steps from (u0, v0) into (u, v).  If trace is not NULL it receives
@@ -24,8 +26,9 @@ cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, 
 // Adjoint of `len` steps whose input states are states[j] (j = 0..len-1, layout as
 // trace above): lam_out = J^T ... J^T lam_in; adds dt-weighted parameter gradients
 // (F, k, Du, Dv, vx, vy) into grad[0..5].
+// err: device word set non-zero if a bounded wait inside the kernel gave up.
 template <typename T>
 cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, const T* lu_in, const T* lv_in, T* lu_out,
-                               T* lv_out, double* grad, cudaStream_t st);
+                               T* lv_out, double* grad, int* err, cudaStream_t st);
 
 }  // namespace gpgmp

@@ -25,7 +25,7 @@ class GSParams(C.Structure):
     _fields_ = [("n", C.c_int32), ("steps", C.c_int32),
                 ("F", C.c_double), ("k", C.c_double), ("Du", C.c_double), ("Dv", C.c_double),
                 ("vx", C.c_double), ("vy", C.c_double), ("dt", C.c_double),
-                ("checkpoint_every", C.c_int32), ("cluster", C.c_int32)]
+                ("checkpoint_every", C.c_int32), ("cluster", C.c_int32), ("variant", C.c_int32)]
 
 
 _SIGS = {
@@ -65,11 +65,12 @@ class GrayScottConfig:
     dt: float = 1.0
     checkpoint_every: int = 100
     cluster: int = 0
+    variant: int = 0
     seed: int = 1234
 
     def params(self, **over) -> GSParams:
         d = dict(n=self.n, steps=self.steps, F=self.F, k=self.k, Du=self.Du, Dv=self.Dv, vx=self.vx, vy=self.vy,
-                 dt=self.dt, checkpoint_every=self.checkpoint_every, cluster=self.cluster)
+                 dt=self.dt, checkpoint_every=self.checkpoint_every, cluster=self.cluster, variant=self.variant)
         d.update(over)
         p = GSParams()
         for k_, v_ in d.items():
@@ -131,6 +132,10 @@ def adjoint(p: GSParams, checkpoints, lam_u, lam_v):
                          C.c_void_p(lam_v.contiguous().data_ptr()), C.c_void_p(gu.data_ptr()),
                          C.c_void_p(gv.data_ptr()), C.c_void_p(g6.data_ptr()), C.c_void_p(work.data_ptr()),
                          _stream_ptr(torch, lam_u.device)), name)
+    # the work buffer's last 16 bytes hold the kernels' status word
+    status = work.view(torch.uint8)[wb - 16: wb - 12].view(torch.int32)
+    if int(status.item()) != 0:
+        raise _lib.GpgmpError(5, name, "a bounded wait for a TMA copy in the adjoint gave up")
     return gu, gv, g6
 
 
@@ -145,7 +150,7 @@ def _make_autograd():
             th = theta.detach().double().cpu().tolist()
             n = u0.shape[-1]
             p = GSParams(n=n, steps=steps, F=th[0], k=th[1], Du=th[2], Dv=th[3], vx=th[4], vy=th[5], dt=dt,
-                         checkpoint_every=checkpoint_every, cluster=0)
+                         checkpoint_every=checkpoint_every, cluster=0, variant=0)
             eb = 8 if u0.dtype == torch.float64 else 4
             ckb, _ = buffer_sizes(p, eb)
             ck = torch.empty(ckb // eb, dtype=u0.dtype, device=u0.device)

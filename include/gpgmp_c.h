@@ -151,6 +151,7 @@ typedef struct gpgmp_gs_params {
     double  F, k, Du, Dv, vx, vy, dt;
     int32_t checkpoint_every;   /* <= 0: 100 */
     int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
+    int32_t variant;            /* 0: column-walk kernels where the lattice allows, 1: one cell per iteration */
 } gpgmp_gs_params;
 
 /* bytes of the checkpoint buffer and of the adjoint's work buffer */

@@ -43,10 +43,10 @@ def _oracle_forward64(cfg, u0, v0):
     return u, v
 
 
-@pytest.mark.parametrize("cluster", [0, 1, 4, 8])
-def test_forward_f64_matches_oracle(gpgmp, cluster):
+@pytest.mark.parametrize("cluster,variant", [(0, 0), (1, 0), (4, 0), (8, 0), (16, 0), (4, 1), (16, 1)])
+def test_forward_f64_matches_oracle(gpgmp, cluster, variant):
     import torch
-    cfg = _cfg(n=64, steps=300, vx=0.05, vy=-0.03, cluster=cluster)
+    cfg = _cfg(n=64, steps=300, vx=0.05, vy=-0.03, cluster=cluster, variant=variant)
     u0, v0 = _init(cfg)
     gu, gv = _gpu_forward(cfg, u0, v0, torch.float64)
     ou, ov = _oracle_forward64(cfg, u0, v0)
@@ -64,10 +64,11 @@ def test_forward_f32_within_1e5_of_f64(gpgmp):
     assert err < 1e-5, err
 
 
-def test_adjoint_f64_matches_oracle_adjoint(gpgmp):
+@pytest.mark.parametrize("cluster", [2, 16])
+def test_adjoint_f64_matches_oracle_adjoint(gpgmp, cluster):
     import torch
     from inchman_b200 import gray_scott as gs
-    cfg = _cfg(n=32, steps=250, checkpoint_every=40, vx=0.1, vy=0.05, cluster=2)
+    cfg = _cfg(n=64, steps=250, checkpoint_every=40, vx=0.1, vy=0.05, cluster=cluster)
     u0, v0 = _init(cfg)
     rng = np.random.default_rng(3)
     ut = u0 + 0.05 * rng.standard_normal(u0.shape)
