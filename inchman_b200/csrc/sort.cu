@@ -1,0 +1,436 @@
+// Scan, radix sort and cell offsets of the individual-particle path.
+//
+// Reference: IndividualSolver sorts (cell, id) pairs with an LSD radix sort of
+// 4-bit digits built from block sort / radix offsets / 3-kernel exclusive scan /
+// reorder, 6 synchronous launches per pass and 8 passes (IndividualSolver.cpp:673-808,
+// kernels IndividualSolver.cl:36-369, 493-553), then derives each cell's first and
+// last particle (computeCellIndices, IndividualSolver.cl:564-619).  The result is
+// the stable sort by cell.
+//
+// Here, from the published methods (not from the reference's SDK-derived code):
+//  - exclusive scan: single pass with decoupled look-back (Merrill & Garland 2016);
+//  - radix sort: onesweep (Adinets & Merrill 2022): one histogram kernel for every
+//    digit position, then one kernel per 8-bit digit that ranks its tile (warp
+//    match_any), publishes per-digit tile counts, looks back for the prefix and
+//    scatters through shared memory; stable;
+//  - cell offsets: key histogram + exclusive scan (start), count; the reference's
+//    left/right indices follow from them.
+// Every look-back spin has an iteration limit; exceeding it sets the error word
+// (GPGMP_ERR_TIMEOUT for the caller) and the kernel continues without waiting.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "sort_kernels.h"
+
+namespace gpgmp {
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;   // 4096
+constexpr uint64_t kScanFlagA = 1ull << 32;
+constexpr uint64_t kScanFlagP = 2ull << 32;
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+__device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// ---- exclusive scan ------------------------------------------------------------
+// scratch: [0] tile counter, [1] error word, then one status word per tile:
+// (flag << 32) | value, flag 0 = not ready, 1 = tile aggregate, 2 = inclusive prefix.
+__global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t* __restrict__ in,
+                                                                 uint32_t* __restrict__ out, int64_t n,
+                                                                 uint64_t* __restrict__ scratch) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    __shared__ uint32_t s_prefix;
+    unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
+    int* err = reinterpret_cast<int*>(scratch) + 2;
+    uint64_t* status = scratch + 2;
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    if (base + kScanItems <= n) {
+        const uint4* p = reinterpret_cast<const uint4*>(in + base);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            uint4 w = p[q];
+            v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) v[q] = base + q < n ? in[base + q] : 0u;
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) sum += v[q];
+    // block exclusive scan of the thread sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < kScanThreads / 32) s_warp[lane] = w;   // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t warp_excl = warp == 0 ? 0u : s_warp[warp - 1];
+    const uint32_t thread_excl = warp_excl + incl - sum;
+    const uint32_t aggregate = s_warp[kScanThreads / 32 - 1];
+    // decoupled look-back by warp 0
+    if (warp == 0) {
+        uint32_t exclusive = 0;
+        if (tile == 0) {
+            if (lane == 0) st_release_u64(&status[0], kScanFlagP | aggregate);
+        } else {
+            if (lane == 0) st_release_u64(&status[tile], kScanFlagA | aggregate);
+            int64_t look = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            bool done = false;
+            while (!done) {
+                const int64_t idx = look - lane;
+                uint64_t w = idx >= 0 ? ld_volatile_u64(&status[idx]) : kScanFlagP;
+                uint32_t flag = (uint32_t)(w >> 32);
+                // wait until every lane of the window has at least an aggregate
+                if (__any_sync(0xffffffffu, flag == 0)) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) atomicExch(err, 1);
+                        break;
+                    }
+                    continue;
+                }
+                const unsigned pmask = __ballot_sync(0xffffffffu, flag == 2);
+                // lanes up to and including the first inclusive prefix contribute
+                const int first_p = pmask ? __ffs(pmask) - 1 : 32;
+                uint32_t val = lane <= first_p ? (uint32_t)w : 0u;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                exclusive += val;
+                if (pmask) done = true;
+                else look -= 32;
+            }
+            if (lane == 0) st_release_u64(&status[tile], kScanFlagP | (uint32_t)(exclusive + aggregate));
+        }
+        if (lane == 0) s_prefix = exclusive;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + thread_excl;
+    if (base + kScanItems <= n) {
+        uint4* p = reinterpret_cast<uint4*>(out + base);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            uint4 w;
+            w.x = run; run += v[4 * q];
+            w.y = run; run += v[4 * q + 1];
+            w.z = run; run += v[4 * q + 2];
+            w.w = run; run += v[4 * q + 3];
+            p[q] = w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) {
+            if (base + q < n) out[base + q] = run;
+            run += v[q];
+        }
+    }
+}
+
+// ---- radix sort ------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 15;
+constexpr int kSortTile = kSortThreads * kSortItems;   // 3840
+constexpr int kWarps = kSortThreads / 32;
+constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
+
+// one pass over the keys counts every digit position: hist[pass][256]
+__global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n, int passes,
+                                                         uint32_t* __restrict__ hist) {
+    __shared__ uint32_t s_h[4][256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xffu], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+        const uint32_t c = (&s_h[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// exclusive scan of each pass's 256 bins (one block per pass)
+__global__ void k_radix_bin_offsets(uint32_t* __restrict__ hist) {
+    __shared__ uint32_t s[256];
+    uint32_t* h = hist + blockIdx.x * 256;
+    s[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    h[threadIdx.x] = s[threadIdx.x] - h[threadIdx.x];
+}
+
+// One onesweep pass.  Warp w of a tile owns keys [w*32*IT, (w+1)*32*IT) of the tile
+// in a warp-striped layout (item j of lane l is key j*32 + l), so processing items in
+// order and lanes in order is index order: the ranks are stable.
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ kin,
+                                                           const uint32_t* __restrict__ vin,
+                                                           uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                           int64_t n, int shift, const uint32_t* __restrict__ bins,
+                                                           uint32_t* __restrict__ look, unsigned int* tile_counter,
+                                                           int* err) {
+    __shared__ uint32_t s_warp_hist[kWarps][256];
+    __shared__ uint32_t s_tile_off[256];     // exclusive offset of each digit inside the tile
+    __shared__ uint32_t s_global[256];       // global start of each digit's run of this tile
+    __shared__ uint32_t s_keys[kSortTile];
+    __shared__ uint32_t s_vals[kSortTile];
+    __shared__ uint32_t s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < kWarps * 256; i += kSortThreads) (&s_warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int64_t tbase = (int64_t)tile * kSortTile;
+    const int64_t wbase = tbase + (int64_t)warp * 32 * kSortItems;
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int64_t idx = wbase + j * 32 + lane;
+        const bool ok = idx < n;
+        key[j] = ok ? kin[idx] : 0xffffffffu;
+        val[j] = ok ? vin[idx] : 0u;
+    }
+    // warp-level ranking (stable)
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int64_t idx = wbase + j * 32 + lane;
+        const bool ok = idx < n;
+        const unsigned active = __ballot_sync(0xffffffffu, ok);
+        const uint32_t d = (key[j] >> shift) & 0xffu;
+        unsigned peers = __match_any_sync(0xffffffffu, ok ? d : 0x100u + lane);
+        peers &= active;
+        uint32_t prior = 0;
+        if (ok) {
+            const int leader = __ffs(peers) - 1;
+            const uint32_t cnt = __popc(peers);
+            if (lane == leader) prior = s_warp_hist[warp][d], s_warp_hist[warp][d] = prior + cnt;
+            prior = __shfl_sync(peers, prior, leader);
+            rank[j] = prior + __popc(peers & lt);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: counts over warps -> warp offsets (in place) and the tile count
+    const int d = threadIdx.x;   // 256 threads = 256 digits
+    uint32_t tile_count = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = s_warp_hist[w][d];
+        s_warp_hist[w][d] = tile_count;
+        tile_count += c;
+    }
+    // publish the tile count, then look back for the prefix of this digit
+    uint32_t* lk = look + (size_t)tile * 256;
+    if (tile == 0) st_release_u32(&lk[d], kFlagP | tile_count);
+    else st_release_u32(&lk[d], kFlagA | tile_count);
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+            const uint32_t w = ld_acquire_u32(&look[(size_t)t * 256 + d]);
+            const uint32_t f = w & ~kValMask;
+            if (f == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                continue;
+            }
+            excl += w & kValMask;
+            if (f == kFlagP) break;
+            --t;
+        }
+        st_release_u32(&lk[d], kFlagP | ((excl + tile_count) & kValMask));
+    }
+    // tile-local digit offsets (exclusive scan of tile_count over digits)
+    {
+        uint32_t incl = tile_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        __shared__ uint32_t s_w[kWarps];
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        uint32_t wo = 0;
+        for (int w = 0; w < warp; ++w) wo += s_w[w];
+        s_tile_off[d] = wo + incl - tile_count;
+        s_global[d] = bins[d] + excl;
+    }
+    __syncthreads();
+    // stage keys and values in tile-sorted order
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int64_t idx = wbase + j * 32 + lane;
+        if (idx < n) {
+            const uint32_t dd = (key[j] >> shift) & 0xffu;
+            const uint32_t lp = s_tile_off[dd] + s_warp_hist[warp][dd] + rank[j];
+            s_keys[lp] = key[j];
+            s_vals[lp] = val[j];
+        }
+    }
+    __syncthreads();
+    const int valid = (int)(n - tbase < kSortTile ? n - tbase : kSortTile);
+    for (int i = threadIdx.x; i < valid; i += kSortThreads) {
+        const uint32_t k = s_keys[i];
+        const uint32_t dd = (k >> shift) & 0xffu;
+        const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
+        kout[g] = k;
+        vout[g] = s_vals[i];
+    }
+}
+
+__global__ void k_histogram_cells(const uint32_t* __restrict__ keys, int64_t n, uint32_t ncells,
+                                  uint32_t* __restrict__ count) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k < ncells) atomicAdd(&count[k], 1u);
+    }
+}
+
+__global__ void k_left_right(const uint32_t* __restrict__ start, const uint32_t* __restrict__ count, int64_t ncells,
+                             uint32_t* __restrict__ left, uint32_t* __restrict__ right) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = start[c], k = count[c];
+        left[c] = s;
+        right[c] = k ? s + k - 1 : s;
+    }
+}
+
+inline unsigned grid_cap(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return (unsigned)b;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+size_t scan_scratch_bytes(int64_t n) {
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    return (size_t)(2 + tiles) * sizeof(uint64_t);
+}
+
+cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st);
+    if (e != cudaSuccess) return e;
+    k_scan_exclusive<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, (uint64_t*)scratch);
+    return cudaGetLastError();
+}
+
+int scan_error_flag_offset() { return 8; }   // byte offset of the error word inside the scan scratch
+
+SortLayout sort_layout(int64_t n, int key_bits) {
+    SortLayout L{};
+    L.passes = (key_bits + 7) / 8;
+    if (L.passes < 1) L.passes = 1;
+    if (L.passes > 4) L.passes = 4;
+    L.tiles = (n + kSortTile - 1) / kSortTile;
+    size_t off = 0;
+    L.off_hist = off;    off += align256(sizeof(uint32_t) * 256 * 4);
+    L.off_counters = off; off += align256(sizeof(uint32_t) * 8);     // tile counters [4], error word [4]
+    L.off_look = off;    off += align256(sizeof(uint32_t) * 256 * (size_t)(L.tiles > 0 ? L.tiles : 1) * L.passes);
+    L.off_alt_keys = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    L.off_alt_vals = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    L.bytes = off;
+    return L;
+}
+
+cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
+                                 int key_bits, void* scratch, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const SortLayout L = sort_layout(n, key_bits);
+    char* base = (char*)scratch;
+    uint32_t* hist = (uint32_t*)(base + L.off_hist);
+    uint32_t* counters = (uint32_t*)(base + L.off_counters);
+    uint32_t* look = (uint32_t*)(base + L.off_look);
+    uint32_t* ak = (uint32_t*)(base + L.off_alt_keys);
+    uint32_t* av = (uint32_t*)(base + L.off_alt_vals);
+    cudaError_t e = cudaMemsetAsync(base, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
+    if (e != cudaSuccess) return e;
+    k_radix_histogram<<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
+    k_radix_bin_offsets<<<L.passes, 256, 0, st>>>(hist);
+    // ping-pong so that the last pass lands in (kout, vout)
+    const uint32_t* sk = kin;
+    const uint32_t* sv = vin;
+    for (int p = 0; p < L.passes; ++p) {
+        const bool last = p == L.passes - 1;
+        const bool to_out = ((L.passes - 1 - p) % 2) == 0;
+        uint32_t* dk = to_out ? kout : ak;
+        uint32_t* dv = to_out ? vout : av;
+        (void)last;
+        k_onesweep<<<(unsigned)L.tiles, kSortThreads, 0, st>>>(sk, sv, dk, dv, n, 8 * p, hist + 256 * p,
+                                                               look + (size_t)256 * L.tiles * p, counters + p,
+                                                               (int*)(counters + 4));
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        sk = dk;
+        sv = dv;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
+                             void* scan_scratch, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * (size_t)ncells, st);
+    if (e != cudaSuccess) return e;
+    if (n > 0) k_histogram_cells<<<grid_cap(n, 256), 256, 0, st>>>(sorted_keys, n, (uint32_t)ncells, count);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return scan_exclusive_u32(count, start, ncells, scan_scratch, st);
+}
+
+cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left,
+                           uint32_t* right, cudaStream_t st) {
+    k_left_right<<<grid_cap(ncells, 256), 256, 0, st>>>(start, count, ncells, left, right);
+    return cudaGetLastError();
+}
+
+}  // namespace gpgmp

@@ -1,0 +1,32 @@
+// Launchers of the scan / radix sort / cell-offset kernels (sort.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpgmp {
+
+// scratch of one exclusive scan of n values: a tile counter, an error word and one
+// status word per 4096-value tile; the error word sits at byte scan_error_flag_offset()
+size_t scan_scratch_bytes(int64_t n);
+int scan_error_flag_offset();
+cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, cudaStream_t st);
+
+struct SortLayout {
+    int passes;
+    int64_t tiles;
+    size_t off_hist, off_counters, off_look, off_alt_keys, off_alt_vals, bytes;
+};
+// scratch layout of one radix sort; the error word is the uint32 at off_counters + 16
+SortLayout sort_layout(int64_t n, int key_bits);
+cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
+                                 int key_bits, void* scratch, cudaStream_t st);
+
+// count[c] = number of keys equal to c, start = exclusive scan of count
+cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
+                             void* scan_scratch, cudaStream_t st);
+// the reference's [left, right] cell indices from start and count
+cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left,
+                           uint32_t* right, cudaStream_t st);
+
+}  // namespace gpgmp

@@ -176,6 +176,58 @@ int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float
 int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const float* v0, const float* ut,
                             const float* vt, double* loss, double* grad6);
 
+/* ---- individual particles: exclusive scan, radix sort, cell offsets -------------
+ * The reference sorts each individual species' (cell, id) keys with a stable LSD
+ * radix sort (IndividualSolver::sortSpecies / radixSortStep / scanExclusive,
+ * IndividualSolver.cpp:673-808) and derives cell index ranges
+ * (IndividualSolver::computeCellIndices, IndividualSolver.cpp:1083-1098,
+ * kernel IndividualSolver.cl:564-619).  Device pointers; the caller passes a
+ * scratch buffer of at least the queried size.  The calls are asynchronous on
+ * `stream`; a look-back wait that exceeded its iteration limit is reported by
+ * gpgmp_scratch_status (kind 0: scan scratch, 1: sort scratch) as GPGMP_ERR_TIMEOUT. */
+int gpgmp_scan_scratch_bytes(int64_t n, size_t* bytes);
+/* out[i] = in[0] + ... + in[i-1] (mod 2^32); out[0] = 0 */
+int gpgmp_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, size_t scratch_bytes,
+                             void* stream);
+int gpgmp_sort_scratch_bytes(int64_t n, int32_t key_bits, size_t* bytes);
+/* stable sort of (key, value) by the low key_bits bits of key; n < 2^30; in and out
+ * must not overlap */
+int gpgmp_sort_pairs_u32(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                         int64_t n, int32_t key_bits, void* scratch, size_t scratch_bytes, void* stream);
+/* count[c] = #keys == c, start[c] = exclusive scan of count (scratch: scan of ncells) */
+int gpgmp_cell_offsets(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
+                       void* scratch, size_t scratch_bytes, void* stream);
+/* the reference's cell index ranges: left = start, right = start + count - 1
+ * (= start for an empty cell, the index of the next particle) */
+int gpgmp_cell_indices(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left, uint32_t* right,
+                       void* stream);
+int gpgmp_scratch_status(const void* scratch, int32_t kind, int64_t n, int32_t key_bits, int32_t* status);
+
+/* ---- individual particles on the lattice: move, bin, react, compact ---------------
+ * The reference's individual solver (IndividualSolver.cpp:416-712, 458-671) moves
+ * (cell, id) keys cell by cell, re-sorts them and keeps the population by scans and
+ * compaction.  This handle keeps continuous positions and a species byte (0 = A,
+ * 1 = B) per particle on a G x G lattice of unit cells; one step is a Brownian move
+ * (diffusion D, drift (vx, vy), reflecting walls), binning by stable radix sort of the
+ * cell index plus exclusive scan of the cell counts, in-cell A + B -> 0 (the k-th A
+ * pairs with the k-th B in sorted order, each pair reacts with probability p_react)
+ * and compaction of the survivors in sorted order. */
+typedef struct gpgmp_particles gpgmp_particles;
+int gpgmp_particles_create(int64_t capacity, int32_t grid, float D, float vx, float vy, float dt, float p_react,
+                           uint32_t seed, gpgmp_particles** out);
+int gpgmp_particles_destroy(gpgmp_particles* h);
+int gpgmp_particles_set_stream(gpgmp_particles* h, void* stream);
+/* host arrays in; step = index of the next step (keys the random streams) */
+int gpgmp_particles_set(gpgmp_particles* h, const float* x, const float* y, const uint8_t* species, int64_t n,
+                        int32_t step);
+int gpgmp_particles_get(gpgmp_particles* h, float* x, float* y, uint8_t* species, int64_t* n);
+int gpgmp_particles_step(gpgmp_particles* h, int32_t nsteps);
+/* the last step's bins (host arrays, any may be NULL): start/count per cell, the sorted
+ * cell keys and the sorting permutation */
+int gpgmp_particles_bins(gpgmp_particles* h, uint32_t* start, uint32_t* count, uint32_t* sorted_keys,
+                         uint32_t* sorted_index, int64_t* n_binned);
+int gpgmp_particles_status(gpgmp_particles* h, int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,101 @@
+"""GPU parity of the individual-particle path: scan, radix sort, cell offsets,
+the reference's cell indices and the full binning step -- all bit-exact against
+the oracle (stable sort / prefix sums / the CPU replay of the step)."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+
+def _np(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("n", [0, 1, 5, 4095, 4096, 4097, 100_003, 1 << 22])
+def test_exclusive_scan_bit_exact(gpgmp, n):
+    from inchman_b200 import individual as ind
+    rng = np.random.default_rng(n)
+    x = rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    if n:
+        x[: min(n, 7)] = 0xFFFFFFFF   # wrap-around mod 2^32
+    want = np.zeros(n, np.uint32)
+    oracle.orc().orc_exclusive_scan_u32(oracle.ptr(x), oracle.ptr(want), n)
+    if n == 0:
+        return
+    scratch = ind.scan_scratch(n)
+    got = _np(ind.exclusive_scan_u32(_t(x), scratch))
+    assert np.array_equal(got, want)
+    assert ind.scratch_status(scratch, 0) == 0
+
+
+@pytest.mark.parametrize("n,bits", [(1, 32), (3839, 8), (3841, 20), (65536, 32), (1_000_003, 21), (1 << 22, 20)])
+def test_sort_pairs_stable_bit_exact(gpgmp, n, bits):
+    from inchman_b200 import individual as ind
+    rng = np.random.default_rng(bits + n)
+    hi = 1 << bits
+    keys = rng.integers(0, hi, size=n, dtype=np.uint64).astype(np.uint32)
+    keys[::2] %= 4096          # many equal keys: stability matters
+    vals = np.arange(n, dtype=np.uint32)
+    wk, wv = keys.copy(), vals.copy()
+    oracle.orc().orc_sort_pairs_u32(oracle.ptr(wk), oracle.ptr(wv), n)
+    ko, vo, scratch = ind.sort_pairs_u32(_t(keys), _t(vals), bits)
+    assert np.array_equal(_np(ko), wk)
+    assert np.array_equal(_np(vo), wv)
+    assert ind.scratch_status(scratch, 1, n, bits) == 0
+
+
+def test_sort_full_32_bit_keys_with_duplicates(gpgmp):
+    from inchman_b200 import individual as ind
+    rng = np.random.default_rng(11)
+    n = 300_000
+    keys = rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    keys[n // 2:] = keys[: n - n // 2]          # many equal keys: stability matters
+    vals = rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    wk, wv = keys.copy(), vals.copy()
+    oracle.orc().orc_sort_pairs_u32(oracle.ptr(wk), oracle.ptr(wv), n)
+    ko, vo, _ = ind.sort_pairs_u32(_t(keys), _t(vals), 32)
+    assert np.array_equal(_np(ko), wk) and np.array_equal(_np(vo), wv)
+
+
+@pytest.mark.parametrize("ncells,n", [(16, 0), (16, 1), (1 << 10, 5000), (1 << 20, 1 << 22)])
+def test_cell_offsets_and_reference_indices(gpgmp, ncells, n):
+    from inchman_b200 import individual as ind
+    rng = np.random.default_rng(ncells)
+    keys = np.sort(rng.integers(0, ncells, size=n).astype(np.uint32))
+    ws, wc = np.zeros(ncells, np.uint32), np.zeros(ncells, np.uint32)
+    oracle.orc().orc_cell_offsets(oracle.ptr(keys), n, ncells, oracle.ptr(ws), oracle.ptr(wc))
+    import torch
+    tk = _t(keys) if n else torch.zeros(1, dtype=torch.int32, device="cuda")
+    s, c = ind.cell_offsets(tk[:n] if n else tk[:0], ncells)
+    assert np.array_equal(_np(s), ws) and np.array_equal(_np(c), wc)
+    if n:
+        wl, wr = np.zeros(ncells, np.uint32), np.zeros(ncells, np.uint32)
+        oracle.orc().orc_cell_indices_ref(oracle.ptr(keys), n, ncells, oracle.ptr(wl), oracle.ptr(wr))
+        left, right = ind.cell_indices(s, c)
+        assert np.array_equal(_np(left), wl) and np.array_equal(_np(right), wr)
+
+
+@pytest.mark.parametrize("n,grid,steps", [(10_000, 64, 5), (200_000, 256, 3), (1 << 22, 1024, 2)])
+def test_particle_steps_bit_exact(gpgmp, n, grid, steps):
+    from inchman_b200 import individual as ind
+    x, y, sp = ind.uniform_particles(n, grid, seed=5)
+    p = ind.Particles(n, grid, D=0.5, vx=0.1, vy=0.0, dt=1.0, p_react=0.05, seed=1234)
+    p.set(x, y, sp, step=0)
+    p.step(steps)
+    gx, gy, gsp = p.get()
+    assert p.status() == 0
+    ox, oy, osp = x.copy(), y.copy(), sp.copy()
+    m = oracle.orc().orc_particles_run(n, oracle.ptr(ox), oracle.ptr(oy), oracle.ptr(osp), grid, 0.5, 0.1, 0.0, 1.0,
+                                       0.05, 1234, 0, steps)
+    assert len(gx) == m
+    assert np.array_equal(gx, ox[:m]) and np.array_equal(gy, oy[:m]) and np.array_equal(gsp, osp[:m])
+    # removals come in A/B pairs
+    assert (np.sum(gsp == 0) - np.sum(gsp == 1)) == (np.sum(sp == 0) - np.sum(sp == 1))
+    assert m < n
