@@ -18,8 +18,11 @@
 // Every look-back spin has an iteration limit; exceeding it sets the error word
 // (GPGMP_ERR_TIMEOUT for the caller) and the kernel continues without waiting.
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "sort_kernels.h"
+#include "host_common.h"
+#include "../../include/gpgmp_c.h"
 
 namespace gpgmp {
 namespace {
@@ -434,3 +437,57 @@ cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t
 }
 
 }  // namespace gpgmp
+
+// ---- exclusive scan without allocation -----------------------------------------
+// For callers that must not call cudaMalloc: the scan's scratch (tile counter,
+// error word, one status word per 4096-value tile) lives in a fixed file-scope
+// device array instead of a caller buffer.  Every device that loads this library
+// holds the array (128 KiB) until the process exits; it serves scans of up to
+// kNoAllocMaxN values.
+namespace gpgmp {
+namespace {
+constexpr int64_t kNoAllocMaxN = (int64_t)1 << 26;
+constexpr size_t kNoAllocWords = 2 + (size_t)(kNoAllocMaxN / kScanTile);
+static __device__ __align__(256) uint64_t g_noalloc_scan_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the array on the current device.  In host code the array's
+// name only stands in for the symbol, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(GPGMP_ERR_UNSUPPORTED, "device %d", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(GPGMP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return GPGMP_OK;
+}
+}  // namespace
+}  // namespace gpgmp
+
+extern "C" int gpgmp_exclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, void* stream) {
+    using namespace gpgmp;
+    if (n < 0 || (n > 0 && (!in || !out))) return set_error(GPGMP_ERR_INVALID, "bad argument");
+    if (n > kNoAllocMaxN)
+        return set_error(GPGMP_ERR_INVALID, "n = %lld exceeds the %lld values the built-in scratch serves",
+                         (long long)n, (long long)kNoAllocMaxN);
+    if (n == 0) return GPGMP_OK;
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // zeroes the counter and the status words this scan uses, then scans
+    cudaError_t e = scan_exclusive_u32(in, out, n, scratch, (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "scan: %s", cudaGetErrorString(e));
+    return GPGMP_OK;
+}

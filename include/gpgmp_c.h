@@ -202,6 +202,17 @@ int gpgmp_cell_offsets(const uint32_t* sorted_keys, int64_t n, int64_t ncells, u
 int gpgmp_cell_indices(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left, uint32_t* right,
                        void* stream);
 int gpgmp_scratch_status(const void* scratch, int32_t kind, int64_t n, int32_t key_bits, int32_t* status);
+/* gpgmp_exclusive_scan_u32 for callers that may not allocate device memory: code
+ * whose device memory is owned and accounted by another allocator (a framework's
+ * memory pool), or that cannot take cudaMalloc's implicit synchronisation or its
+ * failure in the middle of a time loop.  No counterpart in the reference.  The
+ * scratch is a fixed 128 KiB device array inside the library, so n is at most
+ * 2^26 (67,108,864) values; larger n is rejected with GPGMP_ERR_INVALID.  The first
+ * call on each device looks the array up (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  Every call on a device
+ * shares the one array: calls whose kernels overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  Allocates nothing. */
+int gpgmp_exclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, void* stream);
 
 /* ---- individual particles on the lattice: move, bin, react, compact ---------------
  * The reference's individual solver (IndividualSolver.cpp:416-712, 458-671) moves
