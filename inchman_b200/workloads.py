@@ -1,0 +1,128 @@
+"""Benchmark workloads besides the default Gray-Scott line (bench.py --workload ...).
+
+Each returns one JSON-ready dict in bench.py's format.  Inputs are synthetic and
+seeded.  Units:
+  cell-steps/s      lattice cells x realisations x event-loop steps per second
+  particle-steps/s  particles x steps per second
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+METRIC = "cell-steps/s per B200, batched vs plain at same stats; adjoint/forward time ratio"
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _base(args, world, metric_value, unit, workload, cfg, ms_per_step, extra):
+    d = {"metric": METRIC, "value": metric_value, "unit": unit, "n_gpus": world, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+         "config": dict({"workload": workload}, **cfg)}
+    d.update(extra)
+    return d
+
+
+def ssa_plain(args, rank, world):
+    """Homogeneous SSA + diffusion, 32 x 32, A+B<->C, 16 realisations, t = 10:
+    the reference's structure (one solver per realisation, wait after every launch)
+    against one launch per kernel for all 16 realisations."""
+    import torch
+    from .model import plain_ssa_model
+    from .solver import Solver
+    m = plain_ssa_model(width=32, max_time=10.0)
+    R, seed = 16, 1234
+    lam = [100.0, 100.0, 0.0]
+
+    def run_plain():
+        steps = 0
+        for r in range(R):
+            with Solver(m, realisations=1, seed=seed + r, sync_each_launch=True) as s:
+                s.init_poisson(lam)
+                _, _, n = s.solve(count_only=True)
+                steps += n
+        return steps
+
+    def run_wide():
+        with Solver(m, realisations=R, seed=seed) as s:
+            s.init_poisson(lam)
+            _, _, n = s.solve(count_only=True)
+        return n * R
+
+    res = {}
+    for name, fn in (("plain", run_plain), ("wide", run_wide)):
+        for _ in range(1):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        res[name] = (m.area * steps / t, t)
+    return _base(args, world, res["wide"][0], "cell-steps/s", "ssa_homogeneous_32x32_ABC_16real_t10",
+                 {"grid": [32, 32], "realisations": R, "t_end": 10.0}, res["wide"][1] * 1e3,
+                 {"plain": {"value": res["plain"][0], "seconds": res["plain"][1]},
+                  "wide_over_plain": res["wide"][0] / res["plain"][0]})
+
+
+def lotka_volterra(args, rank, world):
+    """Inhomogeneous drift-diffusion SSA, 512 x 512, Lotka-Volterra, lognormal D,
+    sinusoidal drift, 256 realisations; timed over t in [0, t_sample]."""
+    import torch
+    from .model import lotka_volterra_model
+    from .solver import Solver
+    t_sample = float(getattr(args, "t_sample", 0.5))
+    m = lotka_volterra_model(width=512, max_time=t_sample)
+    R = 256
+    with Solver(m, realisations=R, seed=1234) as s:
+        s.init_poisson([50.0, 50.0])
+        torch.cuda.synchronize()
+        a, b = _events()
+        a.record()
+        _, _, steps = s.solve(count_only=True)
+        b.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / 1e3
+        st = s.status()
+    cs = m.area * R * steps
+    return _base(args, world, cs / t, "cell-steps/s", "lotka_volterra_512x512_256real",
+                 {"grid": [512, 512], "realisations": R, "t_sample": t_sample, "steps": steps},
+                 t / max(steps, 1) * 1e3, {"status_nonzero": int((st != 0).sum())})
+
+
+def particles(args, rank, world):
+    """2^22 particles on 1024 x 1024 cells: Brownian step (D = 0.5, drift (0.1, 0)),
+    radix-sort binning + exclusive scan, in-cell A+B->0 (p = 0.05); K steps timed."""
+    import torch
+    from .individual import Particles, uniform_particles
+    n, G = 1 << 22, 1024
+    x, y, sp = uniform_particles(n, G, seed=1234)
+    p = Particles(n, G, D=0.5, vx=0.1, vy=0.0, dt=1.0, p_react=0.05, seed=1234)
+    p.set(x, y, sp, step=0)
+    p.step(args.warmup)
+    torch.cuda.synchronize()
+    a, b = _events()
+    x0, _, _ = p.get()
+    n0 = len(x0)
+    a.record()
+    p.step(args.steps)
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    x1, _, _ = p.get()
+    ps = (n0 + len(x1)) / 2 * args.steps
+    return _base(args, world, ps / t, "particle-steps/s", "particles_2^22_1024x1024",
+                 {"particles": n, "grid": [G, G], "steps_timed": args.steps}, t / args.steps * 1e3,
+                 {"particles_left": len(x1), "dtype": "f32+u32"})
+
+
+def run(args, rank, world):
+    table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles}
+    if args.workload not in table:
+        raise SystemExit(f"unknown workload {args.workload}; one of gray_scott, {', '.join(table)}")
+    return table[args.workload](args, rank, world)

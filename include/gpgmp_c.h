@@ -239,6 +239,49 @@ int gpgmp_particles_bins(gpgmp_particles* h, uint32_t* start, uint32_t* count, u
                          uint32_t* sorted_index, int64_t* n_binned);
 int gpgmp_particles_status(gpgmp_particles* h, int32_t* status);
 
+/* ---- batched ensembles: one persistent kernel for many independent instances ------
+ * Replaces running the reference's solver once per model or realisation
+ * (DiffusionModel.cpp:513-532 rebuilds and reruns everything per run; every launch
+ * waits, Kernel.h:252-253).  Each instance is a homogeneous stochastic model (square
+ * lattice, own species, mass-action network, diffusion constants, p0, end time,
+ * reflecting or absorbing walls; no source walls) whose event loop runs on the device;
+ * a CTA takes instances from a queue ordered by estimated cost.  An instance gives the
+ * same bits as a gpgmp_solver of the same model with seed = instance seed and
+ * realisation index = instance realisation. */
+typedef struct gpgmp_instance {
+    int32_t width;              /* square lattice side */
+    int32_t num_species, num_reactions;
+    int32_t species_offset;     /* first entry of the instance in the diffusion (and lambda) array */
+    int32_t reaction_offset;    /* first entry in the reaction array */
+    int32_t boundary_mask[4];
+    float   physical_length, p0, max_time, output_interval;
+    int32_t max_steps;          /* < 0: unlimited */
+    int32_t flags;              /* GPGMP_FLAG_STOP_ON_ERROR */
+    uint32_t seed, realisation; /* random stream key */
+    int32_t max_snapshots;
+    int32_t reserved;
+    int64_t state_offset;       /* first int32 of the instance's [S][W][W] counts in the state array */
+    int64_t snapshot_offset;    /* first int32 of its snapshots, or -1 for none */
+} gpgmp_instance;
+
+typedef struct gpgmp_ensemble gpgmp_ensemble;
+/* lambda (optional, aligned with diffusion): Poisson mean of the initial counts */
+int gpgmp_ensemble_create(const gpgmp_instance* instances, int32_t n, const float* diffusion, int64_t n_diffusion,
+                          const float* lambda, const gpgmp_reaction* reactions, int64_t n_reactions,
+                          gpgmp_ensemble** out);
+int gpgmp_ensemble_destroy(gpgmp_ensemble* h);
+/* launch shape of the persistent kernel (threads 128/256/512, CTAs per SM) */
+int gpgmp_ensemble_configure(gpgmp_ensemble* h, int32_t threads_per_cta, int32_t ctas_per_sm);
+int gpgmp_ensemble_launch_shape(gpgmp_ensemble* h, int32_t* threads, int32_t* ctas_per_sm, int32_t* grid);
+/* device state: Poisson(lambda) initial counts for every instance */
+int gpgmp_ensemble_init_poisson(gpgmp_ensemble* h, int32_t* state, void* stream);
+/* runs every instance to its end time (device state in place, device snapshots
+ * optional); captured as a CUDA graph on first use, replayed afterwards */
+int gpgmp_ensemble_run(gpgmp_ensemble* h, int32_t* state, int32_t* snapshots, void* stream);
+/* waits for the device; per-instance status bits and event-loop steps; snapshot
+ * times of the instances with snapshots, concatenated */
+int gpgmp_ensemble_results(gpgmp_ensemble* h, int32_t* status, int64_t* steps, float* snapshot_times);
+
 #ifdef __cplusplus
 }
 #endif
