@@ -36,6 +36,7 @@ struct Ctrl {
 struct EnsArgs {
     const gpgmp_instance* inst;
     const int32_t* order;
+    int max_reactions;
     const float* diffusion;
     const gpgmp_reaction* reactions;
     int32_t* state;
@@ -59,7 +60,9 @@ __global__ void k_ensemble(EnsArgs A) {
     __shared__ int s_item;
     const int NT = blockDim.x;
     gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
-    int* xs = reinterpret_cast<int*>(smem + sizeof(gpgmp_reaction) * MAX_REACTIONS);
+    uint32_t* deps = reinterpret_cast<uint32_t*>(smem + sizeof(gpgmp_reaction) * MAX_REACTIONS);
+    int* xs = reinterpret_cast<int*>(deps + 4 * MAX_REACTIONS);
+    float* hs = reinterpret_cast<float*>(xs + (size_t)A.max_species * NT);
     int32_t* lost = A.lost + (int64_t)blockIdx.x * A.lost_stride;
     for (;;) {
         if (threadIdx.x == 0) s_item = (int)atomicAdd(A.queue, 1u);
@@ -71,6 +74,8 @@ __global__ void k_ensemble(EnsArgs A) {
         __syncthreads();
         const int W = s_inst.width, area = W * W, S = s_inst.num_species, R = s_inst.num_reactions;
         for (int i = threadIdx.x; i < R; i += NT) rt[i] = A.reactions[s_inst.reaction_offset + i];
+        __syncthreads();
+        build_deps(rt, R, deps);
         int32_t* st = A.state + s_inst.state_offset;
         const uint32_t key0 = s_inst.seed, key1 = s_inst.realisation;
         const int bm[4] = {s_inst.boundary_mask[0], s_inst.boundary_mask[1], s_inst.boundary_mask[2],
@@ -137,7 +142,8 @@ __global__ void k_ensemble(EnsArgs A) {
                     for (int s = 0; s < S; ++s) x[s * NT] = st[(int64_t)s * area + cell];
                     Stream rs;
                     rs.init(key0, key1, sd, (uint32_t)cell, PH_SSA);
-                    err |= ssa_cell(rt, R, x, NT, rs, c.window);
+                    err |= R > 6 ? ssa_cell_inc(rt, deps, R, x, NT, hs + threadIdx.x, rs, c.window)
+                                 : ssa_cell(rt, R, x, NT, rs, c.window);
                     for (int s = 0; s < S; ++s) st[(int64_t)s * area + cell] = x[s * NT];
                 }
                 if (err) atomicOr(&A.status[id], err);
@@ -209,7 +215,7 @@ __global__ void k_ensemble_init(const gpgmp_instance* inst, int n_inst, const fl
 
 struct gpgmp_ensemble {
     int n = 0;
-    int max_species = 0, max_area = 0;
+    int max_species = 0, max_area = 0, max_reactions = 0;
     std::vector<gpgmp_instance> inst;
     gpgmp_instance* d_inst = nullptr;
     int32_t* d_order = nullptr;
@@ -260,10 +266,11 @@ double est_cost(const gpgmp_instance& I, const float* diffusion) {
 }
 
 int configure(gpgmp_ensemble* h, int threads, int ctas_per_sm) {
-    if (threads != 128 && threads != 256 && threads != 512)
-        return set_error(GPGMP_ERR_INVALID, "threads per CTA must be 128, 256 or 512");
+    if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+        return set_error(GPGMP_ERR_INVALID, "threads per CTA must be 128, 256, 512 or 1024");
     h->threads = threads;
-    h->smem = sizeof(gpgmp_reaction) * MAX_REACTIONS + sizeof(int) * (size_t)h->max_species * threads;
+    h->smem = sizeof(gpgmp_reaction) * MAX_REACTIONS + sizeof(uint32_t) * 4 * MAX_REACTIONS +
+              sizeof(int) * (size_t)h->max_species * threads + sizeof(float) * (size_t)h->max_reactions * threads;
     CK(cudaFuncSetAttribute(k_ensemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem));
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
@@ -320,6 +327,7 @@ int gpgmp_ensemble_create(const gpgmp_instance* instances, int32_t n, const floa
             }
         }
         h->max_species = std::max(h->max_species, I.num_species);
+        h->max_reactions = std::max(h->max_reactions, I.num_reactions);
         h->max_area = std::max(h->max_area, I.width * I.width);
         if (I.snapshot_offset >= 0 && I.max_snapshots > 0) {
             snap_off[i] = snap_total;
@@ -406,6 +414,7 @@ int gpgmp_ensemble_run(gpgmp_ensemble* h, int32_t* state, int32_t* snapshots, vo
         a.snap_time_off = h->d_snap_time_off; a.status = h->d_status; a.steps = h->d_steps;
         a.lost = h->d_lost; a.lost_stride = 4 * (int64_t)h->max_area; a.queue = h->d_queue; a.n_inst = h->n;
         a.max_species = h->max_species;
+        a.max_reactions = h->max_reactions;
         cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaMemsetAsync(h->d_queue, 0, sizeof(unsigned int), cap);

@@ -64,6 +64,75 @@ __device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x,
     }
 }
 
+
+// Dependency masks of the incremental SSA: bit q of deps[j * 4 + q / 32] is set when
+// reaction j changes the count of a species that reaction q consumes, i.e. when q's
+// hazard must be recomputed after j fires (Gibson & Bruck's dependency graph).  Built
+// by all threads of a block; R <= 128.
+__device__ __forceinline__ void build_deps(const gpgmp_reaction* rt, int R, uint32_t* deps) {
+    for (int idx = threadIdx.x; idx < R * 4; idx += blockDim.x) deps[idx] = 0u;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < R * R; idx += blockDim.x) {
+        const int j = idx / R, q = idx % R;
+        const gpgmp_reaction& a = rt[j];
+        const gpgmp_reaction& b = rt[q];
+        bool dep = false;
+        for (int u = 0; u < b.num_reactants && !dep; ++u) {
+            const int sp = b.reactant_species[u];
+            int net = 0;
+            for (int v = 0; v < a.num_reactants; ++v) if (a.reactant_species[v] == sp) net -= a.reactant_stoich[v];
+            for (int v = 0; v < a.num_products; ++v) if (a.product_species[v] == sp) net += a.product_stoich[v];
+            dep = net != 0;
+        }
+        if (dep) atomicOr(&deps[j * 4 + (q >> 5)], 1u << (q & 31));
+    }
+    __syncthreads();
+}
+
+// The same SSA window as ssa_cell with per-reaction hazards kept in h[r * stride]
+// and recomputed only where the fired reaction changed a reactant count.  The total
+// and the selection sum the same values in the same order as the full recomputation,
+// so the result is bit-identical.
+__device__ __forceinline__ int ssa_cell_inc(const gpgmp_reaction* rt, const uint32_t* deps, int R, int* x, int stride,
+                                            float* h, Stream& st, float window) {
+    for (int r = 0; r < R; ++r) h[r * stride] = hazard(rt[r], x, stride);
+    float t = 0.0f;
+    int events = 0;
+    for (;;) {
+        float h0 = 0.0f;
+        for (int r = 0; r < R; ++r) h0 = h0 + h[r * stride];
+        if (!(h0 > 0.0f)) return 0;
+        const uint32_t a = st.next(), b = st.next();
+        const float r1 = u01_open0(a);
+        const float r2 = u01(b) * h0;
+        const float dtev = -gp_logf(r1) / h0;
+        t = t + dtev;
+        if (!(t < window)) return 0;
+        int j = -1;
+        float hc = 0.0f;
+        for (int r = 0; r < R; ++r) {
+            hc = hc + h[r * stride];
+            if (r2 < hc) { j = r; break; }
+        }
+        if (j >= 0) {
+            const gpgmp_reaction& rc = rt[j];
+            for (int q = 0; q < rc.num_products; ++q)
+                if (x[rc.product_species[q] * stride] > INT32_MAX - rc.product_stoich[q]) return SIM_OVERFLOW;
+            for (int q = 0; q < rc.num_reactants; ++q) x[rc.reactant_species[q] * stride] -= rc.reactant_stoich[q];
+            for (int q = 0; q < rc.num_products; ++q) x[rc.product_species[q] * stride] += rc.product_stoich[q];
+            for (int w = 0; w * 32 < R; ++w) {
+                uint32_t m = deps[j * 4 + w];
+                while (m) {
+                    const int q = w * 32 + __ffs(m) - 1;
+                    m &= m - 1;
+                    h[q * stride] = hazard(rt[q], x, stride);
+                }
+            }
+        }
+        if (++events >= SSA_EVENT_CAP) return SIM_EVENT_CAP;
+    }
+}
+
 // Four lost counts (-x, +x, -y, +y) of one cell of n particles.
 __device__ __forceinline__ void homog_lost(int n, float pmove, Stream& st, int x, int y, int W, int H,
                                            const int* bmask, int l[4]) {

@@ -13,6 +13,7 @@ namespace gpgmp {
 namespace {
 
 constexpr int kSsaThreads = 128;
+constexpr int kIncMinReactions = 6;   // networks above this size keep per-reaction hazards
 constexpr int TW = 32, TH = 16, NT = 256;
 
 __global__ void k_init_poisson(Planes planes, int S, int area, int R, uint32_t seed, const float* __restrict__ lam) {
@@ -32,11 +33,14 @@ __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int a
                                                      const gpgmp_reaction* __restrict__ reactions, int nreac,
                                                      uint32_t seed, uint32_t step_seed, float window,
                                                      int32_t* __restrict__ status) {
-    extern __shared__ unsigned char smem[];
+    extern __shared__ __align__(16) unsigned char smem[];
     gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
-    int* xs = reinterpret_cast<int*>(smem + sizeof(gpgmp_reaction) * nreac);
+    uint32_t* deps = reinterpret_cast<uint32_t*>(smem + sizeof(gpgmp_reaction) * nreac);
+    float* hs = reinterpret_cast<float*>(deps + 4 * nreac);
+    int* xs = reinterpret_cast<int*>(hs + (size_t)nreac * kSsaThreads);
     for (int i = threadIdx.x; i < nreac; i += blockDim.x) rt[i] = reactions[i];
     __syncthreads();
+    build_deps(rt, nreac, deps);
     const int64_t total = (int64_t)R * area;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -46,7 +50,9 @@ __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int a
     for (int s = 0; s < S; ++s) x[s * kSsaThreads] = planes.p[s][((int64_t)r * S + s) * area + c];
     Stream st;
     st.init(seed, (uint32_t)r, step_seed, (uint32_t)c, PH_SSA);
-    const int e = ssa_cell(rt, nreac, x, kSsaThreads, st, window);
+    // both forms give the same bits; the incremental one pays off for larger networks
+    const int e = nreac > kIncMinReactions ? ssa_cell_inc(rt, deps, nreac, x, kSsaThreads, hs + threadIdx.x, st, window)
+                                           : ssa_cell(rt, nreac, x, kSsaThreads, st, window);
     for (int s = 0; s < S; ++s) planes.p[s][((int64_t)r * S + s) * area + c] = x[s * kSsaThreads];
     if (e) atomicOr(&status[r], e);
 }
@@ -277,7 +283,8 @@ cudaError_t launch_ssa(const GridDesc& g, Planes planes, const gpgmp_reaction* d
     if (nreac <= 0) return cudaSuccess;
     const int area = g.W * g.H;
     const int64_t total = (int64_t)g.R * area;
-    const size_t smem = sizeof(gpgmp_reaction) * nreac + sizeof(int) * g.S * kSsaThreads;
+    const size_t smem = sizeof(gpgmp_reaction) * nreac + sizeof(uint32_t) * 4 * nreac +
+                        sizeof(float) * (size_t)nreac * kSsaThreads + sizeof(int) * g.S * kSsaThreads;
     const unsigned blocks = (unsigned)((total + kSsaThreads - 1) / kSsaThreads);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_ssa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -233,7 +233,7 @@ def random_ensemble(n: int, seed: int, max_time: float = 5.0) -> List[InstanceSp
 # ---------------------------------------------------------------------------------
 
 TUNE_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_tune")
-CANDIDATES = [(128, 4), (128, 8), (256, 2), (256, 4), (512, 1), (512, 2)]
+CANDIDATES = [(256, 2), (256, 4), (512, 1), (512, 2), (1024, 1)]
 
 
 def _signature(specs: List[InstanceSpec]) -> str:

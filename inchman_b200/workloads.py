@@ -54,8 +54,21 @@ def ssa_plain(args, rank, world):
             _, _, n = s.solve(count_only=True)
         return n * R
 
+    from .ensemble import Ensemble, autotune, replicate
+    specs = replicate(m, lam, R, seed)
+    (thr, cps), _ = autotune(specs)
+    ens = Ensemble(specs)
+    ens.configure(thr, cps)
+    est = ens.alloc_state()
+
+    def run_batched():
+        ens.init_poisson(est)
+        ens.run(est)
+        _, st, _ = ens.results()
+        return int(st.sum())
+
     res = {}
-    for name, fn in (("plain", run_plain), ("wide", run_wide)):
+    for name, fn in (("plain", run_plain), ("wide", run_wide), ("batched", run_batched)):
         for _ in range(1):
             fn()
         torch.cuda.synchronize()
@@ -64,10 +77,62 @@ def ssa_plain(args, rank, world):
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
         res[name] = (m.area * steps / t, t)
-    return _base(args, world, res["wide"][0], "cell-steps/s", "ssa_homogeneous_32x32_ABC_16real_t10",
-                 {"grid": [32, 32], "realisations": R, "t_end": 10.0}, res["wide"][1] * 1e3,
+    return _base(args, world, res["batched"][0], "cell-steps/s", "ssa_homogeneous_32x32_ABC_16real_t10",
+                 {"grid": [32, 32], "realisations": R, "t_end": 10.0}, res["batched"][1] * 1e3,
                  {"plain": {"value": res["plain"][0], "seconds": res["plain"][1]},
+                  "wide": {"value": res["wide"][0], "seconds": res["wide"][1]},
+                  "batched_over_plain": res["batched"][0] / res["plain"][0],
                   "wide_over_plain": res["wide"][0] / res["plain"][0]})
+
+
+def ensemble(args, rank, world):
+    """4096 random heterogeneous instances (side 16..128, 4..12 species, 8..32
+    reactions), t = 5, in one persistent kernel (launch shape from the autotuner),
+    against the reference's structure -- one solver per instance, a wait after every
+    launch -- timed on a sample of the instances and compared per cell-step."""
+    import torch
+    from .ensemble import Ensemble, autotune, random_ensemble
+    from .solver import Solver
+    n = int(getattr(args, "instances", 4096))
+    specs = random_ensemble(n, seed=2024, max_time=5.0)
+    (thr, cps), tune = autotune(specs)
+    ens = Ensemble(specs)
+    ens.configure(thr, cps)
+    state = ens.alloc_state()
+    ens.init_poisson(state)
+    ens.run(state)                    # capture + warm-up
+    torch.cuda.synchronize()
+    ens.init_poisson(state)
+    a, b = _events()
+    a.record()
+    ens.run(state)
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    status, steps, _ = ens.results()
+    cs = ens.cell_steps(steps)
+    batched = cs / t
+    # plain: the reference's structure on a sample of the instances
+    k = int(getattr(args, "plain_sample", 24))
+    pick = np.random.default_rng(1).choice(n, size=k, replace=False)
+    pcs, pt = 0, 0.0
+    for i in pick:
+        sp = specs[int(i)]
+        with Solver(sp.model, realisations=1, seed=sp.seed, sync_each_launch=True) as s:
+            s.init_poisson(sp.lam)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, _, nsteps = s.solve(count_only=True)
+            torch.cuda.synchronize()
+            pt += time.perf_counter() - t0
+            pcs += sp.model.area * nsteps
+    plain = pcs / pt
+    return _base(args, world, batched, "cell-steps/s", "ensemble_4096_random_instances_t5",
+                 {"instances": n, "launch": {"threads": thr, "ctas_per_sm": cps}, "autotune_ms": tune.get("ms")},
+                 t * 1e3,
+                 {"plain": {"value": plain, "sample_instances": k, "seconds": pt},
+                  "batched_over_plain": batched / plain, "instances_with_status": int((status != 0).sum()),
+                  "cell_steps": cs})
 
 
 def lotka_volterra(args, rank, world):
@@ -122,7 +187,8 @@ def particles(args, rank, world):
 
 
 def run(args, rank, world):
-    table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles}
+    table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles,
+             "ensemble": ensemble}
     if args.workload not in table:
         raise SystemExit(f"unknown workload {args.workload}; one of gray_scott, {', '.join(table)}")
     return table[args.workload](args, rank, world)

@@ -270,7 +270,7 @@ int gpgmp_ensemble_create(const gpgmp_instance* instances, int32_t n, const floa
                           const float* lambda, const gpgmp_reaction* reactions, int64_t n_reactions,
                           gpgmp_ensemble** out);
 int gpgmp_ensemble_destroy(gpgmp_ensemble* h);
-/* launch shape of the persistent kernel (threads 128/256/512, CTAs per SM) */
+/* launch shape of the persistent kernel (threads 128/256/512/1024, CTAs per SM) */
 int gpgmp_ensemble_configure(gpgmp_ensemble* h, int32_t threads_per_cta, int32_t ctas_per_sm);
 int gpgmp_ensemble_launch_shape(gpgmp_ensemble* h, int32_t* threads, int32_t* ctas_per_sm, int32_t* grid);
 /* device state: Poisson(lambda) initial counts for every instance */
