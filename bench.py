@@ -303,6 +303,9 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gray_scott")
+    ap.add_argument("--instances", type=int, default=4096, help="ensemble workload: number of instances")
+    ap.add_argument("--plain-sample", type=int, default=24, help="ensemble workload: instances timed plain")
+    ap.add_argument("--t-sample", type=float, default=0.5, help="lotka_volterra workload: simulated time")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3) if args.impl != "reference" else args.warmup
     rank, world, local = dist_setup(args)

@@ -94,6 +94,7 @@ def ensemble(args, rank, world):
     from .ensemble import Ensemble, autotune, random_ensemble
     from .solver import Solver
     n = int(getattr(args, "instances", 4096))
+    n = max(1, n)
     specs = random_ensemble(n, seed=2024, max_time=5.0)
     (thr, cps), tune = autotune(specs)
     ens = Ensemble(specs)
