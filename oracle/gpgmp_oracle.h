@@ -78,6 +78,7 @@ void orc_ref_det_diffuse(const orc_model* m, const float* in, float* out, float 
 void orc_ref_rk4(const orc_model* m, float* state, float deltat);
 int orc_ref_solve(const orc_model* m, int32_t* state, uint32_t seed_base,
                   int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots, int64_t* steps);
+void orc_ref_solve_many(const orc_model* m, const int32_t* init, int R, uint32_t seed_base, int32_t* finals);
 
 /* ---- replay of the CUDA algorithms --------------------------------------------- */
 void orc_rep_init_poisson(int W, int H, int S, int R, uint32_t seed, const float* lambda_per_species, int32_t* state);

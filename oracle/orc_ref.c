@@ -447,3 +447,21 @@ int orc_ref_solve(const orc_model* m, int32_t* state, uint32_t seed_base,
     free(dtv); free(next); free(lost);
     return 0;
 }
+
+/* R independent reference-exact runs from the same initial state (OpenMP over the
+ * runs, seed base seed_base + r); final states only.  For statistical comparisons. */
+#include <omp.h>
+void orc_ref_solve_many(const orc_model* m, const int32_t* init, int R, uint32_t seed_base, int32_t* finals) {
+    const size_t block = (size_t)m->num_species * m->width * m->height;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < R; ++r) {
+        int32_t* st = finals + (size_t)r * block;
+        memcpy(st, init, sizeof(int32_t) * block);
+        int32_t* snaps = (int32_t*)malloc(sizeof(int32_t) * block);
+        float t;
+        int ns;
+        int64_t steps;
+        orc_ref_solve(m, st, seed_base + (uint32_t)r * 7919u, snaps, &t, 1, &ns, &steps);
+        free(snaps);
+    }
+}
