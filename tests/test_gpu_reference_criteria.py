@@ -94,3 +94,47 @@ def test_statistics_match_reference_exact_restatement_1e4_realisations(gpgmp):
     assert (ok | ((f > lo) & (f < hi))).all()
     pmin = min(stats.ks_2samp(gpu[:, j], ref[:, j]).pvalue for j in range(k))
     assert pmin > alpha, pmin
+
+
+def test_homogeneous_drift_diffusion(gpgmp):
+    """doc/examples/HomogeneousDrift.xml: inhomogeneous solver, 512 x 512, L = 32,
+    Dx = 0.6, Dy = 0.8, drift (0.8, 0.4), 1e5 molecules in cell (256, 256), t = 5,
+    10 runs.  Pass: RMSE of the mean final density against the drifted 2-D Gaussian
+    <= 1e-4 (python/gpgmp/test/homogeneous_drift_diffusion.py:27, 117, 140).  The
+    drift moves the centre by (4, 2); the test also checks that mean position."""
+    from inchman_b200 import _lib
+    from inchman_b200.model import DiffusionModel
+    from inchman_b200.solver import Solver
+    nx, L, N, T, runs = 512, 32.0, 100_000, 5.0, 10
+    m = DiffusionModel(width=nx, height=nx, physical_length=L, p0=0.1, max_time=T, output_interval=1.0,
+                       solver=_lib.STOCHASTIC_INHOMOGENEOUS, drift_method=_lib.DRIFT_HOMOGENEOUS,
+                       drift_params=(0.6, 0.8, 0.8, 0.4, 0, 0, 0, 0))
+    m.add_species("A", 1.0)
+    init = np.zeros((runs, 1, nx, nx), np.int32)
+    init[:, 0, 256, 256] = N
+    with Solver(m, realisations=runs, seed=3) as s:
+        s.set_state(init)
+        snaps, times, steps = s.solve(max_snapshots=8)
+    sample_t = float(times[-1])                 # the last output, as the reference samples it
+    final = snaps[-1][:, 0].astype(np.float64)
+    dx = L / nx
+    xc = np.arange(nx) * dx - L / 2.0
+    nstate = final.mean(axis=0)
+
+    def biased(xc, yc, t, dxc, dyc, qx, qy):
+        gx = np.outer(xc, np.ones_like(xc))
+        gy = np.outer(np.ones_like(yc), yc)
+        px = 1.0 / np.sqrt(4.0 * dxc * np.pi * t) * np.exp(-((gx - t * qx) ** 2) / (4.0 * dxc * t))
+        py = 1.0 / np.sqrt(4.0 * dyc * np.pi * t) * np.exp(-((gy - t * qy) ** 2) / (4.0 * dyc * t))
+        return px * py
+
+    # first array axis is y (D = 0.8, drift 0.4), second is x (D = 0.6, drift 0.8),
+    # the argument order of the reference's call
+    theo = biased(xc, xc, sample_t, 0.8, 0.6, 0.4, 0.8) * dx * dx
+    rmse = np.sqrt(np.sum((nstate / nstate.sum() - theo) ** 2) / nx / nx)
+    assert rmse <= 1e-4, rmse
+    w = nstate / nstate.sum()
+    mx = (w.sum(axis=0) * xc).sum()
+    my = (w.sum(axis=1) * xc).sum()
+    assert abs(mx - 0.8 * sample_t) < 0.05 and abs(my - 0.4 * sample_t) < 0.05, (mx, my)
+    assert (nstate.sum() == N) and sample_t >= T - 1.0
