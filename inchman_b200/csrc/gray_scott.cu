@@ -522,6 +522,24 @@ __global__ void __launch_bounds__(512, 1) k_gs_adjoint_cw(GSArgs<T> a, const T* 
 }
 
 #include "gs_f32x2.cuh"
+#include "gs_rr.cuh"
+
+// register-resident forward kernel for an n x n float32 lattice with *wpc warps per
+// CTA (*wpc = 0: the default split, written back), or NULL where the lattice does
+// not fit it
+const void* rr_kernel(int n, int* wpc, bool drift, size_t* smem) {
+#define GS_RR_CASE(N_, W_)                                                                        \
+    if (n == N_ && *wpc == W_) {                                                                  \
+        *smem = RRShape<N_, W_>::kSmem;                                                           \
+        return drift ? (const void*)k_gs_forward_rr<N_, W_, 1> : (const void*)k_gs_forward_rr<N_, W_, 0>; \
+    }
+    if (*wpc == 0) *wpc = n == 256 ? 8 : n == 128 ? 4 : 2;
+    GS_RR_CASE(64, 1) GS_RR_CASE(64, 2) GS_RR_CASE(64, 4)
+    GS_RR_CASE(128, 2) GS_RR_CASE(128, 4) GS_RR_CASE(128, 8)
+    GS_RR_CASE(256, 4) GS_RR_CASE(256, 8) GS_RR_CASE(256, 16)
+#undef GS_RR_CASE
+    return nullptr;
+}
 
 template <typename T>
 const void* fwd_kernel(int n) {
@@ -638,9 +656,16 @@ cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, 
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     int every = trace_every > 0 ? trace_every : 1;
     void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every};
+    if (sizeof(T) == 4 && cl == kRRCluster && (p.variant == 0 || p.variant == 3 || p.variant > 10)) {
+        size_t smem = 0;
+        int wpc = p.variant > 10 ? p.variant - 10 : 0;
+        const void* rk = rr_kernel(p.n, &wpc, p.vx != 0.0 || p.vy != 0.0, &smem);
+        if (rk) return launch_cluster<T>(rk, p.n, cl, smem, st, args, dim3(32 * wpc, 1, 1));
+        if (p.variant != 0) return cudaErrorInvalidValue;
+    }
     const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl);
     const void* fk = fwd_kernel<T>(p.n);
-    if (blk.x != 0 && fk && !p.generic) return launch_cluster<T>(fk, p.n, cl, smem_bytes<T>(p.n, cl), st, args, blk);
+    if (blk.x != 0 && fk && p.variant != 1) return launch_cluster<T>(fk, p.n, cl, smem_bytes<T>(p.n, cl), st, args, blk);
     return launch_cluster<T>((const void*)k_gs_forward<T>, p.n, cl, smem_bytes<T>(p.n, cl), st, args);
 }
 
@@ -655,8 +680,21 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     const void* ak = adj_kernel<T>(p.n);
     // the packed float32 adjoint also holds two state buffers in shared memory
     const size_t smem = smem_bytes<T>(p.n, cl) * (sizeof(T) == 4 ? 2 : 1);
-    if (blk.x != 0 && ak && !p.generic) return launch_cluster<T>(ak, p.n, cl, smem, st, args, blk);
+    if (blk.x != 0 && ak && p.variant != 1) return launch_cluster<T>(ak, p.n, cl, smem, st, args, blk);
     return launch_cluster<T>((const void*)k_gs_adjoint<T>, p.n, cl, smem_bytes<T>(p.n, cl), st, args);
+}
+
+cudaError_t gs_forward_status(int* out, bool clear) {
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_gs_fwd_err, sizeof(int));
+    if (e != cudaSuccess) return e;
+    if (clear && v) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_gs_fwd_err, &zero, sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
+    *out = v;
+    return cudaSuccess;
 }
 
 template cudaError_t gs_forward<float>(const GSParams&, const float*, const float*, float*, float*, float*, int,

@@ -40,7 +40,7 @@ GSParams to_params(const gpgmp_gs_params* p) {
     g.n = p->n; g.steps = p->steps;
     g.F = p->F; g.k = p->k; g.Du = p->Du; g.Dv = p->Dv; g.vx = p->vx; g.vy = p->vy; g.dt = p->dt;
     g.cluster = p->cluster;
-    g.generic = p->variant == 1;
+    g.variant = p->variant;
     return g;
 }
 
@@ -132,6 +132,15 @@ int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* ck, const doubl
     return adjoint<double>(p, ck, lu, lv, gu, gv, grad6, work, stream);
 }
 
+int gpgmp_gs_status(int32_t* flags) {
+    if (!flags) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    CK(cudaDeviceSynchronize());
+    int v = 0;
+    CK(gs_forward_status(&v, true));
+    *flags = v;
+    return GPGMP_OK;
+}
+
 int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v) {
     int rc = check(p, 4);
     if (rc) return rc;
@@ -149,6 +158,11 @@ int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float
     }
     CK(cudaFreeAsync(d, st));
     CK(cudaStreamSynchronize(st));
+    if (rc == GPGMP_OK) {
+        int bad = 0;
+        CK(gs_forward_status(&bad, true));
+        if (bad) return set_error(GPGMP_ERR_TIMEOUT, "a bounded halo wait in the forward solve gave up");
+    }
     return rc;
 }
 
@@ -196,6 +210,8 @@ int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const flo
     CK(cudaFreeAsync(dg, st));
     CK(cudaStreamSynchronize(st));
     if (err) return set_error(GPGMP_ERR_TIMEOUT, "a bounded wait for a TMA copy in the adjoint gave up");
+    CK(gs_forward_status(&err, true));
+    if (err) return set_error(GPGMP_ERR_TIMEOUT, "a bounded halo wait in the forward solve gave up");
     *loss = L;
     return GPGMP_OK;
 }

@@ -38,23 +38,33 @@ struct GSCoef2 {
     }
 };
 
-// forward update of the pair C = (x, x+1), L = (x-1, x), R = (x+1, x+2)
-__device__ __forceinline__ void gs_update2(const GSCoef2& k, float2 uU, float2 uC, float2 uD, float uLs, float uRs,
-                                           float2 vU, float2 vC, float2 vD, float vLs, float vRs, float2* un,
-                                           float2* vn) {
-    const float2 uL = make_float2(uLs, uC.x), uR = make_float2(uC.y, uRs);
-    const float2 vL = make_float2(vLs, vC.x), vR = make_float2(vC.y, vRs);
+// forward update of two cells at once: C the cells, L / R / U / D their left,
+// right, upper and lower neighbours (any pairing of cells; the arithmetic per cell
+// is the same as in the scalar kernels' gs_update).  DRIFT: 1 with the drift
+// terms, 0 without, -1 decided by k.drift at run time.
+template <int DRIFT = -1>
+__device__ __forceinline__ void gs_update2f(const GSCoef2& k, float2 uL, float2 uR, float2 uU, float2 uC, float2 uD,
+                                            float2 vL, float2 vR, float2 vU, float2 vC, float2 vD, float2* un,
+                                            float2* vn) {
     const float2 uvv = mul2(uC, mul2(vC, vC));
     const float2 lu = fma2(k.m4, uC, add2(add2(uL, uR), add2(uU, uD)));
     const float2 lv = fma2(k.m4, vC, add2(add2(vL, vR), add2(vU, vD)));
     float2 a = fma2(k.du, lu, fma2(k.mdtF, uC, k.dtF));
     float2 b = fma2(k.mdtFk, vC, mul2(k.dv, lv));
-    if (k.drift) {
+    if (DRIFT == 1 || (DRIFT < 0 && k.drift)) {
         a = fma2(k.hx, sub2(uL, uR), fma2(k.hy, sub2(uU, uD), a));
         b = fma2(k.hx, sub2(vL, vR), fma2(k.hy, sub2(vU, vD), b));
     }
     *un = add2(uC, fma2(k.mdt, uvv, a));
     *vn = add2(vC, fma2(k.dt, uvv, b));
+}
+
+// forward update of the adjacent pair C = (x, x+1), L = (x-1, x), R = (x+1, x+2)
+__device__ __forceinline__ void gs_update2(const GSCoef2& k, float2 uU, float2 uC, float2 uD, float uLs, float uRs,
+                                           float2 vU, float2 vC, float2 vD, float vLs, float vRs, float2* un,
+                                           float2* vn) {
+    gs_update2f(k, make_float2(uLs, uC.x), make_float2(uC.y, uRs), uU, uC, uD, make_float2(vLs, vC.x),
+                make_float2(vC.y, vRs), vU, vC, vD, un, vn);
 }
 
 template <int N>

@@ -9,8 +9,13 @@ struct GSParams {
     int n, steps;
     double F, k, Du, Dv, vx, vy, dt;
     int cluster;   // CTAs per cluster, 0 = 16 where the lattice fits, else the smallest that fits
-    int generic;   // 1: use the one-cell-per-iteration kernels instead of the column walk
+    int variant;   // 0 automatic, 1 one cell per iteration, 2 shared-memory column walk,
+                   // 3 register-resident (float32), 10 + w register-resident with w warps per CTA
 };
+
+// reads (and with clear, resets) the device word that the register-resident forward
+// kernel sets when one of its bounded waits gave up; synchronous
+cudaError_t gs_forward_status(int* out, bool clear);
 
 // cluster size (<= 16) for an n x n lattice of elem_bytes values: 16 when the
 // lattice splits evenly into 16 slabs that fit, else the smallest that fits

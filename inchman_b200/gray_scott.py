@@ -37,6 +37,7 @@ _SIGS = {
     "gpgmp_gs_adjoint_f64": (C.c_int, [C.POINTER(GSParams)] + [C.c_void_p] * 8),
     "gpgmp_gs_forward_host": (C.c_int, [C.POINTER(GSParams)] + [C.c_void_p] * 4),
     "gpgmp_gs_loss_grad_host": (C.c_int, [C.POINTER(GSParams)] + [C.c_void_p] * 6),
+    "gpgmp_gs_status": (C.c_int, [C.POINTER(C.c_int32)]),
 }
 _lib.SIGNATURES.update(_SIGS)
 
@@ -116,6 +117,15 @@ def forward(u0, v0, p: GSParams, checkpoints=None):
     _lib.check(_fn(name)(C.byref(p), C.c_void_p(u0.data_ptr()), C.c_void_p(v0.data_ptr()), C.c_void_p(u.data_ptr()),
                          C.c_void_p(v.data_ptr()), ck, _stream_ptr(torch, u0.device)), name)
     return u, v
+
+
+def status() -> int:
+    """Flags of the forward kernels since the last call (synchronises the device):
+    non-zero if a bounded halo wait inside a register-resident forward solve gave up
+    (that solve's output is NaN).  Clears the flags."""
+    f = C.c_int32(0)
+    _lib.check(_fn("gpgmp_gs_status")(C.byref(f)), "gpgmp_gs_status")
+    return int(f.value)
 
 
 def adjoint(p: GSParams, checkpoints, lam_u, lam_v):

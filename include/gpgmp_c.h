@@ -151,7 +151,11 @@ typedef struct gpgmp_gs_params {
     double  F, k, Du, Dv, vx, vy, dt;
     int32_t checkpoint_every;   /* <= 0: 100 */
     int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
-    int32_t variant;            /* 0: column-walk kernels where the lattice allows, 1: one cell per iteration */
+    int32_t variant;            /* kernel family (float32): 0 automatic = register-resident where
+                                   the lattice allows (n 64, 128, 256 on a 16-CTA cluster), else the
+                                   shared-memory column walk; 1 one cell per iteration; 2 shared-memory
+                                   column walk; 3 register-resident; 10 + w register-resident with w
+                                   warps per CTA.  float64 always uses 0 / 1 (column walk / per cell). */
 } gpgmp_gs_params;
 
 /* bytes of the checkpoint buffer and of the adjoint's work buffer */
@@ -168,6 +172,11 @@ int gpgmp_gs_adjoint_f32(const gpgmp_gs_params* p, const float* checkpoints, con
 int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* checkpoints, const double* lam_u,
                          const double* lam_v, double* grad_u0, double* grad_v0, double* grad6, void* work,
                          void* stream);
+/* Status of the forward kernels on the current device: *flags != 0 if a bounded wait
+ * inside a register-resident forward solve gave up since the last call (that solve's
+ * output is NaN).  Synchronises the device and clears the flags.  No counterpart in
+ * the reference (its kernels have no waits). */
+int gpgmp_gs_status(int32_t* flags);
 /* Host buffers in and out: copies (u0, v0) to the device, runs the forward solve,
  * copies (u, v) back.  Allocates its device buffers from the stream-ordered pool. */
 int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v);

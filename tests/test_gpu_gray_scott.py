@@ -64,6 +64,38 @@ def test_forward_f32_within_1e5_of_f64(gpgmp):
     assert err < 1e-5, err
 
 
+_RR_WARPS = {64: [1, 2, 4], 128: [2, 4, 8], 256: [4, 8, 16]}
+
+
+@pytest.mark.parametrize("n,steps,drift,every", [(64, 0, False, 1), (64, 1, True, 1), (64, 37, True, 5),
+                                                 (128, 2, False, 1), (128, 101, True, 10), (256, 300, False, 100),
+                                                 (256, 301, True, 7)])
+def test_register_resident_forward_bit_exact(gpgmp, n, steps, drift, every):
+    """The register-resident kernel (every warp split) gives the same bits as the
+    shared-memory column-walk kernel: final state and every stored checkpoint."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=n, steps=steps, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0, checkpoint_every=every)
+    u0, v0 = _init(cfg, np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    nck = max(1, -(-steps // every))
+
+    def run(variant):
+        ck = torch.full((nck, 2, n, n), float("nan"), device="cuda")
+        u, v = gs.forward(tu, tv, cfg.params(variant=variant), checkpoints=ck if steps else None)
+        return u, v, ck
+
+    ru, rv, rck = run(2)
+    for var in [0, 3] + [10 + w for w in _RR_WARPS[n]]:
+        u, v, ck = run(var)
+        assert torch.equal(u, ru) and torch.equal(v, rv), var
+        if steps:
+            assert torch.equal(ck, rck), var
+    assert gs.status() == 0
+    if steps == 0:
+        assert torch.equal(ru, tu) and torch.equal(rv, tv)
+
+
 @pytest.mark.parametrize("cluster", [2, 16])
 def test_adjoint_f64_matches_oracle_adjoint(gpgmp, cluster):
     import torch
