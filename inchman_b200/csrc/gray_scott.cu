@@ -541,6 +541,21 @@ const void* rr_kernel(int n, int* wpc, bool drift, size_t* smem) {
     return nullptr;
 }
 
+// register-resident adjoint kernel with wpc warps per CTA
+const void* rr_adj_kernel(int n, int* wpc, bool drift, size_t* smem) {
+#define GS_RRA_CASE(N_, W_)                                                                        \
+    if (n == N_ && *wpc == W_) {                                                                   \
+        *smem = RRAdjShape<N_, W_>::kSmem;                                                         \
+        return drift ? (const void*)k_gs_adjoint_rr<N_, W_, 1> : (const void*)k_gs_adjoint_rr<N_, W_, 0>; \
+    }
+    if (*wpc == 0) *wpc = n == 256 ? 8 : n == 128 ? 4 : 2;
+    GS_RRA_CASE(64, 1) GS_RRA_CASE(64, 2) GS_RRA_CASE(64, 4)
+    GS_RRA_CASE(128, 2) GS_RRA_CASE(128, 4) GS_RRA_CASE(128, 8)
+    GS_RRA_CASE(256, 8)
+#undef GS_RRA_CASE
+    return nullptr;
+}
+
 template <typename T>
 const void* fwd_kernel(int n) {
     if (sizeof(T) == 4) {
@@ -676,6 +691,13 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     if (cl <= 0) return cudaErrorInvalidValue;
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad, &err};
+    if (sizeof(T) == 4 && cl == kRRCluster && (p.variant == 0 || p.variant == 3 || p.variant > 10)) {
+        size_t smem = 0;
+        int wpc = p.variant > 10 ? p.variant - 10 : 0;
+        const void* rk = rr_adj_kernel(p.n, &wpc, p.vx != 0.0 || p.vy != 0.0, &smem);
+        if (rk) return launch_cluster<T>(rk, p.n, cl, smem, st, args, dim3(32 * wpc, 1, 1));
+        if (p.variant != 0) return cudaErrorInvalidValue;
+    }
     const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl, 512);
     const void* ak = adj_kernel<T>(p.n);
     // the packed float32 adjoint also holds two state buffers in shared memory

@@ -2,12 +2,14 @@
 //
 // The adjoint uses two-level checkpointing: the forward pass keeps the state every
 // checkpoint_every steps; the backward pass walks the segments last to first,
-// recomputes the segment's states from its checkpoint into the work buffer
-// (one forward launch), then runs the transposed steps over them (one adjoint
-// launch).  Memory: ceil(steps/c) + c states; time: about two forward solves plus
-// the adjoint steps.
+// recomputes each segment's states from its checkpoint into a work buffer (one
+// forward launch, on a side stream, up to two segments ahead), then runs the
+// transposed steps over them (one adjoint launch on the caller's stream).  Memory:
+// ceil(steps/c) + 2c states; time: the forward solve plus the adjoint steps, with
+// the recomputation overlapped.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include <cuda_runtime.h>
 #include "gs_kernels.h"
@@ -55,6 +57,39 @@ int forward(const gpgmp_gs_params* p, const T* u0, const T* v0, T* u, T* v, T* c
     return GPGMP_OK;
 }
 
+// Side stream and events of the backward pipeline, one set per device, created on
+// first use and kept for the life of the process.  The mutex also makes the
+// enqueue of one backward pass atomic with respect to another host thread's.
+struct GSPipe {
+    cudaStream_t side = nullptr;
+    cudaEvent_t start = nullptr, rec[2] = {nullptr, nullptr}, adj[2] = {nullptr, nullptr};
+};
+std::mutex& pipe_mutex() {
+    static std::mutex m;
+    return m;
+}
+int side_pipe(GSPipe** out) {
+    static GSPipe pipes[64];
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(GPGMP_ERR_UNSUPPORTED, "device ordinal %d", dev);
+    GSPipe& q = pipes[dev];
+    if (!q.side) {
+        CK(cudaStreamCreateWithFlags(&q.side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&q.start, cudaEventDisableTiming));
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaEventCreateWithFlags(&q.rec[b], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&q.adj[b], cudaEventDisableTiming));
+        }
+    }
+    *out = &q;
+    return GPGMP_OK;
+}
+
+// Backward pass.  The recomputation of a segment's states depends only on its
+// checkpoint, so it runs on a side stream up to two segments ahead of the adjoint
+// steps on the caller's stream (two segment buffers; a buffer is refilled after
+// the adjoint launch that read it).  The two run concurrently on different SMs.
 template <typename T>
 int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T* gu, T* gv, double* grad6,
             void* work, void* stream) {
@@ -64,8 +99,9 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
     cudaStream_t st = (cudaStream_t)stream;
     const int c = ck_every(p);
     const size_t nn = (size_t)p->n * p->n;
-    T* seg = (T*)work;                       // c states, 2 nn each
-    T* lam = seg + (size_t)2 * c * nn;       // two adjoint buffers (u, v) x 2
+    T* segb[2] = {(T*)work, (T*)work + (size_t)2 * c * nn};   // c states, 2 nn each
+    T* fin[2] = {segb[1] + (size_t)2 * c * nn, segb[1] + (size_t)2 * c * nn + 2 * nn};   // recomputed end states
+    T* lam = fin[1] + 2 * nn;                // two adjoint buffers (u, v) x 2
     T* la[2] = {lam, lam + 2 * nn};
     int* err = (int*)(lam + 4 * nn);         // status word: a bounded in-kernel wait gave up
     CK(cudaMemsetAsync(grad6, 0, 6 * sizeof(double), st));
@@ -73,29 +109,50 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
     CK(cudaMemcpyAsync(la[0], lu, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(la[0] + nn, lv, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
     const int nseg = (p->steps + c - 1) / c;
-    int cur = 0;
-    GSParams g = to_params(p);
-    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
-        const int s0 = sgi * c;
-        const int len = std::min(c, p->steps - s0);
-        const T* cku = ckpt + (size_t)2 * sgi * nn;
-        GSParams gf = g;
-        gf.steps = len;
-        // states before steps 0..len-1 of the segment; the final state lands in the spare slot
-        T* scratch = la[1 - cur];
-        CK(gs_forward<T>(gf, cku, cku + nn, scratch, scratch + nn, seg, 1, st));
-        T* out = la[1 - cur];
-        T* outg = (sgi == 0) ? nullptr : out;
-        if (sgi == 0) {
-            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, gu, gv, grad6, err, st));
-        } else {
-            CK(gs_adjoint_segment<T>(g, seg, len, la[cur], la[cur] + nn, outg, outg + nn, grad6, err, st));
-            cur = 1 - cur;
-        }
-    }
     if (nseg == 0) {
         CK(cudaMemcpyAsync(gu, lu, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(gv, lv, nn * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        return GPGMP_OK;
+    }
+    GSParams g = to_params(p);
+    std::lock_guard<std::mutex> lk(pipe_mutex());
+    GSPipe* pp = nullptr;
+    rc = side_pipe(&pp);
+    if (rc) return rc;
+    CK(cudaEventRecord(pp->start, st));               // checkpoints and inputs are ready
+    CK(cudaStreamWaitEvent(pp->side, pp->start, 0));
+    bool used[2] = {false, false};
+    auto seg_len = [&](int sgi) { return std::min(c, p->steps - sgi * c); };
+    auto recompute = [&](int sgi) -> int {
+        const int b = sgi & 1;
+        if (used[b]) CK(cudaStreamWaitEvent(pp->side, pp->adj[b], 0));
+        GSParams gf = g;
+        gf.steps = seg_len(sgi);
+        const T* cku = ckpt + (size_t)2 * sgi * nn;
+        // states before steps 0..len-1 of the segment into segb[b]
+        CK(gs_forward<T>(gf, cku, cku + nn, fin[b], fin[b] + nn, segb[b], 1, pp->side));
+        CK(cudaEventRecord(pp->rec[b], pp->side));
+        return GPGMP_OK;
+    };
+    int next = nseg - 1;
+    for (int q = 0; q < 2 && next >= 0; ++q, --next) {
+        rc = recompute(next);
+        if (rc) return rc;
+    }
+    int cur = 0;
+    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+        const int b = sgi & 1;
+        CK(cudaStreamWaitEvent(st, pp->rec[b], 0));
+        T* ou = sgi == 0 ? gu : la[1 - cur];
+        T* ov = sgi == 0 ? gv : la[1 - cur] + nn;
+        CK(gs_adjoint_segment<T>(g, segb[b], seg_len(sgi), la[cur], la[cur] + nn, ou, ov, grad6, err, st));
+        CK(cudaEventRecord(pp->adj[b], st));
+        used[b] = true;
+        cur = 1 - cur;
+        if (next >= 0) {
+            rc = recompute(next--);
+            if (rc) return rc;
+        }
     }
     return GPGMP_OK;
 }
@@ -111,7 +168,8 @@ int gpgmp_gs_buffer_sizes(const gpgmp_gs_params* p, int32_t elem_bytes, size_t* 
     const size_t nn = (size_t)p->n * p->n;
     const size_t nseg = (size_t)((p->steps + c - 1) / c);
     *ck_bytes = std::max<size_t>(1, nseg) * 2 * nn * elem_bytes;
-    *work_bytes = ((size_t)2 * c * nn + 4 * nn) * elem_bytes + 16;  // + status word
+    // two segment buffers, two recomputed end states, two adjoint buffers, status word
+    *work_bytes = ((size_t)4 * c * nn + 8 * nn) * elem_bytes + 16;
     return GPGMP_OK;
 }
 

@@ -203,20 +203,18 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // adjoint update of a column pair (transpose of gs_update2), with the gradient
 // partial sums of gs_adj_update in packed form
-__device__ __forceinline__ void gs_adj_update2(const GSCoef2& k, float2 aU, float2 aC, float2 aD, float aLs, float aRs,
-                                               float2 bU, float2 bC, float2 bD, float bLs, float bRs, float2 uU,
-                                               float2 uC, float2 uD, float uLs, float uRs, float2 vU, float2 vC,
-                                               float2 vD, float vLs, float vRs, float2* an, float2* bn, float2 t[6]) {
-    const float2 aL = make_float2(aLs, aC.x), aR = make_float2(aC.y, aRs);
-    const float2 bL = make_float2(bLs, bC.x), bR = make_float2(bC.y, bRs);
-    const float2 uL = make_float2(uLs, uC.x), uR = make_float2(uC.y, uRs);
-    const float2 vL = make_float2(vLs, vC.x), vR = make_float2(vC.y, vRs);
+// (any pairing of cells, full neighbour pairs; DRIFT as in gs_update2f)
+template <int DRIFT = -1>
+__device__ __forceinline__ void gs_adj_update2f(const GSCoef2& k, float2 aL, float2 aR, float2 aU, float2 aC, float2 aD,
+                                                float2 bL, float2 bR, float2 bU, float2 bC, float2 bD, float2 uL,
+                                                float2 uR, float2 uU, float2 uC, float2 uD, float2 vL, float2 vR,
+                                                float2 vU, float2 vC, float2 vD, float2* an, float2* bn, float2 t[6]) {
     const float2 lap_a = fma2(k.m4, aC, add2(add2(aL, aR), add2(aU, aD)));
     const float2 lap_b = fma2(k.m4, bC, add2(add2(bL, bR), add2(bU, bD)));
     const float2 ba = sub2(bC, aC);
     float2 x = fma2(k.du, lap_a, mul2(k.mdtF, aC));
     float2 y = fma2(k.dv, lap_b, mul2(k.mdtFk, bC));
-    if (k.drift) {
+    if (DRIFT == 1 || (DRIFT < 0 && k.drift)) {
         x = fma2(k.hx, sub2(aR, aL), fma2(k.hy, sub2(aD, aU), x));
         y = fma2(k.hx, sub2(bR, bL), fma2(k.hy, sub2(bD, bU), y));
     }
@@ -232,6 +230,15 @@ __device__ __forceinline__ void gs_adj_update2(const GSCoef2& k, float2 aU, floa
     t[3] = fma2(bC, lv, t[3]);
     t[4] = fma2(aC, sub2(uR, uL), fma2(bC, sub2(vR, vL), t[4]));
     t[5] = fma2(aC, sub2(uD, uU), fma2(bC, sub2(vD, vU), t[5]));
+}
+
+__device__ __forceinline__ void gs_adj_update2(const GSCoef2& k, float2 aU, float2 aC, float2 aD, float aLs, float aRs,
+                                               float2 bU, float2 bC, float2 bD, float bLs, float bRs, float2 uU,
+                                               float2 uC, float2 uD, float uLs, float uRs, float2 vU, float2 vC,
+                                               float2 vD, float vLs, float vRs, float2* an, float2* bn, float2 t[6]) {
+    gs_adj_update2f(k, make_float2(aLs, aC.x), make_float2(aC.y, aRs), aU, aC, aD, make_float2(bLs, bC.x),
+                    make_float2(bC.y, bRs), bU, bC, bD, make_float2(uLs, uC.x), make_float2(uC.y, uRs), uU, uC, uD,
+                    make_float2(vLs, vC.x), make_float2(vC.y, vRs), vU, vC, vD, an, bn, t);
 }
 
 template <int N>

@@ -367,3 +367,247 @@ __global__ void __launch_bounds__(32 * WPC, 1)
         rr_store<H>(vo + (size_t)(row0 + r) * N + col0, pv);
     }
 }
+
+// ---- register-resident adjoint -----------------------------------------------------
+// The transposed steps of a segment, last to first, with the adjoint fields
+// (lambda_u, lambda_v) in registers and exchanged between warps exactly like the
+// forward state.  The stored forward states of the segment stream through shared
+// memory: lane 0 of warp 0 issues TMA bulk copies (cp.async.bulk, completion on a
+// "full" mbarrier) of the CTA's rows plus one halo row above and below, two steps
+// ahead into a ring of four buffers; every warp releases a buffer on an "empty"
+// mbarrier when it is done with it, and a buffer is refilled only after all warps
+// released it.  The per-cell arithmetic is gs_adj_update2f, the same as the
+// shared-memory adjoint kernel, so the adjoint fields are bit-identical to it; the
+// parameter-gradient partial sums are formed per lane and step in float and summed
+// in double, as there.
+
+template <int N, int WPC>
+struct RRAdjShape {
+    using F = RRShape<N, WPC>;
+    static constexpr int R = F::R, H = F::H;
+    static constexpr int RC = WPC * R;                      // rows per CTA
+    static constexpr int NB = 4;                            // state buffers in the ring
+    static constexpr int kAhead = 2;                        // steps issued ahead
+    static constexpr uint32_t kPipe = F::kHalo + (uint32_t)WPC * 16u;   // full[NB], empty[NB]
+    static constexpr uint32_t kFlag = kPipe + 16u * NB;
+    static constexpr uint32_t kState = (kFlag + 16u + 127u) / 128u * 128u;   // [buf][field][RC + 2][N]
+    static constexpr uint32_t kPlane = (uint32_t)(RC + 2) * 4u * N;
+    static constexpr uint32_t kSmem = kState + 2u * NB * kPlane;
+};
+
+template <int H, int DRIFT>
+__device__ __forceinline__ void rr_adj_row(const GSCoef2& k, const float2 (&aU)[H], const float2 (&aC)[H],
+                                           const float2 (&aD)[H], const float2 (&bU)[H], const float2 (&bC)[H],
+                                           const float2 (&bD)[H], const float2 (&uU)[H], const float2 (&uC)[H],
+                                           const float2 (&uD)[H], float ul, float ur, const float2 (&vU)[H],
+                                           const float2 (&vC)[H], const float2 (&vD)[H], float vl, float vr,
+                                           float2 (&an)[H], float2 (&bn)[H], float2 t[6], int lane) {
+    const int lft = (lane + 31) & 31, rgt = (lane + 1) & 31;
+    const float al = __shfl_sync(0xffffffffu, aC[H - 1].y, lft), ar = __shfl_sync(0xffffffffu, aC[0].x, rgt);
+    const float bl = __shfl_sync(0xffffffffu, bC[H - 1].y, lft), br = __shfl_sync(0xffffffffu, bC[0].x, rgt);
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        const int jl = j == 0 ? 0 : j - 1, jr = j == H - 1 ? 0 : j + 1;
+        const float2 aL = j == 0 ? make_float2(al, aC[H - 1].x) : aC[jl];
+        const float2 aR = j == H - 1 ? make_float2(aC[0].y, ar) : aC[jr];
+        const float2 bL = j == 0 ? make_float2(bl, bC[H - 1].x) : bC[jl];
+        const float2 bR = j == H - 1 ? make_float2(bC[0].y, br) : bC[jr];
+        const float2 uL = j == 0 ? make_float2(ul, uC[H - 1].x) : uC[jl];
+        const float2 uR = j == H - 1 ? make_float2(uC[0].y, ur) : uC[jr];
+        const float2 vL = j == 0 ? make_float2(vl, vC[H - 1].x) : vC[jl];
+        const float2 vR = j == H - 1 ? make_float2(vC[0].y, vr) : vC[jr];
+        gs_adj_update2f<DRIFT>(k, aL, aR, aU[j], aC[j], aD[j], bL, bR, bU[j], bC[j], bD[j], uL, uR, uU[j], uC[j],
+                               uD[j], vL, vR, vU[j], vC[j], vD[j], &an[j], &bn[j], t);
+    }
+}
+
+// issues the TMA copies of the forward state of adjoint step q (stored state
+// len - 1 - q) into ring buffer q % NB, after all warps released that buffer's
+// previous use (step q - NB); one thread
+template <int N, int WPC>
+__device__ __forceinline__ void rr_adj_issue(const RRCtx<N, WPC>& c, const float* __restrict__ states, int len, int q,
+                                             int rc0) {
+    using S = RRAdjShape<N, WPC>;
+    constexpr int NN = N * N, RC = S::RC;
+    const int b = q % S::NB, j = len - 1 - q;
+    uint64_t* full = reinterpret_cast<uint64_t*>(const_cast<unsigned char*>(c.smem) + S::kPipe) + b;
+    if (q >= S::NB) rr_wait(c.sbase + S::kPipe + 8u * (S::NB + b), (uint32_t)((q - S::NB) / S::NB) & 1u, c.failed);
+    fence_proxy_async();
+    const uint32_t row_bytes = 4u * N;
+    mbar_expect_tx(full, 2u * (RC + 2) * row_bytes);
+    for (int f = 0; f < 2; ++f) {
+        const float* src = states + (size_t)(2 * j + f) * NN;
+        float* dst = reinterpret_cast<float*>(const_cast<unsigned char*>(c.smem) + S::kState +
+                                              (uint32_t)(2 * b + f) * S::kPlane);
+        bulk_g2s(dst, src + (size_t)((rc0 + N - 1) & (N - 1)) * N, row_bytes, full);
+        bulk_g2s(dst + N, src + (size_t)rc0 * N, RC * row_bytes, full);
+        bulk_g2s(dst + (RC + 1) * N, src + (size_t)((rc0 + RC) & (N - 1)) * N, row_bytes, full);
+    }
+}
+
+// one transposed step X -> Y of the warp's adjoint rows; the forward state of the
+// step is buffer s % NB of the state ring
+template <int N, int WPC, int DRIFT>
+__device__ __forceinline__ void rr_adj_step(const RRCtx<N, WPC>& c, const GSCoef2& k,
+                                            const float2 (&xa)[RRShape<N, WPC>::R][RRShape<N, WPC>::H],
+                                            const float2 (&xb)[RRShape<N, WPC>::R][RRShape<N, WPC>::H],
+                                            float2 (&ya)[RRShape<N, WPC>::R][RRShape<N, WPC>::H],
+                                            float2 (&yb)[RRShape<N, WPC>::R][RRShape<N, WPC>::H], int s, bool send,
+                                            double (&g)[6]) {
+    using S = RRAdjShape<N, WPC>;
+    constexpr int R = S::R, H = S::H;
+    const int par = s & 1, sb = s % S::NB;
+    const uint32_t full = c.sbase + S::kPipe + 8u * sb;
+    const uint32_t empty = c.sbase + S::kPipe + 8u * (S::NB + sb);
+    rr_wait(full, (uint32_t)(s / S::NB) & 1u, c.failed);        // the forward state of this step
+    rr_wait(c.bar(c.w, par), (uint32_t)(s >> 1) & 1u, c.failed);   // the adjoint halo rows
+    __syncwarp();
+    if (c.lane == 0) rr_arm(c.bar(c.w, par), c.tx);
+    float2 ha[H], hb[H], la[H], lb[H];
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 0) - c.sbase), c.lane, ha);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 1) - c.sbase), c.lane, hb);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 0) - c.sbase), c.lane, la);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 1) - c.sbase), c.lane, lb);
+    // state rows -1 .. R of the warp (shared-memory rows w R .. w R + R + 1)
+    const float* Us = reinterpret_cast<const float*>(c.smem + S::kState + (uint32_t)(2 * sb) * S::kPlane);
+    const float* Vs = reinterpret_cast<const float*>(c.smem + S::kState + (uint32_t)(2 * sb + 1) * S::kPlane);
+    const int col0 = c.lane * 2 * H;
+    float2 su[R + 2][H], sv[R + 2][H];
+    float sul[R], sur[R], svl[R], svr[R];
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r) {
+        rr_load<H>(Us + (c.w * R + r) * N + col0, su[r]);
+        rr_load<H>(Vs + (c.w * R + r) * N + col0, sv[r]);
+    }
+    const int cl_ = (col0 + N - 1) & (N - 1), cr = (col0 + 2 * H) & (N - 1);   // columns left / right of the block
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int o = (c.w * R + r + 1) * N;
+        sul[r] = Us[o + cl_];
+        sur[r] = Us[o + cr];
+        svl[r] = Vs[o + cl_];
+        svr[r] = Vs[o + cr];
+    }
+    float2 t[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
+    if constexpr (R == 1) {
+        rr_adj_row<H, DRIFT>(k, ha, xa[0], la, hb, xb[0], lb, su[0], su[1], su[2], sul[0], sur[0], sv[0], sv[1], sv[2],
+                             svl[0], svr[0], ya[0], yb[0], t, c.lane);
+    } else {
+        rr_adj_row<H, DRIFT>(k, ha, xa[0], xa[1], hb, xb[0], xb[1], su[0], su[1], su[2], sul[0], sur[0], sv[0], sv[1],
+                             sv[2], svl[0], svr[0], ya[0], yb[0], t, c.lane);
+        rr_adj_row<H, DRIFT>(k, xa[R - 2], xa[R - 1], la, xb[R - 2], xb[R - 1], lb, su[R - 1], su[R], su[R + 1],
+                             sul[R - 1], sur[R - 1], sv[R - 1], sv[R], sv[R + 1], svl[R - 1], svr[R - 1], ya[R - 1],
+                             yb[R - 1], t, c.lane);
+    }
+    if (send) {
+        const int np = par ^ 1;
+        rr_send<H>(ya[0], yb[0], c.slot(c.up_w, np, 1, 0), c.slot(c.up_w, np, 1, 1), c.bar(c.up_w, np), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(ya[R - 1], yb[R - 1], c.slot(c.dn_w, np, 0, 0), c.slot(c.dn_w, np, 0, 1), c.bar(c.dn_w, np),
+                   c.dn_remote, c.dn_rank, c.lane);
+    }
+#pragma unroll
+    for (int r = 1; r < R - 1; ++r)
+        rr_adj_row<H, DRIFT>(k, xa[r - 1], xa[r], xa[r + 1], xb[r - 1], xb[r], xb[r + 1], su[r], su[r + 1], su[r + 2],
+                             sul[r], sur[r], sv[r], sv[r + 1], sv[r + 2], svl[r], svr[r], ya[r], yb[r], t, c.lane);
+    __syncwarp();
+    if (c.lane == 0) rr_arrive(empty);                       // this warp is done with the state buffer
+#pragma unroll
+    for (int q = 0; q < 6; ++q) g[q] += (double)t[q].x + (double)t[q].y;
+}
+
+template <int N, int WPC, int DRIFT>
+__global__ void __launch_bounds__(32 * WPC, 1)
+    k_gs_adjoint_rr(GSArgs<float> a, const float* __restrict__ states, int len, const float* __restrict__ lu_in,
+                    const float* __restrict__ lv_in, float* __restrict__ lu_out, float* __restrict__ lv_out,
+                    double* __restrict__ grad, int* __restrict__ err) {
+    using S = RRAdjShape<N, WPC>;
+    constexpr int R = S::R, H = S::H, RC = S::RC;
+    constexpr int NN = N * N;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red[6][32];
+    RRCtx<N, WPC> c;
+    c.smem = smem_raw;
+    c.sbase = smem_u32(smem_raw);
+    c.lane = threadIdx.x & 31;
+    c.w = threadIdx.x >> 5;
+    const uint32_t rank = rr_ctarank();
+    c.up_remote = c.w == 0;
+    c.dn_remote = c.w == WPC - 1;
+    c.up_rank = c.up_remote ? (rank + kRRCluster - 1) % kRRCluster : rank;
+    c.dn_rank = c.dn_remote ? (rank + 1) % kRRCluster : rank;
+    c.up_w = c.up_remote ? WPC - 1 : c.w - 1;
+    c.dn_w = c.dn_remote ? 0 : c.w + 1;
+    c.failed = reinterpret_cast<volatile int*>(smem_raw + S::kFlag);
+    const int nremote = (int)c.up_remote + (int)c.dn_remote;
+    c.tx = (uint32_t)nremote * 2u * RRShape<N, WPC>::kRow;
+    uint64_t* pipe = reinterpret_cast<uint64_t*>(smem_raw + S::kPipe);   // full[0..NB-1], empty[0..NB-1]
+    const int rc0 = (int)rank * RC;
+    const int row0 = rc0 + c.w * R;
+    const int col0 = c.lane * 2 * H;
+    const GSCoef2 k(a);
+
+    const bool issuer = threadIdx.x == 0;
+    if (issuer) {
+        for (int b = 0; b < S::NB; ++b) {
+            mbar_init(&pipe[b], 1);
+            mbar_init(&pipe[S::NB + b], WPC);
+        }
+        *c.failed = 0;
+        fence_mbar_init();
+    }
+    if (c.lane == 0) {
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 0) - c.sbase)), 1 + 32 * (2 - nremote));
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 1) - c.sbase)), 1 + 32 * (2 - nremote));
+        fence_mbar_init();
+    }
+    float2 xa[R][H], xb[R][H], ya[R][H], yb[R][H];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        rr_load<H>(lu_in + (size_t)(row0 + r) * N + col0, xa[r]);
+        rr_load<H>(lv_in + (size_t)(row0 + r) * N + col0, xb[r]);
+    }
+    __syncthreads();
+    cluster_arrive();     // every CTA's mbarriers exist before anyone sends
+    cluster_wait();
+    double g[6] = {0, 0, 0, 0, 0, 0};
+    if (issuer)
+        for (int q = 0; q < S::kAhead && q < len; ++q) rr_adj_issue<N, WPC>(c, states, len, q, rc0);
+    if (len > 0) {
+        if (c.lane == 0) {
+            rr_arm(c.bar(c.w, 0), c.tx);
+            rr_arm(c.bar(c.w, 1), c.tx);
+        }
+        rr_send<H>(xa[0], xb[0], c.slot(c.up_w, 0, 1, 0), c.slot(c.up_w, 0, 1, 1), c.bar(c.up_w, 0), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(xa[R - 1], xb[R - 1], c.slot(c.dn_w, 0, 0, 0), c.slot(c.dn_w, 0, 0, 1), c.bar(c.dn_w, 0),
+                   c.dn_remote, c.dn_rank, c.lane);
+    }
+    int s = 0;
+    for (; s + 2 <= len; s += 2) {
+        if (issuer && s + S::kAhead < len) rr_adj_issue<N, WPC>(c, states, len, s + S::kAhead, rc0);
+        rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, true, g);
+        if (issuer && s + 1 + S::kAhead < len) rr_adj_issue<N, WPC>(c, states, len, s + 1 + S::kAhead, rc0);
+        rr_adj_step<N, WPC, DRIFT>(c, k, ya, yb, xa, xb, s + 1, s + 2 < len, g);
+    }
+    const bool odd = s < len;
+    if (odd) rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, false, g);
+    __syncthreads();
+    cluster_arrive();     // no CTA leaves while a neighbour may still address its shared memory
+    cluster_wait();
+    const bool bad = *c.failed != 0;
+    if (bad && threadIdx.x == 0) atomicOr(err, 1);
+    const float nan = __int_as_float(0x7fc00000);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        float2 pa[H], pb[H];
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            pa[j] = bad ? make_float2(nan, nan) : (odd ? ya[r][j] : xa[r][j]);
+            pb[j] = bad ? make_float2(nan, nan) : (odd ? yb[r][j] : xb[r][j]);
+        }
+        rr_store<H>(lu_out + (size_t)(row0 + r) * N + col0, pa);
+        rr_store<H>(lv_out + (size_t)(row0 + r) * N + col0, pb);
+    }
+    grad_reduce(g, (double)a.dt, grad, red, (int)threadIdx.x, (int)blockDim.x);
+}

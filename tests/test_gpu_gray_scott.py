@@ -96,6 +96,40 @@ def test_register_resident_forward_bit_exact(gpgmp, n, steps, drift, every):
         assert torch.equal(ru, tu) and torch.equal(rv, tv)
 
 
+_RR_ADJ_WARPS = {64: [1, 2, 4], 128: [2, 4, 8], 256: [8]}
+
+
+@pytest.mark.parametrize("n,steps,every,drift", [(64, 7, 3, True), (64, 1, 1, False), (128, 50, 20, False),
+                                                 (256, 203, 100, True), (256, 100, 100, False)])
+def test_register_resident_adjoint_matches_shared_memory_adjoint(gpgmp, n, steps, every, drift):
+    """The register-resident adjoint (TMA-fed state ring, adjoint fields in registers)
+    against the shared-memory adjoint kernel: the adjoint fields bit-identical, the
+    parameter gradient (float partial sums in a different order) to 1e-5."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=n, steps=steps, checkpoint_every=every, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0)
+    u0, v0 = _init(cfg, np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    rng = np.random.default_rng(5)
+    lu = torch.tensor(rng.standard_normal((n, n)).astype(np.float32), device="cuda")
+    lv = torch.tensor(rng.standard_normal((n, n)).astype(np.float32), device="cuda")
+
+    def run(variant):
+        p = cfg.params(variant=variant)
+        ckb, _ = gs.buffer_sizes(p, 4)
+        ck = torch.empty(ckb // 4, dtype=torch.float32, device="cuda")
+        gs.forward(tu, tv, p, checkpoints=ck)
+        return gs.adjoint(p, ck, lu, lv)
+
+    ru, rv, rg = run(2)
+    rg = rg.cpu().numpy()
+    for var in [0, 3] + [10 + w for w in _RR_ADJ_WARPS[n]]:
+        gu, gv, g6 = run(var)
+        assert torch.equal(gu, ru) and torch.equal(gv, rv), var
+        np.testing.assert_allclose(g6.cpu().numpy(), rg, rtol=1e-5, atol=1e-5 * np.abs(rg).max())
+    assert gs.status() == 0
+
+
 @pytest.mark.parametrize("cluster", [2, 16])
 def test_adjoint_f64_matches_oracle_adjoint(gpgmp, cluster):
     import torch
