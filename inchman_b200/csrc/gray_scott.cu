@@ -551,7 +551,7 @@ const void* rr_adj_kernel(int n, int* wpc, bool drift, size_t* smem) {
     if (*wpc == 0) *wpc = n == 256 ? 8 : n == 128 ? 4 : 2;
     GS_RRA_CASE(64, 1) GS_RRA_CASE(64, 2) GS_RRA_CASE(64, 4)
     GS_RRA_CASE(128, 2) GS_RRA_CASE(128, 4) GS_RRA_CASE(128, 8)
-    GS_RRA_CASE(256, 8)
+    GS_RRA_CASE(256, 4) GS_RRA_CASE(256, 8)
 #undef GS_RRA_CASE
     return nullptr;
 }

@@ -232,6 +232,38 @@ __device__ __forceinline__ void gs_adj_update2f(const GSCoef2& k, float2 aL, flo
     t[5] = fma2(aC, sub2(uD, uU), fma2(bC, sub2(vD, vU), t[5]));
 }
 
+// The same adjoint update with the gradient partial sums moved onto the adjoint
+// field by summation by parts over the periodic lattice, which needs the forward
+// state only at the cells themselves:
+//   sum a lap(u) = sum u lap(a),   sum a (uR - uL) = -sum u (aR - aL)  (and in y).
+// t[2], t[3] as in gs_adj_update2f; t[4], t[5] hold the NEGATED drift sums.  The
+// adjoint fields an, bn are the same bits as gs_adj_update2f's.
+template <int DRIFT>
+__device__ __forceinline__ void gs_adj_update2s(const GSCoef2& k, float2 aL, float2 aR, float2 aU, float2 aC, float2 aD,
+                                                float2 bL, float2 bR, float2 bU, float2 bC, float2 bD, float2 uC,
+                                                float2 vC, float2* an, float2* bn, float2 t[6]) {
+    const float2 lap_a = fma2(k.m4, aC, add2(add2(aL, aR), add2(aU, aD)));
+    const float2 lap_b = fma2(k.m4, bC, add2(add2(bL, bR), add2(bU, bD)));
+    const float2 ba = sub2(bC, aC);
+    float2 x = fma2(k.du, lap_a, mul2(k.mdtF, aC));
+    float2 y = fma2(k.dv, lap_b, mul2(k.mdtFk, bC));
+    const float2 dxa = sub2(aR, aL), dya = sub2(aD, aU), dxb = sub2(bR, bL), dyb = sub2(bD, bU);
+    if (DRIFT == 1) {
+        x = fma2(k.hx, dxa, fma2(k.hy, dya, x));
+        y = fma2(k.hx, dxb, fma2(k.hy, dyb, y));
+    }
+    x = fma2(mul2(k.dt, mul2(vC, vC)), ba, x);
+    y = fma2(mul2(k.two_dt, mul2(uC, vC)), ba, y);
+    *an = add2(aC, x);
+    *bn = add2(bC, y);
+    t[0] = fma2(aC, sub2(k.one, uC), t[0]);
+    t[1] = fma2(bC, vC, t[1]);
+    t[2] = fma2(uC, lap_a, t[2]);
+    t[3] = fma2(vC, lap_b, t[3]);
+    t[4] = fma2(uC, dxa, fma2(vC, dxb, t[4]));
+    t[5] = fma2(uC, dya, fma2(vC, dyb, t[5]));
+}
+
 __device__ __forceinline__ void gs_adj_update2(const GSCoef2& k, float2 aU, float2 aC, float2 aD, float aLs, float aRs,
                                                float2 bU, float2 bC, float2 bD, float bLs, float bRs, float2 uU,
                                                float2 uC, float2 uD, float uLs, float uRs, float2 vU, float2 vC,

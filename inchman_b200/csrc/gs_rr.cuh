@@ -214,6 +214,7 @@ struct RRShape {
     // mbarriers, then the CTA's failure flag
     static constexpr uint32_t kHalo = (uint32_t)WPC * 8u * kRow;
     static constexpr uint32_t kSmem = kHalo + (uint32_t)WPC * 16u + 16u;
+    static_assert(kSmem <= 227u * 1024u, "forward shared memory exceeds a B200 CTA's");
     static_assert(R >= 1 && R * kRRCluster * WPC == N && H >= 1 && 64 * H == N, "lattice split");
 };
 
@@ -373,13 +374,14 @@ __global__ void __launch_bounds__(32 * WPC, 1)
 // (lambda_u, lambda_v) in registers and exchanged between warps exactly like the
 // forward state.  The stored forward states of the segment stream through shared
 // memory: lane 0 of warp 0 issues TMA bulk copies (cp.async.bulk, completion on a
-// "full" mbarrier) of the CTA's rows plus one halo row above and below, two steps
-// ahead into a ring of four buffers; every warp releases a buffer on an "empty"
-// mbarrier when it is done with it, and a buffer is refilled only after all warps
-// released it.  The per-cell arithmetic is gs_adj_update2f, the same as the
-// shared-memory adjoint kernel, so the adjoint fields are bit-identical to it; the
-// parameter-gradient partial sums are formed per lane and step in float and summed
-// in double, as there.
+// "full" mbarrier) of the CTA's rows two steps ahead into a ring of four buffers;
+// every warp releases a buffer on an "empty" mbarrier when it is done with it, and
+// a buffer is refilled only after all warps released it.  The per-cell update is
+// gs_adj_update2s: the adjoint fields are bit-identical to the shared-memory
+// adjoint kernel's, and the parameter-gradient sums, taken by parts over the
+// periodic lattice, need the forward state only at the cell itself (so no state
+// halo rows).  The partial sums are formed per lane and step in float and summed
+// in double.
 
 template <int N, int WPC>
 struct RRAdjShape {
@@ -390,17 +392,16 @@ struct RRAdjShape {
     static constexpr int kAhead = 2;                        // steps issued ahead
     static constexpr uint32_t kPipe = F::kHalo + (uint32_t)WPC * 16u;   // full[NB], empty[NB]
     static constexpr uint32_t kFlag = kPipe + 16u * NB;
-    static constexpr uint32_t kState = (kFlag + 16u + 127u) / 128u * 128u;   // [buf][field][RC + 2][N]
-    static constexpr uint32_t kPlane = (uint32_t)(RC + 2) * 4u * N;
+    static constexpr uint32_t kState = (kFlag + 16u + 127u) / 128u * 128u;   // [buf][field][RC][N]
+    static constexpr uint32_t kPlane = (uint32_t)RC * 4u * N;
     static constexpr uint32_t kSmem = kState + 2u * NB * kPlane;
+    static_assert(kSmem <= 227u * 1024u, "adjoint shared memory exceeds a B200 CTA's");
 };
 
 template <int H, int DRIFT>
 __device__ __forceinline__ void rr_adj_row(const GSCoef2& k, const float2 (&aU)[H], const float2 (&aC)[H],
                                            const float2 (&aD)[H], const float2 (&bU)[H], const float2 (&bC)[H],
-                                           const float2 (&bD)[H], const float2 (&uU)[H], const float2 (&uC)[H],
-                                           const float2 (&uD)[H], float ul, float ur, const float2 (&vU)[H],
-                                           const float2 (&vC)[H], const float2 (&vD)[H], float vl, float vr,
+                                           const float2 (&bD)[H], const float2 (&uC)[H], const float2 (&vC)[H],
                                            float2 (&an)[H], float2 (&bn)[H], float2 t[6], int lane) {
     const int lft = (lane + 31) & 31, rgt = (lane + 1) & 31;
     const float al = __shfl_sync(0xffffffffu, aC[H - 1].y, lft), ar = __shfl_sync(0xffffffffu, aC[0].x, rgt);
@@ -412,12 +413,8 @@ __device__ __forceinline__ void rr_adj_row(const GSCoef2& k, const float2 (&aU)[
         const float2 aR = j == H - 1 ? make_float2(aC[0].y, ar) : aC[jr];
         const float2 bL = j == 0 ? make_float2(bl, bC[H - 1].x) : bC[jl];
         const float2 bR = j == H - 1 ? make_float2(bC[0].y, br) : bC[jr];
-        const float2 uL = j == 0 ? make_float2(ul, uC[H - 1].x) : uC[jl];
-        const float2 uR = j == H - 1 ? make_float2(uC[0].y, ur) : uC[jr];
-        const float2 vL = j == 0 ? make_float2(vl, vC[H - 1].x) : vC[jl];
-        const float2 vR = j == H - 1 ? make_float2(vC[0].y, vr) : vC[jr];
-        gs_adj_update2f<DRIFT>(k, aL, aR, aU[j], aC[j], aD[j], bL, bR, bU[j], bC[j], bD[j], uL, uR, uU[j], uC[j],
-                               uD[j], vL, vR, vU[j], vC[j], vD[j], &an[j], &bn[j], t);
+        gs_adj_update2s<DRIFT>(k, aL, aR, aU[j], aC[j], aD[j], bL, bR, bU[j], bC[j], bD[j], uC[j], vC[j], &an[j],
+                               &bn[j], t);
     }
 }
 
@@ -428,20 +425,17 @@ template <int N, int WPC>
 __device__ __forceinline__ void rr_adj_issue(const RRCtx<N, WPC>& c, const float* __restrict__ states, int len, int q,
                                              int rc0) {
     using S = RRAdjShape<N, WPC>;
-    constexpr int NN = N * N, RC = S::RC;
+    constexpr int NN = N * N;
     const int b = q % S::NB, j = len - 1 - q;
     uint64_t* full = reinterpret_cast<uint64_t*>(const_cast<unsigned char*>(c.smem) + S::kPipe) + b;
     if (q >= S::NB) rr_wait(c.sbase + S::kPipe + 8u * (S::NB + b), (uint32_t)((q - S::NB) / S::NB) & 1u, c.failed);
     fence_proxy_async();
-    const uint32_t row_bytes = 4u * N;
-    mbar_expect_tx(full, 2u * (RC + 2) * row_bytes);
+    mbar_expect_tx(full, 2u * S::kPlane);
     for (int f = 0; f < 2; ++f) {
-        const float* src = states + (size_t)(2 * j + f) * NN;
+        const float* src = states + (size_t)(2 * j + f) * NN + (size_t)rc0 * N;
         float* dst = reinterpret_cast<float*>(const_cast<unsigned char*>(c.smem) + S::kState +
                                               (uint32_t)(2 * b + f) * S::kPlane);
-        bulk_g2s(dst, src + (size_t)((rc0 + N - 1) & (N - 1)) * N, row_bytes, full);
-        bulk_g2s(dst + N, src + (size_t)rc0 * N, RC * row_bytes, full);
-        bulk_g2s(dst + (RC + 1) * N, src + (size_t)((rc0 + RC) & (N - 1)) * N, row_bytes, full);
+        bulk_g2s(dst, src, S::kPlane, full);
     }
 }
 
@@ -453,7 +447,7 @@ __device__ __forceinline__ void rr_adj_step(const RRCtx<N, WPC>& c, const GSCoef
                                             const float2 (&xb)[RRShape<N, WPC>::R][RRShape<N, WPC>::H],
                                             float2 (&ya)[RRShape<N, WPC>::R][RRShape<N, WPC>::H],
                                             float2 (&yb)[RRShape<N, WPC>::R][RRShape<N, WPC>::H], int s, bool send,
-                                            double (&g)[6]) {
+                                            float2 t[6]) {
     using S = RRAdjShape<N, WPC>;
     constexpr int R = S::R, H = S::H;
     const int par = s & 1, sb = s % S::NB;
@@ -468,35 +462,21 @@ __device__ __forceinline__ void rr_adj_step(const RRCtx<N, WPC>& c, const GSCoef
     rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 1) - c.sbase), c.lane, hb);
     rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 0) - c.sbase), c.lane, la);
     rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 1) - c.sbase), c.lane, lb);
-    // state rows -1 .. R of the warp (shared-memory rows w R .. w R + R + 1)
+    // the forward state at the warp's rows (shared-memory rows w R .. w R + R - 1)
     const float* Us = reinterpret_cast<const float*>(c.smem + S::kState + (uint32_t)(2 * sb) * S::kPlane);
     const float* Vs = reinterpret_cast<const float*>(c.smem + S::kState + (uint32_t)(2 * sb + 1) * S::kPlane);
     const int col0 = c.lane * 2 * H;
-    float2 su[R + 2][H], sv[R + 2][H];
-    float sul[R], sur[R], svl[R], svr[R];
+    float2 su[R][H], sv[R][H];
 #pragma unroll
-    for (int r = 0; r < R + 2; ++r) {
+    for (int r = 0; r < R; ++r) {
         rr_load<H>(Us + (c.w * R + r) * N + col0, su[r]);
         rr_load<H>(Vs + (c.w * R + r) * N + col0, sv[r]);
     }
-    const int cl_ = (col0 + N - 1) & (N - 1), cr = (col0 + 2 * H) & (N - 1);   // columns left / right of the block
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int o = (c.w * R + r + 1) * N;
-        sul[r] = Us[o + cl_];
-        sur[r] = Us[o + cr];
-        svl[r] = Vs[o + cl_];
-        svr[r] = Vs[o + cr];
-    }
-    float2 t[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
     if constexpr (R == 1) {
-        rr_adj_row<H, DRIFT>(k, ha, xa[0], la, hb, xb[0], lb, su[0], su[1], su[2], sul[0], sur[0], sv[0], sv[1], sv[2],
-                             svl[0], svr[0], ya[0], yb[0], t, c.lane);
+        rr_adj_row<H, DRIFT>(k, ha, xa[0], la, hb, xb[0], lb, su[0], sv[0], ya[0], yb[0], t, c.lane);
     } else {
-        rr_adj_row<H, DRIFT>(k, ha, xa[0], xa[1], hb, xb[0], xb[1], su[0], su[1], su[2], sul[0], sur[0], sv[0], sv[1],
-                             sv[2], svl[0], svr[0], ya[0], yb[0], t, c.lane);
-        rr_adj_row<H, DRIFT>(k, xa[R - 2], xa[R - 1], la, xb[R - 2], xb[R - 1], lb, su[R - 1], su[R], su[R + 1],
-                             sul[R - 1], sur[R - 1], sv[R - 1], sv[R], sv[R + 1], svl[R - 1], svr[R - 1], ya[R - 1],
+        rr_adj_row<H, DRIFT>(k, ha, xa[0], xa[1], hb, xb[0], xb[1], su[0], sv[0], ya[0], yb[0], t, c.lane);
+        rr_adj_row<H, DRIFT>(k, xa[R - 2], xa[R - 1], la, xb[R - 2], xb[R - 1], lb, su[R - 1], sv[R - 1], ya[R - 1],
                              yb[R - 1], t, c.lane);
     }
     if (send) {
@@ -508,12 +488,10 @@ __device__ __forceinline__ void rr_adj_step(const RRCtx<N, WPC>& c, const GSCoef
     }
 #pragma unroll
     for (int r = 1; r < R - 1; ++r)
-        rr_adj_row<H, DRIFT>(k, xa[r - 1], xa[r], xa[r + 1], xb[r - 1], xb[r], xb[r + 1], su[r], su[r + 1], su[r + 2],
-                             sul[r], sur[r], sv[r], sv[r + 1], sv[r + 2], svl[r], svr[r], ya[r], yb[r], t, c.lane);
+        rr_adj_row<H, DRIFT>(k, xa[r - 1], xa[r], xa[r + 1], xb[r - 1], xb[r], xb[r + 1], su[r], sv[r], ya[r], yb[r], t,
+                             c.lane);
     __syncwarp();
     if (c.lane == 0) rr_arrive(empty);                       // this warp is done with the state buffer
-#pragma unroll
-    for (int q = 0; q < 6; ++q) g[q] += (double)t[q].x + (double)t[q].y;
 }
 
 template <int N, int WPC, int DRIFT>
@@ -583,15 +561,30 @@ __global__ void __launch_bounds__(32 * WPC, 1)
         rr_send<H>(xa[R - 1], xb[R - 1], c.slot(c.dn_w, 0, 0, 0), c.slot(c.dn_w, 0, 0, 1), c.bar(c.dn_w, 0),
                    c.dn_remote, c.dn_rank, c.lane);
     }
+    // gradient partial sums: float over the two steps of an iteration, then double
+    auto flush = [&](float2 (&t)[6]) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            g[q] += (double)t[q].x + (double)t[q].y;
+            t[q] = f2(0.f);
+        }
+    };
+    float2 t[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
     int s = 0;
     for (; s + 2 <= len; s += 2) {
         if (issuer && s + S::kAhead < len) rr_adj_issue<N, WPC>(c, states, len, s + S::kAhead, rc0);
-        rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, true, g);
+        rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, true, t);
         if (issuer && s + 1 + S::kAhead < len) rr_adj_issue<N, WPC>(c, states, len, s + 1 + S::kAhead, rc0);
-        rr_adj_step<N, WPC, DRIFT>(c, k, ya, yb, xa, xb, s + 1, s + 2 < len, g);
+        rr_adj_step<N, WPC, DRIFT>(c, k, ya, yb, xa, xb, s + 1, s + 2 < len, t);
+        flush(t);
     }
     const bool odd = s < len;
-    if (odd) rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, false, g);
+    if (odd) {
+        rr_adj_step<N, WPC, DRIFT>(c, k, xa, xb, ya, yb, s, false, t);
+        flush(t);
+    }
+    g[4] = -g[4];      // gs_adj_update2s accumulates the drift sums negated
+    g[5] = -g[5];
     __syncthreads();
     cluster_arrive();     // no CTA leaves while a neighbour may still address its shared memory
     cluster_wait();
