@@ -18,6 +18,14 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: 
 STOCHASTIC_HOMOGENEOUS = 0
 STOCHASTIC_INHOMOGENEOUS = 1
 DETERMINISTIC_RK4 = 2
+STOCHASTIC_INHOMOGENEOUS_FPE = 3
+DETERMINISTIC_AQSS = 4
+DETERMINISTIC_INHOMOGENEOUS_RK4 = 5
+DETERMINISTIC_INHOMOGENEOUS_AQSS = 6
+DETERMINISTIC_TYPES = (DETERMINISTIC_RK4, DETERMINISTIC_AQSS, DETERMINISTIC_INHOMOGENEOUS_RK4,
+                       DETERMINISTIC_INHOMOGENEOUS_AQSS)
+INHOMOGENEOUS_TYPES = (STOCHASTIC_INHOMOGENEOUS, STOCHASTIC_INHOMOGENEOUS_FPE, DETERMINISTIC_INHOMOGENEOUS_RK4,
+                       DETERMINISTIC_INHOMOGENEOUS_AQSS)
 
 DRIFT_FIELD = -1
 DRIFT_HOMOGENEOUS = 0
@@ -26,6 +34,8 @@ DRIFT_ORNSTEIN_UHLENBECK = 2
 
 FLAG_STOP_ON_ERROR = 4
 FLAG_LITERAL_REDIFFUSION = 8
+FLAG_AQSS_LITERAL = 16
+FLAG_NO_INHOM_DET_REACTIONS = 32
 CREATE_SYNC_EACH_LAUNCH = 1
 
 SIM_EVENT_CAP = 1

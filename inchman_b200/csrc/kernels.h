@@ -31,11 +31,13 @@ cudaError_t launch_homog_diffuse(const GridDesc& g, const int32_t* in, int32_t* 
                                  uint32_t step_seed, float pmove, cudaStream_t st);
 cudaError_t launch_source(const GridDesc& g, int32_t* plane_base, int species, uint32_t seed, uint32_t step_seed,
                           int boundary, int count, float pi, cudaStream_t st);
+// fpe: the FPE discretisation's jump probabilities (stochastic_inhomogeneous_fpe)
 cudaError_t launch_sweep(const GridDesc& g, const int32_t* in, int32_t* out, int species, int sweep_y,
                          uint32_t seed, uint32_t step_seed, const float* d_D, const float* d_r, float dt, float dx,
-                         cudaStream_t st);
+                         cudaStream_t st, int fpe = 0);
+// kind: 0 stochastic drift-diffusion, 1 FPE (uses stay), 2 deterministic
 cudaError_t launch_timestep(int area, const float* d_D, const float* d_r, float dx, uint32_t* d_min_key,
-                            cudaStream_t st);
+                            cudaStream_t st, int kind = 0, float stay = 0.f);
 cudaError_t launch_diffusivity_drift(const GridDesc& g, int species, int method, const float* params, float L,
                                      float* dx, float* dy, float* rx, float* ry, cudaStream_t st);
 
@@ -44,6 +46,13 @@ cudaError_t launch_det_diffuse(const GridDesc& g, const float* in, float* out, c
                                float dx2, cudaStream_t st);
 cudaError_t launch_rk4(const GridDesc& g, float* state, const gpgmp_reaction* d_reactions, int nreac,
                        float deltat, cudaStream_t st);
+// inhomogeneous deterministic drift-diffusion, one species, one direction (out of place;
+// `out` receives the whole state)
+cudaError_t launch_det_sweep(const GridDesc& g, const float* in, float* out, int species, int sweep_y,
+                             const float* d_D, const float* d_r, float dt, float dx, cudaStream_t st);
+// alpha-QSS reaction window (literal: the reference's corrector coefficient as printed)
+cudaError_t launch_aqss(const GridDesc& g, float* state, const gpgmp_reaction* d_reactions, int nreac, float deltat,
+                        int literal, int32_t* d_status, cudaStream_t st);
 
 // order-preserving float <-> uint key for atomicMin over floats
 inline float key_to_float(uint32_t k) {

@@ -30,6 +30,9 @@ struct gpgmp_solver {
     GridDesc g{};
     size_t area = 0;
     bool deterministic = false, inhom = false;
+    bool aqss = false;      // alpha-QSS reaction windows instead of RK4
+    bool fpe = false;       // stochastic_inhomogeneous_fpe jump rates
+    int ts_kind = 0;        // time step formula of the inhomogeneous solvers (TimestepKind)
     // stochastic state: two buffers, per-species current index
     int32_t* d_buf[2] = {nullptr, nullptr};
     std::vector<int> cur;
@@ -47,10 +50,15 @@ struct gpgmp_solver {
     // InhomogeneousSolver.h m_nextDiffusionTimeX/Y, m_smallestDtX/Y, m_diffusionDtX/Y)
     std::vector<float> dt, next;
     std::vector<float> nextX, nextY, smallX, smallY, ddX, ddY;
-    float pi = 0.f, pmove = 0.f, h = 1.f, det_dt = 0.f;
+    float pi = 0.f, pmove = 0.f, h = 1.f, det_dt = 0.f, stay = 0.f;
 };
 
 namespace {
+
+bool is_inhom_type(int t) {
+    return t == GPGMP_STOCHASTIC_INHOMOGENEOUS || t == GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE ||
+           t == GPGMP_DETERMINISTIC_INHOMOGENEOUS_RK4 || t == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
+}
 
 #define CK(expr)                                                                       \
     do {                                                                               \
@@ -144,8 +152,8 @@ int validate(const gpgmp_model_desc* m, int R) {
             if (r.product_species[j] < 0 || r.product_species[j] >= m->num_species || r.product_stoich[j] < 0)
                 return set_error(GPGMP_ERR_INVALID, "reaction %d: bad product %d", i, j);
     }
-    if (m->solver_type < 0 || m->solver_type > 2) return set_error(GPGMP_ERR_UNSUPPORTED, "solver_type %d", m->solver_type);
-    if (m->solver_type == GPGMP_STOCHASTIC_INHOMOGENEOUS) {
+    if (m->solver_type < 0 || m->solver_type > 6) return set_error(GPGMP_ERR_UNSUPPORTED, "solver_type %d", m->solver_type);
+    if (is_inhom_type(m->solver_type)) {
         if (m->drift_method == GPGMP_DRIFT_FIELD &&
             (!m->field_dx || !m->field_dy || !m->field_rx || !m->field_ry))
             return set_error(GPGMP_ERR_INVALID, "field drift method needs all four field arrays");
@@ -157,7 +165,8 @@ int validate(const gpgmp_model_desc* m, int R) {
 }
 
 // InhomogeneousSolver.cpp:164-212: diffusivity/drift per species, then the first
-// time steps (computeTimestepX/Y read back one float each).
+// time steps (computeTimestepX/Y read back one float each; the formula depends on
+// the solver type).
 int inhom_init(gpgmp_solver* h) {
     const size_t n = h->area * h->g.S;
     if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
@@ -173,10 +182,12 @@ int inhom_init(gpgmp_solver* h) {
     const float dx = h->m.physical_length / (float)h->m.width;
     for (int s = 0; s < h->g.S; ++s) {
         uint32_t key[2];
-        CK(launch_timestep((int)h->area, h->d_Dx + s * h->area, h->d_rx + s * h->area, dx, h->d_minkey, h->stream));
+        CK(launch_timestep((int)h->area, h->d_Dx + s * h->area, h->d_rx + s * h->area, dx, h->d_minkey, h->stream,
+                           h->ts_kind, h->stay));
         CK(cudaMemcpyAsync(&key[0], h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        CK(launch_timestep((int)h->area, h->d_Dy + s * h->area, h->d_ry + s * h->area, dx, h->d_minkey, h->stream));
+        CK(launch_timestep((int)h->area, h->d_Dy + s * h->area, h->d_ry + s * h->area, dx, h->d_minkey, h->stream,
+                           h->ts_kind, h->stay));
         CK(cudaMemcpyAsync(&key[1], h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         h->smallX[s] = key_to_float(key[0]);
@@ -210,8 +221,13 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     if (model->num_reactions > 0) h->reactions.assign(model->reactions, model->reactions + model->num_reactions);
     h->m.diffusion = h->diffusion.data();
     h->m.reactions = h->reactions.empty() ? nullptr : h->reactions.data();
-    h->deterministic = model->solver_type == GPGMP_DETERMINISTIC_RK4;
-    h->inhom = model->solver_type == GPGMP_STOCHASTIC_INHOMOGENEOUS;
+    const int ty = model->solver_type;
+    h->deterministic = ty == GPGMP_DETERMINISTIC_RK4 || ty == GPGMP_DETERMINISTIC_AQSS ||
+                       ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_RK4 || ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
+    h->inhom = is_inhom_type(ty);
+    h->aqss = ty == GPGMP_DETERMINISTIC_AQSS || ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
+    h->fpe = ty == GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE;
+    h->ts_kind = h->deterministic ? 2 : (h->fpe ? 1 : 0);
     h->g.W = model->width;
     h->g.H = model->height;
     h->g.S = model->num_species;
@@ -259,11 +275,12 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     }
     // stay probability and jump probability as the reference's header computes them
     const float stay = (float)(1.0 - (double)model->p0);
+    h->stay = stay;
     h->pi = (float)((1.0 - (double)stay) / 6.0);
     h->pmove = h->pi * 4.0f;
     h->dt.assign(S, 0.f);
     h->next.assign(S, 0.f);
-    if (h->deterministic) {
+    if (h->deterministic && !h->inhom) {
         // HomogeneousSolver.cpp:168-192: one common step, the smallest over species
         float dtd = 0.f;
         for (int i = 0; i < S; ++i) {
@@ -359,6 +376,11 @@ int gpgmp_init_poisson(gpgmp_solver* h, const float* lambda) {
 int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
     if (!h || !seed) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (h->deterministic) {
+        if (h->inhom && (h->m.flags & GPGMP_FLAG_NO_INHOM_DET_REACTIONS)) return GPGMP_OK;
+        if (h->aqss)
+            return after_launch(h, launch_aqss(h->g, h->d_fbuf[h->fcur], h->d_reactions, (int)h->reactions.size(),
+                                               deltat, (h->m.flags & GPGMP_FLAG_AQSS_LITERAL) ? 1 : 0,
+                                               h->d_status, h->stream));
         return after_launch(h, launch_rk4(h->g, h->d_fbuf[h->fcur], h->d_reactions, (int)h->reactions.size(), deltat,
                                           h->stream));
     }
@@ -373,7 +395,7 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
     if (i < 0 || i >= h->g.S) return set_error(GPGMP_ERR_INVALID, "species %d", i);
     const size_t plane_stride = 0;
     (void)plane_stride;
-    if (h->deterministic) {
+    if (h->deterministic && !h->inhom) {
         int rc = after_launch(h, launch_det_diffuse(h->g, h->d_fbuf[h->fcur], h->d_fbuf[1 - h->fcur], h->d_diff,
                                                     h->dt[i], h->h * h->h, h->stream));
         h->fcur ^= 1;
@@ -402,10 +424,28 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
     }
     const float dxw = h->m.physical_length / (float)h->m.width;
     const float dyw = h->m.physical_length / (float)h->m.height;
+    if (h->deterministic) {
+        // InhomogeneousSolver::diffuse, deterministic branch (:282-287, :374-378): the
+        // sweeps take no random numbers, so the seed does not advance
+        for (int dir = 0; dir < 2; ++dir) {
+            float& nxt = dir == 0 ? h->nextX[i] : h->nextY[i];
+            if (!(nxt <= t)) continue;
+            int rc = after_launch(h, launch_det_sweep(h->g, h->d_fbuf[h->fcur], h->d_fbuf[1 - h->fcur], i, dir,
+                                                      dir == 0 ? h->d_Dx : h->d_Dy, dir == 0 ? h->d_rx : h->d_ry,
+                                                      dir == 0 ? h->ddX[i] : h->ddY[i], dir == 0 ? dxw : dyw,
+                                                      h->stream));
+            if (rc) return rc;
+            h->fcur ^= 1;
+            nxt += dir == 0 ? h->smallX[i] : h->smallY[i];
+            (dir == 0 ? h->ddX[i] : h->ddY[i]) = dir == 0 ? h->smallX[i] : h->smallY[i];
+        }
+        h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
+        return GPGMP_OK;
+    }
     if (h->nextX[i] <= t) {
         const int c = h->cur[i];
         int rc = after_launch(h, launch_sweep(h->g, h->d_buf[c], h->d_buf[1 - c], i, 0, h->seed, (uint32_t)*seed,
-                                              h->d_Dx, h->d_rx, h->ddX[i], dxw, h->stream));
+                                              h->d_Dx, h->d_rx, h->ddX[i], dxw, h->stream, h->fpe ? 1 : 0));
         if (rc) return rc;
         h->cur[i] ^= 1;
         (*seed)++;
@@ -415,7 +455,7 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
     if (h->nextY[i] <= t) {
         const int c = h->cur[i];
         int rc = after_launch(h, launch_sweep(h->g, h->d_buf[c], h->d_buf[1 - c], i, 1, h->seed, (uint32_t)*seed,
-                                              h->d_Dy, h->d_ry, h->ddY[i], dyw, h->stream));
+                                              h->d_Dy, h->d_ry, h->ddY[i], dyw, h->stream, h->fpe ? 1 : 0));
         if (rc) return rc;
         h->cur[i] ^= 1;
         (*seed)++;
@@ -506,7 +546,7 @@ int gpgmp_solve(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_sna
             for (int i = 0; i < S; ++i) {
                 if (!(i == minspec || h->next[i] <= mindt)) continue;
                 if (!(h->next[i] > 0)) continue;
-                if (h->deterministic && applied && !(m.flags & GPGMP_FLAG_LITERAL_REDIFFUSION)) {
+                if (h->deterministic && !h->inhom && applied && !(m.flags & GPGMP_FLAG_LITERAL_REDIFFUSION)) {
                     h->next[i] += h->dt[i];
                     continue;
                 }
@@ -520,7 +560,7 @@ int gpgmp_solve(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_sna
             outputLast += m.output_interval;
         }
         simTime = mindt;
-        if (stop_on_error && !h->deterministic) {
+        if (stop_on_error && (!h->deterministic || h->aqss)) {
             rc = gpgmp_get_status(h, st_host.data());
             if (rc) return rc;
             bool any = false;

@@ -14,7 +14,8 @@
 //                 then an equal four-way split) instead of one uniform per particle.
 //   sweep_probs   StochasticInhomogeneousDriftDiffusion.cl:512-520 (X) and
 //                 :642-650 (Y): ps, p1 (towards +), p2-p1 (towards -).
-//   cell_timestep StochasticInhomogeneousDriftDiffusion.cl:124-151.
+//   cell_timestep StochasticInhomogeneousDriftDiffusion.cl:124-151 (and the FPE
+//                 and deterministic variants of the same kernel).
 #pragma once
 #include "common.cuh"
 #include "../../include/gpgmp_c.h"
@@ -174,11 +175,26 @@ __device__ __forceinline__ void sweep_probs(float D, float r, float dt, float dx
     *Pm = pm < 0.0f ? 0.0f : (pm > rest ? rest : pm);
 }
 
+// The FPE discretisation's jump probabilities (stochastic_inhomogeneous_fpe,
+// StochasticInhomogeneousDriftDiffusion.cl:197-203 rates, :493-499 use): rate
+// towards + is D/dx^2 + r/(2 dx), towards - is D/dx^2 - r/(2 dx), times dt.  A rate
+// that comes out negative (|r| dx > 2 D) is clamped to 0.
+__device__ __forceinline__ void sweep_probs_fpe(float D, float r, float dt, float dx, float* Pp, float* Pm) {
+    const float a = D / (dx * dx), b = r / (2.0f * dx);
+    *Pp = clamp01((a + b) * dt);
+    const float pm = (a - b) * dt, rest = 1.0f - *Pp;
+    *Pm = pm < 0.0f ? 0.0f : (pm > rest ? rest : pm);
+}
+
 // (minus, plus) counts of one cell for a directional sweep.
 __device__ __forceinline__ void sweep_lost(int n, float D, float r, float dt, float dx, Stream& st, bool at_lo,
-                                           bool at_hi, int mask_lo, int mask_hi, int* minus, int* plus) {
+                                           bool at_hi, int mask_lo, int mask_hi, int* minus, int* plus,
+                                           bool fpe = false) {
     float Pp, Pm;
-    sweep_probs(D, r, dt, dx, &Pp, &Pm);
+    if (fpe)
+        sweep_probs_fpe(D, r, dt, dx, &Pp, &Pm);
+    else
+        sweep_probs(D, r, dt, dx, &Pp, &Pm);
     const float Pt = Pp + Pm;
     const int moved = binomial(st, n, Pt);
     int p = Pt > 0.0f ? binomial(st, moved, Pp / Pt) : 0;
@@ -192,10 +208,10 @@ __device__ __forceinline__ void sweep_lost(int n, float D, float r, float dt, fl
 // Evaluated in double; below |eps| = 1e-3 tanh and temp come from their series
 // (tanh eps = eps - eps^3/3, temp = 1/3 + 4 eps^2/45) because the closed form
 // cancels there (in float it gives NaN or 0 for small drift).
-__device__ __forceinline__ float cell_timestep(float Df, float rf, float dxf) {
+__device__ __forceinline__ double cell_timestep_d(float Df, float rf, float dxf) {
     const double D = Df, r = rf, dx = dxf;
-    if (r == 0.0) return (float)(dx * dx / (2.0 * D) * (1.0 / 3.0));
-    if (D == 0.0) return (float)(dx / fabs(r));
+    if (r == 0.0) return dx * dx / (2.0 * D) * (1.0 / 3.0);
+    if (D == 0.0) return dx / fabs(r);
     const double eps = dx * r / (2.0 * D);
     const double a = fabs(eps);
     double th, temp;
@@ -211,7 +227,25 @@ __device__ __forceinline__ float cell_timestep(float Df, float rf, float dxf) {
         temp = 1.0 + (-1.0 / (th * eps) + 1.0 / (sha * sha));
         if (temp <= 0.0) temp = 1.0 / 3.0;
     }
-    return (float)(dx / r * th * temp);
+    return dx / r * th * temp;
+}
+__device__ __forceinline__ float cell_timestep(float D, float r, float dx) { return (float)cell_timestep_d(D, r, dx); }
+
+// Time step kinds of the per-cell minimum (StochasticInhomogeneousDriftDiffusion.cl:
+// 124-151 stochastic, :124-129 FPE, :157-190 deterministic RK4 / alpha-QSS).
+enum TimestepKind { kTsStochastic = 0, kTsFpe = 1, kTsDeterministic = 2 };
+
+// FPE: StayProbability / 6 / (D / dx^2 + |r| / (2 dx)), in float.
+__device__ __forceinline__ float fpe_timestep(float D, float r, float dx, float stay) {
+    return stay / 6.0f / (D / (dx * dx) + fabsf(r) / (2.0f * dx));
+}
+
+// deterministic inhomogeneous solvers: the stochastic formula scaled by 0.1 where
+// there is drift (the reference's r == 0 branch is not scaled); with D = 0 the
+// reference divides by zero, here the step is 0.1 dx / |r|.
+__device__ __forceinline__ float det_timestep(float D, float r, float dx) {
+    if (r == 0.0f) return (float)cell_timestep_d(D, r, dx);
+    return (float)(0.1 * cell_timestep_d(D, r, dx));
 }
 
 }  // namespace gpgmp

@@ -65,7 +65,7 @@ template <int MODE>
 __global__ void __launch_bounds__(NT) k_diffuse_tile(const int* __restrict__ in, int* __restrict__ out, int W, int H,
                                                      int S, int species, uint32_t seed, uint32_t step_seed,
                                                      float pmove, int4 bm4, const float* __restrict__ Df,
-                                                     const float* __restrict__ rf, float dt, float dx) {
+                                                     const float* __restrict__ rf, float dt, float dx, int fpe) {
     constexpr int HX = (MODE == 2) ? 0 : 1;
     constexpr int HY = (MODE == 1) ? 0 : 1;
     constexpr int RW = TW + 2 * HX, RH = TH + 2 * HY;
@@ -91,10 +91,12 @@ __global__ void __launch_bounds__(NT) k_diffuse_tile(const int* __restrict__ in,
                 homog_lost(n, pmove, st, gx, gy, W, H, bm, l);
             } else if (MODE == 1) {
                 const int64_t fi = (int64_t)species * area + c;
-                sweep_lost(n, Df[fi], rf[fi], dt, dx, st, gx == 0, gx == W - 1, bm[0], bm[1], &l[0], &l[1]);
+                sweep_lost(n, Df[fi], rf[fi], dt, dx, st, gx == 0, gx == W - 1, bm[0], bm[1], &l[0], &l[1],
+                           fpe != 0);
             } else {
                 const int64_t fi = (int64_t)species * area + c;
-                sweep_lost(n, Df[fi], rf[fi], dt, dx, st, gy == 0, gy == H - 1, bm[2], bm[3], &l[0], &l[1]);
+                sweep_lost(n, Df[fi], rf[fi], dt, dx, st, gy == 0, gy == H - 1, bm[2], bm[3], &l[0], &l[1],
+                           fpe != 0);
             }
             if (lx >= HX && lx < HX + TW && ly >= HY && ly < HY + TH) s_n[(ly - HY) * TW + (lx - HX)] = n;
         }
@@ -154,11 +156,13 @@ __device__ __forceinline__ uint32_t float_key(float f) {
 }
 
 __global__ void k_timestep(int area, const float* __restrict__ D, const float* __restrict__ r, float dx,
-                           uint32_t* min_key) {
+                           uint32_t* min_key, int kind, float stay) {
     uint32_t best = 0xffffffffu;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < area; c += gridDim.x * blockDim.x)
     {
-        const float ts = cell_timestep(D[c], r[c], dx);
+        const float ts = kind == kTsFpe             ? fpe_timestep(D[c], r[c], dx, stay)
+                         : kind == kTsDeterministic ? det_timestep(D[c], r[c], dx)
+                                                    : cell_timestep(D[c], r[c], dx);
         if (ts == ts) best = min(best, float_key(ts));   // NaN is skipped, as fminf does
     }
     for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -262,6 +266,200 @@ __global__ void k_rk4(float* state, int S, int area, int R, const gpgmp_reaction
     for (int s = 0; s < S; ++s) sp[(int64_t)s * area] = x[s * B];
 }
 
+// Deterministic.cl:71-136 (inhomogeneous drift-diffusion, one direction, one
+// species, mirror neighbours): s' = s + dt (D_l s_l + D_r s_r - 2 D s) / dx^2
+// - dt (r_r s_r - r_l s_l) / (2 dx), written out of place; the other species'
+// planes are copied so that `out` is a whole state.
+template <int DIR>
+__global__ void k_det_sweep(const float* __restrict__ in, float* __restrict__ out, int W, int H, int S, int R,
+                            int species, const float* __restrict__ D, const float* __restrict__ rv, float dt,
+                            float dx) {
+    const int area = W * H;
+    const int64_t total = (int64_t)R * S * area;
+    const float dx2 = dx * dx;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % area);
+        const int s = (int)((i / area) % S);
+        if (s != species) {
+            out[i] = in[i];
+            continue;
+        }
+        const int x = c % W, y = c / W;
+        int lo, hi;
+        if (DIR == 0) {
+            lo = x > 0 ? c - 1 : c + 1;
+            hi = x < W - 1 ? c + 1 : c - 1;
+        } else {
+            lo = y > 0 ? c - W : c + W;
+            hi = y < H - 1 ? c + W : c - W;
+        }
+        const float* p = in + (i - c);
+        const float* Dp = D + (int64_t)species * area;
+        const float* rp = rv + (int64_t)species * area;
+        const float sl = p[lo] * Dp[lo], sr = p[hi] * Dp[hi], sh = p[c] * Dp[c];
+        const float lap = sl + sr - 2.0f * sh;
+        const float drift = rp[hi] * p[hi] - rp[lo] * p[lo];
+        out[i] = p[c] + dt * lap / dx2 - dt * drift / (2.0f * dx);
+    }
+}
+
+// ---- alpha-QSS (Mott & Oran 2001), Deterministic.cl:240-522 ------------------------
+constexpr int kAqssMaxSpecies = kMaxSpecies;
+constexpr int kAqssMaxIter = 100000;    // corrector passes per cell and window before giving up
+
+// production q and destruction d of every species: law = rate * prod x^nu
+// (Reaction.cpp:145-162); a reaction adds |net| law to q (net > 0) or d (net < 0)
+// of each species whose net stoichiometry it changes (Solver.cpp:961-1004)
+__device__ __forceinline__ void aqss_rhs(const gpgmp_reaction* rt, int nreac, int S, const float* y, float* q,
+                                         float* d) {
+    for (int i = 0; i < S; ++i) { q[i] = 0.0f; d[i] = 0.0f; }
+    for (int k = 0; k < nreac; ++k) {
+        const gpgmp_reaction& rc = rt[k];
+        float law = rc.rate;
+        for (int j = 0; j < rc.num_reactants; ++j)
+            for (int m = 0; m < rc.reactant_stoich[j]; ++m) law *= y[rc.reactant_species[j]];
+        // every species of the reaction once, in reactant-then-product order
+        for (int pass = 0; pass < 2; ++pass) {
+            const int cnt = pass == 0 ? rc.num_reactants : rc.num_products;
+            for (int j = 0; j < cnt; ++j) {
+                const int sp = pass == 0 ? rc.reactant_species[j] : rc.product_species[j];
+                bool seen = false;
+                for (int a = 0; a < rc.num_reactants && !seen; ++a)
+                    if (rc.reactant_species[a] == sp && (pass == 1 || a < j)) seen = true;
+                for (int a = 0; a < rc.num_products && !seen && pass == 1; ++a)
+                    if (rc.product_species[a] == sp && a < j) seen = true;
+                if (seen) continue;
+                int net = 0;
+                for (int a = 0; a < rc.num_products; ++a) if (rc.product_species[a] == sp) net += rc.product_stoich[a];
+                for (int a = 0; a < rc.num_reactants; ++a) if (rc.reactant_species[a] == sp) net -= rc.reactant_stoich[a];
+                if (net > 0) q[sp] += (float)net * law;
+                else if (net < 0) d[sp] += (float)(-net) * law;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float aqss_alpha(float r) {
+    return (180.0f + r * (60.0f + r * (11.0f + r))) / (360.0f + r * (60.0f + r * (12.0f + r)));
+}
+
+// One window of length dtg for the species x[0..S) of one cell.  A retried step
+// restarts its predictor from the saved start state with the reduced step size
+// (Mott & Oran's method).  literal: the reference's form instead -- the predictor
+// takes the current production/destruction and the outer step's size
+// (Deterministic.cl:381-387, which never shrinks on a retry, so a species growing
+// from zero can be rejected forever) and the corrector coefficient as printed
+// (`180.*+rtaub`, :424).  Returns GPGMP_SIM_EVENT_CAP if the step control did not
+// finish within kAqssMaxIter passes.
+__device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, float dtg, bool literal) {
+    const float epsmin = 1e-2f, sqreps = 0.5f, epscl = 100.0f, epsmax = 10.0f, tfd = 1.000008f, dtmin = 1e-15f,
+                ymin = 1e-20f;
+    constexpr int itermax = 2;
+    float q[kAqssMaxSpecies], d[kAqssMaxSpecies], ys[kAqssMaxSpecies], qs[kAqssMaxSpecies], ds[kAqssMaxSpecies],
+        rtaus[kAqssMaxSpecies], scr[kAqssMaxSpecies], y1[kAqssMaxSpecies];
+    float tn = 0.0f;
+    for (int i = 0; i < S; ++i) y[i] = fmaxf(y[i], ymin);
+    aqss_rhs(rt, nreac, S, y, q, d);
+    float scrtch = 1e-25f;
+    for (int i = 0; i < S; ++i) {
+        const float ascr = fabsf(q[i]);
+        const float scr2 = copysignf(1.0f / y[i], 0.1f * epsmin * ascr - d[i]);
+        const float scr1 = scr2 * d[i];
+        scrtch = fmaxf(fmaxf(scr1, -fabsf(ascr - d[i]) * scr2), scrtch);
+    }
+    float dt = fminf(sqreps / scrtch, dtg);
+    int passes = 0;
+    while (dtg > tn * tfd) {
+        const float ts = tn;
+        const float dtcurrent = dt;
+        for (int i = 0; i < S; ++i) {
+            ys[i] = y[i];
+            qs[i] = q[i];
+            ds[i] = d[i];
+            rtaus[i] = dtcurrent * d[i] / y[i];
+        }
+        while (dtg > tn * tfd) {
+            if (++passes > kAqssMaxIter) return GPGMP_SIM_EVENT_CAP;
+            for (int i = 0; i < S; ++i) {
+                if (literal) {
+                    const float rtaui = dtcurrent * d[i] / y[i];
+                    scr[i] = (q[i] - d[i]) / (1.0f + aqss_alpha(rtaui) * rtaui);
+                } else {
+                    const float rtaui = dt * ds[i] / ys[i];
+                    scr[i] = (qs[i] - ds[i]) / (1.0f + aqss_alpha(rtaui) * rtaui);
+                }
+            }
+            float eps = 1e-10f;
+            for (int iteration = 0; iteration < itermax; ++iteration) {
+                for (int i = 0; i < S; ++i) y[i] = fmaxf(ys[i] + dt * scr[i], ymin);
+                if (iteration == 0) {
+                    tn = ts + dt;
+                    for (int i = 0; i < S; ++i) y1[i] = y[i];
+                }
+                aqss_rhs(rt, nreac, S, y, q, d);
+                eps = 1e-10f;
+                for (int i = 0; i < S; ++i) {
+                    const float rtaub = 0.5f * (rtaus[i] + dt * d[i] / y[i]);
+                    const float alpha =
+                        literal ? (180.0f * rtaub * (60.0f + rtaub * (11.0f + rtaub))) /
+                                      (360.0f + rtaub * (60.0f + rtaub * (12.0f + rtaub)))
+                                : aqss_alpha(rtaub);
+                    const float qt = qs[i] * (1.0f - alpha) + q[i] * alpha;
+                    const float pb = rtaub / dt;
+                    scr[i] = (qt - ys[i] * pb) / (1.0f + alpha * rtaub);
+                }
+            }
+            for (int i = 0; i < S; ++i) {
+                const float scr2 = fmaxf(ys[i] + dt * scr[i], 0.0f);
+                float scr1 = fabsf(scr2 - y1[i]);
+                y[i] = fmaxf(scr2, ymin);
+                if (0.25f * (ys[i] + y[i]) > ymin) {
+                    scr1 = scr1 / y[i];
+                    eps = fmaxf(0.5f * (scr1 + fminf(fabsf(q[i] - d[i]) / (q[i] + d[i] + 1e-30f), scr1)), eps);
+                }
+            }
+            eps = eps * epscl;
+            if (dt <= dtmin + 1e-16f * tn) {
+                dt = dtg - ts;
+                dt = fminf(dtmin, fabsf(dt));
+            }
+            const float stab = 0.01f;     // the stability test needs itermax >= 3
+            if (eps <= epsmax && stab <= 1.0f) {
+                if (dtg <= tn * tfd) break;
+            } else {
+                tn = ts;
+            }
+            const float rteps = sqrtf(eps);
+            float dto = dt;
+            dt = fminf(fminf(dt * (1.0f / rteps + 0.005f), tfd * (dtg - tn)), dto / (stab + 0.001f));
+            if (eps <= epsmax && stab <= 1.0f) break;
+            dto = dt / dto;
+            for (int i = 0; i < S; ++i) rtaus[i] *= dto;
+        }
+        aqss_rhs(rt, nreac, S, y, q, d);
+    }
+    return 0;
+}
+
+__global__ void k_aqss(float* state, int S, int area, int R, const gpgmp_reaction* __restrict__ reactions, int nreac,
+                       float deltat, int literal, int32_t* status) {
+    extern __shared__ unsigned char smem[];
+    gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
+    for (int i = threadIdx.x; i < nreac; i += blockDim.x) rt[i] = reactions[i];
+    __syncthreads();
+    const int64_t total = (int64_t)R * area;
+    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < total;
+         gi += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(gi / area), c = (int)(gi % area);
+        float* sp = state + (int64_t)r * S * area + c;
+        float y[kAqssMaxSpecies];
+        for (int s = 0; s < S; ++s) y[s] = sp[(int64_t)s * area];
+        const int e = aqss_cell(rt, nreac, S, y, deltat, literal != 0);
+        for (int s = 0; s < S; ++s) sp[(int64_t)s * area] = y[s];
+        if (e) atomicOr(&status[r], e);
+    }
+}
+
 inline unsigned grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -300,7 +498,7 @@ cudaError_t launch_homog_diffuse(const GridDesc& g, const int32_t* in, int32_t* 
     dim3 grid((g.W + TW - 1) / TW, (g.H + TH - 1) / TH, g.R);
     int4 bm = make_int4(g.bmask[0], g.bmask[1], g.bmask[2], g.bmask[3]);
     k_diffuse_tile<0><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, pmove, bm, nullptr,
-                                            nullptr, 0.f, 0.f);
+                                            nullptr, 0.f, 0.f, 0);
     return cudaGetLastError();
 }
 
@@ -313,23 +511,45 @@ cudaError_t launch_source(const GridDesc& g, int32_t* plane_base, int species, u
 
 cudaError_t launch_sweep(const GridDesc& g, const int32_t* in, int32_t* out, int species, int sweep_y,
                          uint32_t seed, uint32_t step_seed, const float* d_D, const float* d_r, float dt, float dx,
-                         cudaStream_t st) {
+                         cudaStream_t st, int fpe) {
     dim3 grid((g.W + TW - 1) / TW, (g.H + TH - 1) / TH, g.R);
     int4 bm = make_int4(g.bmask[0], g.bmask[1], g.bmask[2], g.bmask[3]);
     if (!sweep_y)
         k_diffuse_tile<1><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, 0.f, bm, d_D, d_r,
-                                                dt, dx);
+                                                dt, dx, fpe);
     else
         k_diffuse_tile<2><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, 0.f, bm, d_D, d_r,
-                                                dt, dx);
+                                                dt, dx, fpe);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_det_sweep(const GridDesc& g, const float* in, float* out, int species, int sweep_y,
+                             const float* d_D, const float* d_r, float dt, float dx, cudaStream_t st) {
+    const int64_t total = (int64_t)g.R * g.S * g.W * g.H;
+    if (!sweep_y)
+        k_det_sweep<0><<<grid_for(total, 256), 256, 0, st>>>(in, out, g.W, g.H, g.S, g.R, species, d_D, d_r, dt, dx);
+    else
+        k_det_sweep<1><<<grid_for(total, 256), 256, 0, st>>>(in, out, g.W, g.H, g.S, g.R, species, d_D, d_r, dt, dx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aqss(const GridDesc& g, float* state, const gpgmp_reaction* d_reactions, int nreac, float deltat,
+                        int literal, int32_t* d_status, cudaStream_t st) {
+    if (nreac <= 0) return cudaSuccess;
+    const int area = g.W * g.H;
+    const int64_t total = (int64_t)g.R * area;
+    const int threads = 128;
+    const size_t smem = sizeof(gpgmp_reaction) * nreac;
+    k_aqss<<<grid_for(total, threads), threads, smem, st>>>(state, g.S, area, g.R, d_reactions, nreac, deltat, literal,
+                                                             d_status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_timestep(int area, const float* d_D, const float* d_r, float dx, uint32_t* d_min_key,
-                            cudaStream_t st) {
+                            cudaStream_t st, int kind, float stay) {
     cudaError_t e = cudaMemsetAsync(d_min_key, 0xff, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_timestep<<<grid_for(area, 256), 256, 0, st>>>(area, d_D, d_r, dx, d_min_key);
+    k_timestep<<<grid_for(area, 256), 256, 0, st>>>(area, d_D, d_r, dx, d_min_key, kind, stay);
     return cudaGetLastError();
 }
 

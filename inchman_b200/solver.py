@@ -33,7 +33,7 @@ class Solver:
         flags = _lib.CREATE_SYNC_EACH_LAUNCH if sync_each_launch else 0
         _lib.call("gpgmp_solver_create", C.byref(self._desc), self.R, self.seed, flags, C.byref(h))
         self._h = h
-        self.deterministic = model.solver == _lib.DETERMINISTIC_RK4
+        self.deterministic = model.solver in _lib.DETERMINISTIC_TYPES
         self.dtype = np.float32 if self.deterministic else np.int32
         if stream is not None:
             _lib.call("gpgmp_solver_set_stream", self._h, C.c_void_p(stream))

@@ -41,10 +41,16 @@ extern "C" {
 #define GPGMP_SIM_EVENT_CAP 1    /* a cell hit the SSA event cap inside one window */
 #define GPGMP_SIM_OVERFLOW 2     /* a count would have passed INT32_MAX */
 
-/* SolverType (DiffusionModel.h:46-56) for the solvers this build implements */
-#define GPGMP_STOCHASTIC_HOMOGENEOUS 0
-#define GPGMP_STOCHASTIC_INHOMOGENEOUS 1
-#define GPGMP_DETERMINISTIC_RK4 2
+/* SolverType (DiffusionModel.h:46-56); the reference's bit values 1, 2, 4, 8, 16, 32, 64
+ * are numbered 0..6 here */
+#define GPGMP_STOCHASTIC_HOMOGENEOUS 0             /* stochastic_homogeneous */
+#define GPGMP_STOCHASTIC_INHOMOGENEOUS 1           /* stochastic_inhomogeneous */
+#define GPGMP_DETERMINISTIC_RK4 2                  /* deterministic_homogeneous_RK4 */
+#define GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE 3       /* stochastic_inhomogeneous_fpe: FPE jump rates and time step
+                                                      (StochasticInhomogeneousDriftDiffusion.cl:124-129,197-203,493-499) */
+#define GPGMP_DETERMINISTIC_AQSS 4                 /* deterministic_homogeneous_aqss (Deterministic.cl:240-522) */
+#define GPGMP_DETERMINISTIC_INHOMOGENEOUS_RK4 5    /* deterministic_inhomogeneous_RK4 (Deterministic.cl:71-136) */
+#define GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS 6   /* deterministic_inhomogeneous_aqss */
 
 /* drift/diffusivity methods (DiffusionModel.cpp:319-380); FIELD takes per-cell arrays */
 #define GPGMP_DRIFT_FIELD (-1)
@@ -55,6 +61,12 @@ extern "C" {
 /* gpgmp_model_desc.flags */
 #define GPGMP_FLAG_STOP_ON_ERROR 4         /* end a realisation's event loop once its status is set */
 #define GPGMP_FLAG_LITERAL_REDIFFUSION 8   /* deterministic: repeat the stencil per due species (reference) */
+#define GPGMP_FLAG_AQSS_LITERAL 16  /* alpha-QSS as the reference writes it: predictor from the current
+                                       q, d with the outer step's size (Deterministic.cl:381-387) and the
+                                       corrector coefficient as printed (`180.*+rtaub`, :424), instead of
+                                       Mott & Oran's restart from the saved state */
+#define GPGMP_FLAG_NO_INHOM_DET_REACTIONS 32 /* deterministic inhomogeneous: no reaction windows, as the
+                                                reference (Solver.cpp:250-266 runs homogeneous types only) */
 
 /* gpgmp_solver_create flags */
 #define GPGMP_CREATE_SYNC_EACH_LAUNCH 1    /* wait after every launch, as Kernel.h:252-253 does */
@@ -82,7 +94,7 @@ typedef struct gpgmp_model_desc {
     int32_t max_steps;            /* < 0: unlimited */
     int32_t boundary_mask[4];     /* x-, x+, y-, y+ : 0 reflecting, 1 absorbing (DiffusionModel.cpp:233-242) */
     int32_t source_mask[4];       /* > 0: source wall (HomogeneousSolver.cpp:210-227) */
-    int32_t solver_type;          /* GPGMP_STOCHASTIC_* / GPGMP_DETERMINISTIC_RK4 */
+    int32_t solver_type;          /* GPGMP_STOCHASTIC_* / GPGMP_DETERMINISTIC_* */
     int32_t drift_method;         /* GPGMP_DRIFT_* (inhomogeneous solver) */
     int32_t flags;                /* GPGMP_FLAG_* */
     float   drift_params[8];

@@ -103,6 +103,10 @@ double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, dou
                             int checkpoint_every, double* grad6);
 int orc_det_solve(const orc_model* m, float* state, float* snapshots, float* snap_times, int max_snapshots,
                   int* num_snapshots, int64_t* steps);
+void orc_det_sweep(const orc_model* m, const float* in, float* out, int species, int sweep_y, float dt, float dx,
+                   const float* D, const float* rv);
+int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal);
+int orc_aqss(const orc_model* m, float* state, float dtg, int literal);
 
 /* ---- sort, scan, cell offsets, particles -------------------------------------- */
 void orc_sort_pairs_u32(uint32_t* keys, uint32_t* vals, int64_t n);

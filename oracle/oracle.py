@@ -72,6 +72,9 @@ def orc():
             "orc_gs_loss_grad_f64": (f64, [C.c_int, C.c_int, f64, f64, f64, f64, f64, f64, f64, vp, vp, vp, vp,
                                            C.c_int, vp]),
             "orc_det_solve": (C.c_int, [vp, vp, vp, vp, C.c_int, P(C.c_int), P(i64)]),
+            "orc_det_sweep": (None, [vp, vp, vp, C.c_int, C.c_int, f32, f32, vp, vp]),
+            "orc_aqss_cell": (C.c_int, [vp, vp, f32, C.c_int]),
+            "orc_aqss": (C.c_int, [vp, vp, f32, C.c_int]),
             "orc_sort_pairs_u32": (None, [vp, vp, i64]),
             "orc_exclusive_scan_u32": (None, [vp, vp, i64]),
             "orc_cell_indices_ref": (None, [vp, i64, i64, vp, vp]),

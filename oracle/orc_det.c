@@ -11,10 +11,18 @@
  *    whose deterministic laws (Reaction.cpp:145-162) give the ODE right-hand side
  *    -u v^2 + F (1 - u), u v^2 - (F + k) v; a constant drift (vx, vy) enters by
  *    central differences (Deterministic.cl:71-136 with constant velocity).
- *  - The reference's deterministic RK4 event loop (DiffusionModel.cpp:1414-1603,
- *    HomogeneousSolver.cpp:168-192 common time step, Deterministic.cl:17-65 and
- *    :179-238), with one diffusion per event unless flags bit 3 asks for the
- *    reference's repetition of the all-species stencil once per due species.
+ *  - The reference's deterministic event loops (DiffusionModel.cpp:1414-1603):
+ *    homogeneous (HomogeneousSolver.cpp:168-192 common time step,
+ *    Deterministic.cl:17-65 stencil, one diffusion per event unless flags bit 3 asks
+ *    for the reference's repetition of the all-species stencil once per due
+ *    species) and inhomogeneous (InhomogeneousSolver.cpp:254-427 X/Y clocks,
+ *    StochasticInhomogeneousDriftDiffusion.cl:157-190 time steps, Deterministic.cl:
+ *    71-136 drift-diffusion sweeps, written out of place), with RK4
+ *    (Deterministic.cl:143-238) or alpha-QSS (:240-522) reaction windows.  The
+ *    reference runs no reactions in its inhomogeneous deterministic solvers
+ *    (Solver.cpp:250-266); flags bit 5 restores that.
+ *  The sweep and alpha-QSS restatements use float arithmetic in the order the CUDA
+ *  kernels use; the RK4 restatement keeps the reference's double-literal evaluation.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -162,8 +170,243 @@ double orc_gs_loss_grad_f64(int N, int steps, double F, double k, double Du, dou
     return loss;
 }
 
+/* Deterministic.cl:71-136 for one species and direction, out of place, mirror
+ * neighbours: s' = s + dt (D_l s_l + D_r s_r - 2 D s) / dx^2 - dt (r_r s_r - r_l s_l) / (2 dx). */
+void orc_det_sweep(const orc_model* m, const float* in, float* out, int species, int sweep_y, float dt, float dx,
+                   const float* D, const float* rv) {
+    const int W = m->width, H = m->height, S = m->num_species;
+    const size_t area = (size_t)W * H;
+    memcpy(out, in, sizeof(float) * area * S);
+    const float* p = in + (size_t)species * area;
+    float* o = out + (size_t)species * area;
+    const float* Dp = D + (size_t)species * area;
+    const float* rp = rv + (size_t)species * area;
+    const float dx2 = dx * dx;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const int c = x + y * W;
+            int lo, hi;
+            if (!sweep_y) { lo = x > 0 ? c - 1 : c + 1; hi = x < W - 1 ? c + 1 : c - 1; }
+            else { lo = y > 0 ? c - W : c + W; hi = y < H - 1 ? c + W : c - W; }
+            const float sl = p[lo] * Dp[lo], sr = p[hi] * Dp[hi], sh = p[c] * Dp[c];
+            const float lap = sl + sr - 2.0f * sh;
+            const float drift = rp[hi] * p[hi] - rp[lo] * p[lo];
+            o[c] = p[c] + dt * lap / dx2 - dt * drift / (2.0f * dx);
+        }
+}
+
+/* alpha-QSS (Mott & Oran 2001) as Deterministic.cl:240-522 runs it per cell: the
+ * production/destruction split of Solver.cpp:961-1004 with the laws of
+ * Reaction.cpp:145-162.  A retried step restarts its predictor from the saved start
+ * state with the reduced step size (Mott & Oran).  literal = 1 keeps the reference's
+ * predictor (current q, d and the outer step's size, :381-387) and its corrector
+ * coefficient as printed (`180.*+rtaub`, :424).  Returns 1 if the step control did
+ * not finish within ORC_AQSS_MAX_ITER corrector passes. */
+#define ORC_AQSS_MAX_ITER 100000
+static void orc_aqss_rhs(const orc_model* m, const float* y, float* q, float* d) {
+    const int S = m->num_species;
+    for (int i = 0; i < S; ++i) { q[i] = 0.0f; d[i] = 0.0f; }
+    for (int k = 0; k < m->num_reactions; ++k) {
+        const orc_reaction* rc = &m->reactions[k];
+        float law = rc->rate;
+        for (int j = 0; j < rc->num_reactants; ++j)
+            for (int a = 0; a < rc->reactant_stoich[j]; ++a) law *= y[rc->reactant_species[j]];
+        for (int pass = 0; pass < 2; ++pass) {
+            const int cnt = pass == 0 ? rc->num_reactants : rc->num_products;
+            for (int j = 0; j < cnt; ++j) {
+                const int sp = pass == 0 ? rc->reactant_species[j] : rc->product_species[j];
+                int seen = 0;
+                for (int a = 0; a < rc->num_reactants && !seen; ++a)
+                    if (rc->reactant_species[a] == sp && (pass == 1 || a < j)) seen = 1;
+                for (int a = 0; a < rc->num_products && !seen && pass == 1; ++a)
+                    if (rc->product_species[a] == sp && a < j) seen = 1;
+                if (seen) continue;
+                int net = 0;
+                for (int a = 0; a < rc->num_products; ++a) if (rc->product_species[a] == sp) net += rc->product_stoich[a];
+                for (int a = 0; a < rc->num_reactants; ++a) if (rc->reactant_species[a] == sp) net -= rc->reactant_stoich[a];
+                if (net > 0) q[sp] += (float)net * law;
+                else if (net < 0) d[sp] += (float)(-net) * law;
+            }
+        }
+    }
+}
+static float orc_aqss_alpha(float r) {
+    return (180.0f + r * (60.0f + r * (11.0f + r))) / (360.0f + r * (60.0f + r * (12.0f + r)));
+}
+int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
+    const int S = m->num_species;
+    const float epsmin = 1e-2f, sqreps = 0.5f, epscl = 100.0f, epsmax = 10.0f, tfd = 1.000008f, dtmin = 1e-15f,
+                ymin = 1e-20f;
+    const int itermax = 2;
+    float q[64], d[64], ys[64], qs[64], ds[64], rtaus[64], scr[64], y1[64];
+    float tn = 0.0f;
+    for (int i = 0; i < S; ++i) y[i] = fmaxf(y[i], ymin);
+    orc_aqss_rhs(m, y, q, d);
+    float scrtch = 1e-25f;
+    for (int i = 0; i < S; ++i) {
+        const float ascr = fabsf(q[i]);
+        const float scr2 = copysignf(1.0f / y[i], 0.1f * epsmin * ascr - d[i]);
+        const float scr1 = scr2 * d[i];
+        scrtch = fmaxf(fmaxf(scr1, -fabsf(ascr - d[i]) * scr2), scrtch);
+    }
+    float dt = fminf(sqreps / scrtch, dtg);
+    int passes = 0;
+    while (dtg > tn * tfd) {
+        const float ts = tn, dtcurrent = dt;
+        for (int i = 0; i < S; ++i) { ys[i] = y[i]; qs[i] = q[i]; ds[i] = d[i]; rtaus[i] = dtcurrent * d[i] / y[i]; }
+        while (dtg > tn * tfd) {
+            if (++passes > ORC_AQSS_MAX_ITER) return 1;
+            for (int i = 0; i < S; ++i) {
+                if (literal) {
+                    const float rtaui = dtcurrent * d[i] / y[i];
+                    scr[i] = (q[i] - d[i]) / (1.0f + orc_aqss_alpha(rtaui) * rtaui);
+                } else {
+                    const float rtaui = dt * ds[i] / ys[i];
+                    scr[i] = (qs[i] - ds[i]) / (1.0f + orc_aqss_alpha(rtaui) * rtaui);
+                }
+            }
+            float eps = 1e-10f;
+            for (int it = 0; it < itermax; ++it) {
+                for (int i = 0; i < S; ++i) y[i] = fmaxf(ys[i] + dt * scr[i], ymin);
+                if (it == 0) { tn = ts + dt; for (int i = 0; i < S; ++i) y1[i] = y[i]; }
+                orc_aqss_rhs(m, y, q, d);
+                eps = 1e-10f;
+                for (int i = 0; i < S; ++i) {
+                    const float rtaub = 0.5f * (rtaus[i] + dt * d[i] / y[i]);
+                    const float alpha = literal ? (180.0f * rtaub * (60.0f + rtaub * (11.0f + rtaub))) /
+                                                      (360.0f + rtaub * (60.0f + rtaub * (12.0f + rtaub)))
+                                                : orc_aqss_alpha(rtaub);
+                    const float qt = qs[i] * (1.0f - alpha) + q[i] * alpha;
+                    const float pb = rtaub / dt;
+                    scr[i] = (qt - ys[i] * pb) / (1.0f + alpha * rtaub);
+                }
+            }
+            for (int i = 0; i < S; ++i) {
+                const float scr2 = fmaxf(ys[i] + dt * scr[i], 0.0f);
+                float scr1 = fabsf(scr2 - y1[i]);
+                y[i] = fmaxf(scr2, ymin);
+                if (0.25f * (ys[i] + y[i]) > ymin) {
+                    scr1 = scr1 / y[i];
+                    eps = fmaxf(0.5f * (scr1 + fminf(fabsf(q[i] - d[i]) / (q[i] + d[i] + 1e-30f), scr1)), eps);
+                }
+            }
+            eps = eps * epscl;
+            if (dt <= dtmin + 1e-16f * tn) { dt = dtg - ts; dt = fminf(dtmin, fabsf(dt)); }
+            const float stab = 0.01f;
+            if (eps <= epsmax && stab <= 1.0f) {
+                if (dtg <= tn * tfd) break;
+            } else {
+                tn = ts;
+            }
+            const float rteps = sqrtf(eps);
+            float dto = dt;
+            dt = fminf(fminf(dt * (1.0f / rteps + 0.005f), tfd * (dtg - tn)), dto / (stab + 0.001f));
+            if (eps <= epsmax && stab <= 1.0f) break;
+            dto = dt / dto;
+            for (int i = 0; i < S; ++i) rtaus[i] *= dto;
+        }
+        orc_aqss_rhs(m, y, q, d);
+    }
+    return 0;
+}
+/* one alpha-QSS window for every cell of one realisation's state [S][area] */
+int orc_aqss(const orc_model* m, float* state, float dtg, int literal) {
+    const int S = m->num_species;
+    const size_t area = (size_t)m->width * m->height;
+    int bad = 0;
+    if (m->num_reactions <= 0) return 0;
+    #pragma omp parallel for schedule(dynamic, 64) reduction(|:bad)
+    for (int64_t c = 0; c < (int64_t)area; ++c) {
+        float y[64];
+        for (int i = 0; i < S; ++i) y[i] = state[c + (size_t)i * area];
+        bad |= orc_aqss_cell(m, y, dtg, literal);
+        for (int i = 0; i < S; ++i) state[c + (size_t)i * area] = y[i];
+    }
+    return bad;
+}
+
+/* InhomogeneousSolver with a deterministic type: fields and first time steps as
+ * InhomogeneousSolver.cpp:164-212, X/Y sweeps when due (:254-427, no seed), reaction
+ * windows by RK4 (type 5) or alpha-QSS (type 6) unless flags bit 5. */
+static int orc_det_inhom_solve(const orc_model* m, float* state, float* snaps, float* snap_times, int max_snaps,
+                               int* nsnap, int64_t* steps_out) {
+    const int S = m->num_species;
+    const size_t area = (size_t)m->width * m->height;
+    const int aqss = m->solver_type == 6, react = !(m->flags & 32);
+    float *Fdx = (float*)malloc(sizeof(float) * S * area), *Fdy = (float*)malloc(sizeof(float) * S * area);
+    float *Frx = (float*)malloc(sizeof(float) * S * area), *Fry = (float*)malloc(sizeof(float) * S * area);
+    float *nx = (float*)calloc(S, sizeof(float)), *ny = (float*)calloc(S, sizeof(float));
+    float *sdx = (float*)calloc(S, sizeof(float)), *sdy = (float*)calloc(S, sizeof(float));
+    float *ddx = (float*)calloc(S, sizeof(float)), *ddy = (float*)calloc(S, sizeof(float));
+    float* next = (float*)calloc(S, sizeof(float));
+    float* tmp = (float*)malloc(sizeof(float) * S * area);
+    for (int i = 0; i < S; ++i) {
+        orc_rep_diffusivity_drift(m, i, Fdx, Fdy, Frx, Fry);
+        sdx[i] = orc_rep_timestep(m, i, 0, Fdx, Frx);
+        sdy[i] = orc_rep_timestep(m, i, 1, Fdy, Fry);
+        ddx[i] = sdx[i]; ddy[i] = sdy[i];
+        nx[i] = sdx[i]; ny[i] = sdy[i];
+        next[i] = nx[i] < ny[i] ? nx[i] : ny[i];
+    }
+    const float dxw = m->physical_length / (float)m->width, dyw = m->physical_length / (float)m->height;
+    int ns = 0, bad = 0;
+#define SNAP(t) do { if (ns < max_snaps) { memcpy(snaps + (size_t)ns * S * area, state, sizeof(float) * S * area); \
+                      snap_times[ns] = (t); } ns++; } while (0)
+    SNAP(0.f);
+    float simTime = 0.f, outputLast = 0.f;
+    int64_t n = 0;
+    while ((m->max_steps < 0 || n < m->max_steps) && simTime < m->max_time) {
+        n++;
+        float mindt = next[0];
+        int minspec = 0;
+        for (int i = 1; i < S; ++i) if (next[i] < mindt) { mindt = next[i]; minspec = i; }
+        int ev = 0;
+        float mo = outputLast + m->output_interval;
+        if (mo < mindt) { mindt = mo; ev = 1; }
+        float deltat = mindt - simTime;
+        if (m->num_reactions > 0 && react) {
+            if (aqss) bad |= orc_aqss(m, state, deltat, (m->flags & 16) != 0);
+            else orc_ref_rk4(m, state, deltat);
+        }
+        if (ev == 0) {
+            for (int i = 0; i < S; ++i) {
+                if (!(i == minspec || next[i] <= mindt)) continue;
+                if (!(next[i] > 0)) continue;
+                if (nx[i] <= mindt) {
+                    orc_det_sweep(m, state, tmp, i, 0, ddx[i], dxw, Fdx, Frx);
+                    memcpy(state, tmp, sizeof(float) * S * area);
+                    nx[i] += sdx[i];
+                    ddx[i] = sdx[i];
+                }
+                if (ny[i] <= mindt) {
+                    orc_det_sweep(m, state, tmp, i, 1, ddy[i], dyw, Fdy, Fry);
+                    memcpy(state, tmp, sizeof(float) * S * area);
+                    ny[i] += sdy[i];
+                    ddy[i] = sdy[i];
+                }
+                next[i] = nx[i] < ny[i] ? nx[i] : ny[i];
+            }
+        } else if (simTime >= outputLast + m->output_interval) {
+            SNAP(mindt);
+            outputLast += m->output_interval;
+        }
+        simTime = mindt;
+        if ((m->flags & 4) && bad) break;
+    }
+    SNAP(simTime);
+#undef SNAP
+    *nsnap = ns;
+    *steps_out = n;
+    free(Fdx); free(Fdy); free(Frx); free(Fry); free(nx); free(ny); free(sdx); free(sdy); free(ddx); free(ddy);
+    free(next); free(tmp);
+    return bad;
+}
+
 int orc_det_solve(const orc_model* m, float* state, float* snaps, float* snap_times, int max_snaps,
                   int* nsnap, int64_t* steps_out) {
+    const int ty = m->solver_type;
+    if (ty == 5 || ty == 6) return orc_det_inhom_solve(m, state, snaps, snap_times, max_snaps, nsnap, steps_out);
+    const int aqss = ty == 4;
     const int S = m->num_species;
     const size_t area = (size_t)m->width * m->height;
     const float h = m->physical_length / (float)m->width;
@@ -190,7 +433,10 @@ int orc_det_solve(const orc_model* m, float* state, float* snaps, float* snap_ti
         float mo = outputLast + m->output_interval;
         if (mo < mindt) { mindt = mo; ev = 1; }
         float deltat = mindt - simTime;
-        if (m->num_reactions > 0) orc_ref_rk4(m, state, deltat);
+        if (m->num_reactions > 0) {
+            if (aqss) orc_aqss(m, state, deltat, (m->flags & 16) != 0);
+            else orc_ref_rk4(m, state, deltat);
+        }
         if (ev == 0) {
             int applied = 0;
             for (int i = 0; i < S; ++i) {

@@ -164,10 +164,10 @@ static inline double orc_exp_d(double x) {
  *        dt = h/r tanh(eps) temp,
  * with tanh eps = eps - eps^3/3 and temp = 1/3 + 4 eps^2/45 for |eps| < 1e-3, where
  * the closed form cancels. */
-static inline float orc_cell_timestep(float Df, float rf, float dxf) {
+static inline double orc_cell_timestep_d(float Df, float rf, float dxf) {
     const double D = Df, r = rf, dx = dxf;
-    if (r == 0.0) return (float)(dx * dx / (2.0 * D) * (1.0 / 3.0));
-    if (D == 0.0) return (float)(dx / fabs(r));
+    if (r == 0.0) return dx * dx / (2.0 * D) * (1.0 / 3.0);
+    if (D == 0.0) return dx / fabs(r);
     const double eps = dx * r / (2.0 * D);
     const double a = fabs(eps);
     double th, temp;
@@ -183,7 +183,21 @@ static inline float orc_cell_timestep(float Df, float rf, float dxf) {
         temp = 1.0 + (-1.0 / (th * eps) + 1.0 / (sha * sha));
         if (temp <= 0.0) temp = 1.0 / 3.0;
     }
-    return (float)(dx / r * th * temp);
+    return dx / r * th * temp;
+}
+static inline float orc_cell_timestep(float D, float r, float dx) { return (float)orc_cell_timestep_d(D, r, dx); }
+
+/* stochastic_inhomogeneous_fpe (StochasticInhomogeneousDriftDiffusion.cl:124-129):
+ * StayProbability / 6 / (D / dx^2 + |r| / (2 dx)), in float */
+static inline float orc_fpe_timestep(float D, float r, float dx, float stay) {
+    return stay / 6.0f / (D / (dx * dx) + fabsf(r) / (2.0f * dx));
+}
+/* deterministic inhomogeneous solvers (:157-190): the drift formula scaled by 0.1, the
+ * r == 0 formula unscaled; D == 0 with drift gives 0.1 dx / |r| (the reference divides
+ * by zero there) */
+static inline float orc_det_timestep(float D, float r, float dx) {
+    if (r == 0.0f) return (float)orc_cell_timestep_d(D, r, dx);
+    return (float)(0.1 * orc_cell_timestep_d(D, r, dx));
 }
 
 /* Binomial(n, p) by chunked inversion. */

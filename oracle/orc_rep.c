@@ -214,8 +214,18 @@ static inline void rep_sweep_probs(float D, float r, float dt, float dx, float* 
     *Pm = pm < 0.0f ? 0.0f : (pm > rest ? rest : pm);
 }
 
+/* stochastic_inhomogeneous_fpe rates (StochasticInhomogeneousDriftDiffusion.cl:197-203)
+ * times dt; a negative rate is clamped to 0 */
+static inline void rep_sweep_probs_fpe(float D, float r, float dt, float dx, float* Pp, float* Pm) {
+    float a = D / (dx * dx), b = r / (2.0f * dx);
+    *Pp = rep_clamp01((a + b) * dt);
+    float pm = (a - b) * dt, rest = 1.0f - *Pp;
+    *Pm = pm < 0.0f ? 0.0f : (pm > rest ? rest : pm);
+}
+
 void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int sweep_y,
                            uint32_t step_seed, float dt, const float* dfield, const float* rfield) {
+    const int fpe = m->solver_type == 3;
     const int W = m->width, H = m->height, S = m->num_species;
     const size_t area = (size_t)W * H;
     const float dx = sweep_y ? m->physical_length / (float)H : m->physical_length / (float)W;
@@ -232,7 +242,8 @@ void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t s
                 orc_stream_init(&s, seed, (uint32_t)r, step_seed, (uint32_t)c,
                                 ORC_PH_DIFF | ((uint32_t)species << 8) | (sweep_y ? 2u : 1u));
                 float Pp, Pm;
-                rep_sweep_probs(Df[c], rf[c], dt, dx, &Pp, &Pm);
+                if (fpe) rep_sweep_probs_fpe(Df[c], rf[c], dt, dx, &Pp, &Pm);
+                else rep_sweep_probs(Df[c], rf[c], dt, dx, &Pp, &Pm);
                 float Pt = Pp + Pm;
                 int moved = orc_binomial(&s, st[c], Pt);
                 int plus = Pt > 0.0f ? orc_binomial(&s, moved, Pp / Pt) : 0;
@@ -261,15 +272,20 @@ void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t s
 }
 
 float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float* dfield, const float* rfield) {
-    /* StochasticInhomogeneousDriftDiffusion.cl:124-151 per cell, then the minimum (:382-423) */
+    /* StochasticInhomogeneousDriftDiffusion.cl:124-151 per cell (the FPE and deterministic
+     * formulas by solver type), then the minimum (:382-423) */
     const size_t area = (size_t)m->width * m->height;
     const float dx = m->physical_length / (float)m->width;
     const float* Df = dfield + (size_t)species * area;
     const float* rf = rfield + (size_t)species * area;
     (void)sweep_y;
+    const int ty = m->solver_type;
+    const float stay = (float)(1.0 - (double)m->p0);
     float best = INFINITY;
     for (size_t c = 0; c < area; ++c) {
-        float ts = orc_cell_timestep(Df[c], rf[c], dx);
+        float ts = ty == 3 ? orc_fpe_timestep(Df[c], rf[c], dx, stay)
+                 : (ty == 5 || ty == 6) ? orc_det_timestep(Df[c], rf[c], dx)
+                 : orc_cell_timestep(Df[c], rf[c], dx);
         if (ts == ts) best = fminf(best, ts);
     }
     return best;
@@ -324,7 +340,7 @@ int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
     const int S = m->num_species;
     const size_t area = (size_t)m->width * m->height;
     const size_t block = (size_t)R * S * area;
-    const int inhom = m->solver_type == 1;
+    const int inhom = m->solver_type == 1 || m->solver_type == 3;
     const int stop_on_error = (m->flags & 4) != 0;
     const float h = m->physical_length / (float)m->width;
     float* dtv = (float*)calloc(S, sizeof(float));
