@@ -31,6 +31,7 @@ DRIFT_FIELD = -1
 DRIFT_HOMOGENEOUS = 0
 DRIFT_MULTIPLICATIVE_NOISE = 1
 DRIFT_ORNSTEIN_UHLENBECK = 2
+DRIFT_CODE = 3
 
 FLAG_STOP_ON_ERROR = 4
 FLAG_LITERAL_REDIFFUSION = 8
@@ -71,6 +72,9 @@ class ModelDesc(C.Structure):
         ("field_dy", C.POINTER(C.c_float)),
         ("field_rx", C.POINTER(C.c_float)),
         ("field_ry", C.POINTER(C.c_float)),
+        ("code_defines", C.c_char_p),
+        ("drift_code", C.c_char_p),
+        ("custom_laws", C.POINTER(C.c_char_p)),
     ]
 
 

@@ -34,6 +34,33 @@ def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
+# device headers that csrc/jit.cpp compiles again at run time (NVRTC), embedded as
+# string literals in the generated csrc/_jit_sources.h
+JIT_HEADERS = [("common.cuh", os.path.join(CSRC, "common.cuh")),
+               ("stoch_device.cuh", os.path.join(CSRC, "stoch_device.cuh")),
+               ("../../include/gpgmp_c.h", os.path.join(HERE, "..", "include", "gpgmp_c.h"))]
+JIT_OUT = os.path.join(CSRC, "_jit_sources.h")
+
+
+def _gen_jit_sources():
+    parts = ["// Generated by inchman_b200/build.py from the device headers; do not edit.",
+             "#pragma once", "namespace gpgmp {",
+             f"constexpr int kJitHeaderCount = {len(JIT_HEADERS)};",
+             "static const char* const kJitHeaderNames[] = {" +
+             ", ".join(f'"{n}"' for n, _ in JIT_HEADERS) + "};",
+             "static const char* const kJitHeaderSources[] = {"]
+    for name, path in JIT_HEADERS:
+        text = open(path).read()
+        if ")GPGMPJIT\"" in text:
+            raise RuntimeError(f"{path} contains the raw-string delimiter")
+        parts.append(f'R"GPGMPJIT({text})GPGMPJIT",')
+    parts += ["};", "}  // namespace gpgmp", ""]
+    out = "\n".join(parts)
+    if not os.path.exists(JIT_OUT) or open(JIT_OUT).read() != out:
+        with open(JIT_OUT, "w") as f:
+            f.write(out)
+
+
 def _deps_mtime():
     return max(os.path.getmtime(os.path.join(CSRC, f)) for f in os.listdir(CSRC)
                if f.endswith((".cuh", ".h")) or f.endswith((".cu", ".cpp")))
@@ -60,12 +87,14 @@ def build(clean: bool = False, verbose: bool = False) -> str:
     if clean and os.path.isdir(BUILD):
         shutil.rmtree(BUILD)
     os.makedirs(BUILD, exist_ok=True)
+    _gen_jit_sources()
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(_compile, srcs))
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
         return LIB
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    # NVRTC and the driver API are opened with dlopen on first use (csrc/jit.cpp)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -14,9 +14,13 @@
 //   binomial  chunked inversion of the pmf recurrence, (1-q)^m by binary powering
 //   Poisson   count of unit-rate exponential arrivals before lambda
 #pragma once
+#ifdef __CUDACC_RTC__
+#include "gpgmp_rtc_prelude.h"    // run-time compilation: fixed-width types and limits
+#else
 #include <cstdint>
 #include <climits>
 #include <cuda_runtime.h>
+#endif
 
 namespace gpgmp {
 

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include "kernels.h"
 #include "host_common.h"
+#include "jit.h"
 
 using namespace gpgmp;
 
@@ -33,6 +34,11 @@ struct gpgmp_solver {
     bool aqss = false;      // alpha-QSS reaction windows instead of RK4
     bool fpe = false;       // stochastic_inhomogeneous_fpe jump rates
     int ts_kind = 0;        // time step formula of the inhomogeneous solvers (TimestepKind)
+    // model code compiled at run time (jit.h): parameter defines, drift method,
+    // per-reaction custom propensity laws ("" = mass action)
+    std::string code_defines, drift_code;
+    std::vector<std::string> custom_laws;
+    JitFunction jit_ssa = nullptr, jit_drift = nullptr;
     // stochastic state: two buffers, per-species current index
     int32_t* d_buf[2] = {nullptr, nullptr};
     std::vector<int> cur;
@@ -157,8 +163,10 @@ int validate(const gpgmp_model_desc* m, int R) {
         if (m->drift_method == GPGMP_DRIFT_FIELD &&
             (!m->field_dx || !m->field_dy || !m->field_rx || !m->field_ry))
             return set_error(GPGMP_ERR_INVALID, "field drift method needs all four field arrays");
-        if (m->drift_method < GPGMP_DRIFT_FIELD || m->drift_method > GPGMP_DRIFT_ORNSTEIN_UHLENBECK)
+        if (m->drift_method < GPGMP_DRIFT_FIELD || m->drift_method > GPGMP_DRIFT_CODE)
             return set_error(GPGMP_ERR_UNSUPPORTED, "drift_method %d", m->drift_method);
+        if (m->drift_method == GPGMP_DRIFT_CODE && !m->drift_code)
+            return set_error(GPGMP_ERR_INVALID, "GPGMP_DRIFT_CODE needs drift_code");
         if (m->flags & 1) return set_error(GPGMP_ERR_UNSUPPORTED, "nonlinear diffusivity recompute");
     }
     return GPGMP_OK;
@@ -169,7 +177,22 @@ int validate(const gpgmp_model_desc* m, int R) {
 // the solver type).
 int inhom_init(gpgmp_solver* h) {
     const size_t n = h->area * h->g.S;
-    if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
+    if (h->m.drift_method == GPGMP_DRIFT_CODE) {
+        // the reference's generated inhomogeneous_computeDiffusionConstants_forSpecies_<id>
+        // kernels, run species after species on fields that start at zero
+        CK(cudaMemsetAsync(h->d_Dx, 0, n * sizeof(float), h->stream));
+        CK(cudaMemsetAsync(h->d_Dy, 0, n * sizeof(float), h->stream));
+        CK(cudaMemsetAsync(h->d_rx, 0, n * sizeof(float), h->stream));
+        CK(cudaMemsetAsync(h->d_ry, 0, n * sizeof(float), h->stream));
+        if (!h->jit_drift) {
+            int rc = jit_drift_kernel(h->code_defines, h->drift_code, &h->jit_drift);
+            if (rc) return rc;
+        }
+        const int32_t* st0 = h->deterministic ? nullptr : h->d_buf[h->cur.empty() ? 0 : h->cur[0]];
+        for (int s = 0; s < h->g.S; ++s)
+            CK(launch_drift_jit(h->jit_drift, h->g, s, h->m.physical_length, 0.f, h->d_Dx, h->d_Dy, h->d_rx, h->d_ry,
+                                st0, h->stream));
+    } else if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
         CK(cudaMemcpyAsync(h->d_Dx, h->m.field_dx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_Dy, h->m.field_dy, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_rx, h->m.field_rx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -200,6 +223,17 @@ int inhom_init(gpgmp_solver* h) {
     return GPGMP_OK;
 }
 
+// A drift method in code may read the counts (SP(i)->State): like the reference's
+// solver constructor, evaluate it on the initial state, i.e. again once the caller
+// has set the state.
+int refresh_code_fields(gpgmp_solver* h) {
+    if (!h->inhom || h->m.drift_method != GPGMP_DRIFT_CODE) return GPGMP_OK;
+    int rc = inhom_init(h);
+    if (rc) return rc;
+    for (int i = 0; i < h->g.S; ++i) h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
+    return GPGMP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -221,6 +255,19 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     if (model->num_reactions > 0) h->reactions.assign(model->reactions, model->reactions + model->num_reactions);
     h->m.diffusion = h->diffusion.data();
     h->m.reactions = h->reactions.empty() ? nullptr : h->reactions.data();
+    if (model->code_defines) h->code_defines = model->code_defines;
+    if (model->drift_code) h->drift_code = model->drift_code;
+    bool custom = false;
+    if (model->custom_laws) {
+        h->custom_laws.assign(model->num_reactions, std::string());
+        for (int r = 0; r < model->num_reactions; ++r)
+            if (model->custom_laws[r] && model->custom_laws[r][0]) {
+                h->custom_laws[r] = model->custom_laws[r];
+                custom = true;
+            }
+    }
+    h->m.code_defines = h->m.drift_code = nullptr;
+    h->m.custom_laws = nullptr;
     const int ty = model->solver_type;
     h->deterministic = ty == GPGMP_DETERMINISTIC_RK4 || ty == GPGMP_DETERMINISTIC_AQSS ||
                        ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_RK4 || ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
@@ -228,6 +275,18 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     h->aqss = ty == GPGMP_DETERMINISTIC_AQSS || ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
     h->fpe = ty == GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE;
     h->ts_kind = h->deterministic ? 2 : (h->fpe ? 1 : 0);
+    if (custom && h->deterministic) {
+        delete h;
+        return set_error(GPGMP_ERR_UNSUPPORTED, "custom propensity laws with a deterministic solver");
+    }
+    if (custom) {
+        // the reference generates its Gillespie kernel from the laws (Solver.cpp:843-905)
+        int rc2 = jit_ssa_kernel(h->code_defines, h->custom_laws, &h->jit_ssa);
+        if (rc2) {
+            delete h;
+            return rc2;
+        }
+    }
     h->g.W = model->width;
     h->g.H = model->height;
     h->g.S = model->num_species;
@@ -342,7 +401,7 @@ int gpgmp_set_state(gpgmp_solver* h, const void* host) {
         std::fill(h->cur.begin(), h->cur.end(), 0);
     }
     CK(cudaStreamSynchronize(h->stream));
-    return GPGMP_OK;
+    return refresh_code_fields(h);
 }
 
 int gpgmp_get_state(gpgmp_solver* h, void* host) {
@@ -370,7 +429,9 @@ int gpgmp_init_poisson(gpgmp_solver* h, const float* lambda) {
     if (h->deterministic) return set_error(GPGMP_ERR_UNSUPPORTED, "Poisson initial state is for stochastic solvers");
     CK(cudaMemcpyAsync(h->d_lambda, lambda, sizeof(float) * h->g.S, cudaMemcpyHostToDevice, h->stream));
     std::fill(h->cur.begin(), h->cur.end(), 0);
-    return after_launch(h, launch_init_poisson(h->g, planes_of(h), h->seed, h->d_lambda, h->stream));
+    int rc = after_launch(h, launch_init_poisson(h->g, planes_of(h), h->seed, h->d_lambda, h->stream));
+    if (rc) return rc;
+    return refresh_code_fields(h);
 }
 
 int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
@@ -384,8 +445,11 @@ int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
         return after_launch(h, launch_rk4(h->g, h->d_fbuf[h->fcur], h->d_reactions, (int)h->reactions.size(), deltat,
                                           h->stream));
     }
-    int rc = after_launch(h, launch_ssa(h->g, planes_of(h), h->d_reactions, (int)h->reactions.size(), h->seed,
-                                        (uint32_t)*seed, deltat, h->d_status, h->stream));
+    int rc = after_launch(h, h->jit_ssa ? launch_ssa_jit(h->jit_ssa, h->g, planes_of(h), h->d_reactions,
+                                                         (int)h->reactions.size(), h->seed, (uint32_t)*seed, deltat,
+                                                         h->d_status, h->stream)
+                                        : launch_ssa(h->g, planes_of(h), h->d_reactions, (int)h->reactions.size(),
+                                                     h->seed, (uint32_t)*seed, deltat, h->d_status, h->stream));
     (*seed)++;
     return rc;
 }

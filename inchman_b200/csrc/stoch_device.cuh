@@ -32,14 +32,23 @@ __device__ __forceinline__ float hazard(const gpgmp_reaction& rc, const int* x, 
     return v;
 }
 
+// The mass-action hazard as a functor; a model with custom propensity laws supplies
+// its own (compiled at run time, csrc/jit.cpp).
+struct MassActionHazard {
+    __device__ __forceinline__ float operator()(const gpgmp_reaction* rt, int r, const int* x, int stride) const {
+        return hazard(rt[r], x, stride);
+    }
+};
+
 // Runs one SSA window on the counts x[s * stride]; returns a GPGMP_SIM_* bit or 0.
-__device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x, int stride, Stream& st,
-                                        float window) {
+template <class HZ>
+__device__ __forceinline__ int ssa_cell_h(const gpgmp_reaction* rt, int R, int* x, int stride, Stream& st,
+                                          float window, const HZ& hz) {
     float t = 0.0f;
     int events = 0;
     for (;;) {
         float h0 = 0.0f;
-        for (int r = 0; r < R; ++r) h0 = h0 + hazard(rt[r], x, stride);
+        for (int r = 0; r < R; ++r) h0 = h0 + hz(rt, r, x, stride);
         if (!(h0 > 0.0f)) return 0;
         const uint32_t a = st.next(), b = st.next();
         const float r1 = u01_open0(a);
@@ -51,7 +60,7 @@ __device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x,
         int j = -1;
         float hc = 0.0f;
         for (int r = 0; r < R; ++r) {
-            hc = hc + hazard(rt[r], x, stride);
+            hc = hc + hz(rt, r, x, stride);
             if (r2 < hc) { j = r; break; }
         }
         if (j >= 0) {
@@ -64,7 +73,10 @@ __device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x,
         if (++events >= SSA_EVENT_CAP) return SIM_EVENT_CAP;
     }
 }
-
+__device__ __forceinline__ int ssa_cell(const gpgmp_reaction* rt, int R, int* x, int stride, Stream& st,
+                                        float window) {
+    return ssa_cell_h(rt, R, x, stride, st, window, MassActionHazard{});
+}
 
 // Dependency masks of the incremental SSA: bit q of deps[j * 4 + q / 32] is set when
 // reaction j changes the count of a species that reaction q consumes, i.e. when q's

@@ -41,8 +41,11 @@ class Reaction:
 class Compartment:
     """Inclusive rectangle [x0, x1] x [y0, y1] with an initial amount of one species.
 
-    distribution: "homogeneous" (the amount in every cell), "random" (the amount
-    spread over the cells uniformly at random) or "linearx" (DiffusionModel.cpp:568-723)."""
+    distribution (DiffusionModel.cpp:568-723): "homogeneous" spreads the amount
+    evenly, amount // area per cell plus one more in the cells whose grid offset
+    y*width + x is below amount % area (the reference's rule); "random" places each
+    particle in a uniformly chosen cell; "linearx" a ramp in x with slope
+    2 amount / ((nx - 1) nx ny), nx = x1 - x0, ny = y1 - y0, rounded half away from 0."""
     species: str
     x0: int
     y0: int
@@ -74,6 +77,12 @@ class DiffusionModel:
     field_dy: Optional[np.ndarray] = None
     field_rx: Optional[np.ndarray] = None
     field_ry: Optional[np.ndarray] = None
+    # model code compiled at run time (gpgmp_model_desc.code_defines / drift_code /
+    # custom_laws): parameter defines, the drift/diffusivity method for
+    # DRIFT_CODE, and per reaction a C propensity expression in X(i) or None
+    code_defines: Optional[str] = None
+    drift_code: Optional[str] = None
+    custom_laws: Optional[List[Optional[str]]] = None
 
     # -- builders (DiffusionModel.cpp:426-493) --------------------------------
     def add_species(self, id: str, diffusion: float = 0.0, initial: float = 0.0) -> "DiffusionModel":
@@ -152,6 +161,20 @@ class DiffusionModel:
                     raise ValueError(f"{name} must hold [species][height][width] values")
                 keep.append(a)
                 setattr(d, name, a.ctypes.data_as(C.POINTER(C.c_float)))
+        if self.code_defines:
+            b = self.code_defines.encode()
+            keep.append(b)
+            d.code_defines = b
+        if self.drift_code is not None:
+            b = self.drift_code.encode()
+            keep.append(b)
+            d.drift_code = b
+        if self.custom_laws is not None:
+            if len(self.custom_laws) != len(self.reactions):
+                raise ValueError("custom_laws needs one entry (or None) per reaction")
+            laws = (C.c_char_p * max(1, len(self.reactions)))(*[(l.encode() if l else None) for l in self.custom_laws])
+            keep.append(laws)
+            d.custom_laws = C.cast(laws, C.POINTER(C.c_char_p))
         return d, keep
 
     # -- initial state (DiffusionModel.cpp:568-723) ------------------------------
@@ -164,16 +187,23 @@ class DiffusionModel:
                 s = self.species_index(comp.species)
                 ys, xs = slice(comp.y0, comp.y1 + 1), slice(comp.x0, comp.x1 + 1)
                 ncell = (comp.y1 - comp.y0 + 1) * (comp.x1 - comp.x0 + 1)
+                amount = int(comp.amount)
                 if comp.distribution == "homogeneous":
-                    out[r, s, ys, xs] += int(comp.amount)
+                    per, rem = divmod(amount, ncell)
+                    yy, xx = np.mgrid[comp.y0:comp.y1 + 1, comp.x0:comp.x1 + 1]
+                    out[r, s, ys, xs] += (per + ((yy * W + xx) < rem)).astype(np.int32)
                 elif comp.distribution == "random":
-                    cells = rng.integers(0, ncell, size=int(comp.amount))
+                    cells = rng.integers(0, ncell, size=amount)
                     counts = np.bincount(cells, minlength=ncell).reshape(comp.y1 - comp.y0 + 1, -1)
                     out[r, s, ys, xs] += counts.astype(np.int32)
                 elif comp.distribution == "linearx":
-                    nx = comp.x1 - comp.x0 + 1
-                    ramp = np.linspace(0.0, 1.0, nx) * comp.amount
-                    out[r, s, ys, xs] += ramp.astype(np.int32)[None, :]
+                    nx, ny = comp.x1 - comp.x0, comp.y1 - comp.y0
+                    if nx < 2 or ny < 1:
+                        raise ValueError("linearx needs a compartment at least 3 wide and 2 high")
+                    coeff = np.float32(2.0 * amount / ((nx - 1) * nx * ny))
+                    v = coeff * np.arange(comp.x1 - comp.x0 + 1, dtype=np.float32)
+                    ramp = (np.sign(v) * np.floor(np.abs(v) + 0.5)).astype(np.int32)
+                    out[r, s, ys, xs] += ramp[None, :]
                 else:
                     raise ValueError(comp.distribution)
         return out

@@ -23,8 +23,10 @@
  */
 #ifndef GPGMP_C_H
 #define GPGMP_C_H
+#ifndef __CUDACC_RTC__
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -57,6 +59,7 @@ extern "C" {
 #define GPGMP_DRIFT_HOMOGENEOUS 0          /* params: diffX, diffY, driftX, driftY */
 #define GPGMP_DRIFT_MULTIPLICATIVE_NOISE 1 /* params: sigmaX, sigmaY, muX, muY */
 #define GPGMP_DRIFT_ORNSTEIN_UHLENBECK 2   /* params: diffX, diffY, gammaXX, gammaXY, gammaYX, gammaYY */
+#define GPGMP_DRIFT_CODE 3                 /* gpgmp_model_desc.drift_code, compiled at run time */
 
 /* gpgmp_model_desc.flags */
 #define GPGMP_FLAG_STOP_ON_ERROR 4         /* end a realisation's event loop once its status is set */
@@ -104,6 +107,22 @@ typedef struct gpgmp_model_desc {
     const float* field_dy;            /* [S][H][W] diffusivity y */
     const float* field_rx;            /* [S][H][W] drift x */
     const float* field_ry;            /* [S][H][W] drift y */
+    /* Model code compiled at run time for the device (NVRTC), as the reference
+     * generates its kernels from the model (Solver.cpp:643-777, 843-905).  NULL where
+     * unused.
+     *  code_defines: preprocessor lines (e.g. parameter values) put before all code;
+     *  drift_code:   statements of the drift/diffusivity method, GPGMP_DRIFT_CODE:
+     *                they set All->DiffusivityX/Y, All->DriftX/Y of the species being
+     *                computed and may read SP(i)->... of species i (State, MeanX,
+     *                DiffusivityX/Y, DriftX/Y), GridX, GridY, PhysicalX, PhysicalY,
+     *                PhysicalModelWidth/Height, PhysicalCellWidth/Height,
+     *                GridModelWidth/Height and PhysicalSimTime; type Real = float;
+     *  custom_laws:  num_reactions entries, each a C expression for the reaction's
+     *                propensity in X(i) (the count of species i as float), or NULL
+     *                for the mass-action hazard. */
+    const char* code_defines;
+    const char* drift_code;
+    const char* const* custom_laws;
 } gpgmp_model_desc;
 
 typedef struct gpgmp_solver gpgmp_solver;

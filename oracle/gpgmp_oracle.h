@@ -42,8 +42,10 @@ typedef struct orc_model {
     int32_t max_steps;
     int32_t boundary_mask[4];   /* x-, x+, y-, y+ : 0 reflecting, 1 absorbing */
     int32_t source_mask[4];
-    int32_t solver_type;        /* 0 stochastic homogeneous, 1 stochastic inhomogeneous, 2 deterministic RK4 */
-    int32_t drift_method;       /* -1 field arrays, 0 homogeneous, 1 multiplicative noise, 2 OU, 3 nonlinear */
+    int32_t solver_type;        /* 0 stochastic homogeneous, 1 stochastic inhomogeneous, 2 deterministic RK4,
+                                   3 stochastic inhomogeneous FPE, 4 deterministic alpha-QSS, 5/6 deterministic
+                                   inhomogeneous RK4 / alpha-QSS */
+    int32_t drift_method;       /* -1 field arrays, 0 homogeneous, 1 multiplicative noise, 2 OU, 3 run-time code */
     int32_t flags;              /* bit 0 nonlinear diffusivity (recompute after sweeps), bit 1 compute moments */
     float   drift_params[8];
     const float* diffusion;            /* [S] */
@@ -52,6 +54,9 @@ typedef struct orc_model {
     const float* field_dy;
     const float* field_rx;
     const float* field_ry;
+    const char* code_defines;          /* run-time model code (the product compiles it with NVRTC; */
+    const char* drift_code;            /* the oracle takes custom hazards through orc_set_custom_hazard) */
+    const char* const* custom_laws;
 } orc_model;
 
 /* ---- generators and elementary functions ---------------------------------- */
@@ -89,6 +94,7 @@ void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t s
                            uint32_t step_seed, float dt, const float* dfield, const float* rfield);
 float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float* dfield, const float* rfield);
 void orc_rep_diffusivity_drift(const orc_model* m, int species, float* dx, float* dy, float* rx, float* ry);
+void orc_set_custom_hazard(float (*fn)(int r, const int32_t* x));
 int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
                   int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots,
                   int64_t* steps, int32_t* status);

@@ -75,6 +75,7 @@ def orc():
             "orc_det_sweep": (None, [vp, vp, vp, C.c_int, C.c_int, f32, f32, vp, vp]),
             "orc_aqss_cell": (C.c_int, [vp, vp, f32, C.c_int]),
             "orc_aqss": (C.c_int, [vp, vp, f32, C.c_int]),
+            "orc_set_custom_hazard": (None, [vp]),
             "orc_sort_pairs_u32": (None, [vp, vp, i64]),
             "orc_exclusive_scan_u32": (None, [vp, vp, i64]),
             "orc_cell_indices_ref": (None, [vp, i64, i64, vp, vp]),
@@ -152,3 +153,17 @@ def init_poisson(W, H, S, R, seed, lam):
     lam = np.ascontiguousarray(lam, dtype=np.float32)
     orc().orc_rep_init_poisson(W, H, S, R, seed, ptr(lam), ptr(out))
     return out
+
+
+HAZARD_FN = C.CFUNCTYPE(C.c_float, C.c_int, C.POINTER(C.c_int32))
+
+
+def set_custom_hazard(fn):
+    """fn(r, counts) -> float32 hazard for the replay's SSA (None: mass action).
+    Returns the ctypes callback object, which the caller keeps alive while in use."""
+    if fn is None:
+        orc().orc_set_custom_hazard(None)
+        return None
+    cb = HAZARD_FN(lambda r, x: float(fn(r, x)))
+    orc().orc_set_custom_hazard(C.cast(cb, C.c_void_p))
+    return cb

@@ -64,6 +64,13 @@ static int rep_apply(const orc_reaction* rc, int32_t* x) {
     return 0;
 }
 
+/* Custom propensity laws: the product compiles them into its SSA kernel at run time;
+ * the replay takes them from the test as a callback (r, counts) -> hazard that
+ * evaluates the same float operations.  NULL restores the mass-action hazard. */
+typedef float (*orc_hazard_fn)(int r, const int32_t* x);
+static orc_hazard_fn g_custom_hazard = NULL;
+void orc_set_custom_hazard(orc_hazard_fn fn) { g_custom_hazard = fn; }
+
 static int rep_ssa_cell(const orc_model* m, int32_t* x, orc_stream* st, float window) {
     const int R = m->num_reactions;
     float H[128];
@@ -71,7 +78,10 @@ static int rep_ssa_cell(const orc_model* m, int32_t* x, orc_stream* st, float wi
     int events = 0;
     for (;;) {
         float h0 = 0.0f;
-        for (int r = 0; r < R; ++r) { h0 = h0 + rep_hazard(&m->reactions[r], x); H[r] = h0; }
+        for (int r = 0; r < R; ++r) {
+            h0 = h0 + (g_custom_hazard ? g_custom_hazard(r, x) : rep_hazard(&m->reactions[r], x));
+            H[r] = h0;
+        }
         if (!(h0 > 0.0f)) break;
         uint32_t a = orc_stream_next(st), b = orc_stream_next(st);
         float r1 = orc_u01_open0(a);

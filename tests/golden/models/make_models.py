@@ -1,0 +1,121 @@
+"""Writes the annotated-SBML model fixtures of tests/golden/models/ (our own small
+models in the file format of the reference's editor: SBML level 2 with Inchman
+annotations, as InchmanDiffusionModel.cpp reads it).  Run from the repository root:
+    python tests/golden/models/make_models.py
+"""
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+IMNS = "http://www.csse.monash.edu.au/~berndm/inchman"
+MML = "http://www.w3.org/1998/Math/MathML"
+
+
+def num(v):
+    return f'<math:math xmlns:math="{MML}"><math:cn>{v}</math:cn></math:math>'
+
+
+def document(name, solver, W, L, time, out, params, comps, species, reactions, method=""):
+    ps = "\n".join(f'      <parameter id="{k}" value="{v}"><annotation><im:parameter xmlns:im="{IMNS}" '
+                   f'type="float" domain="single"/></annotation></parameter>' for k, v in params.items())
+    cs = "\n".join(f'      <compartment id="{cid}"><annotation><im:compartment xmlns:im="{IMNS}">'
+                   f'<im:x>{num(x)}</im:x><im:y>{num(y)}</im:y><im:width>{num(w)}</im:width>'
+                   f'<im:height>{num(h)}</im:height></im:compartment></annotation></compartment>'
+                   for cid, (x, y, w, h) in comps.items())
+    ss = []
+    for sid, (D, amounts) in species.items():
+        cp = "".join(f'<im:compartmentParameters compartment="{c}"><im:initialAmount>{num(a)}</im:initialAmount>'
+                     f'</im:compartmentParameters>' for c, a in amounts.items())
+        ss.append(f'      <species id="{sid}" compartment="World"><annotation><im:species xmlns:im="{IMNS}">'
+                  f'<im:diffusionConstant>{num(D)}</im:diffusionConstant>'
+                  f'<im:listOfCompartmentParameters>{cp}</im:listOfCompartmentParameters>'
+                  f'</im:species></annotation></species>')
+    rs = []
+    for rid, (re_, pr, law) in reactions.items():
+        rl = "".join(f'<speciesReference species="{s}" stoichiometry="{n}"/>' for s, n in re_.items())
+        pl = "".join(f'<speciesReference species="{s}" stoichiometry="{n}"/>' for s, n in pr.items())
+        rs.append(f'      <reaction id="{rid}"><annotation><im:reaction xmlns:im="{IMNS}">'
+                  f'<im:listOfCompartmentParameters><im:compartmentParameters compartment="World"><im:isAllowed>'
+                  f'<math xmlns="{MML}"><ci>true</ci></math></im:isAllowed></im:compartmentParameters>'
+                  f'</im:listOfCompartmentParameters></im:reaction></annotation>'
+                  f'<listOfReactants>{rl}</listOfReactants><listOfProducts>{pl}</listOfProducts>'
+                  f'<kineticLaw><math xmlns="{MML}">{law}</math></kineticLaw></reaction>')
+    return f'''<?xml version="1.0" encoding="UTF-8"?>
+<sbml xmlns="http://www.sbml.org/sbml/level2" level="2" version="1">
+<annotation><im:sbml xmlns:im="{IMNS}">
+  <im:solver>{solver}</im:solver>
+  <im:runs>{num(1)}</im:runs>
+  <im:time>{num(time)}</im:time>
+  <im:outputInterval>{num(out)}</im:outputInterval>
+  <im:init type="python"><im:script><![CDATA[]]></im:script></im:init>
+  <im:events type="python"><im:script><![CDATA[]]></im:script><im:listOfTimeStamps/></im:events>
+  <im:driftDiffusivity nonLinear="false" computeMoments=""><im:method><![CDATA[{method}]]></im:method></im:driftDiffusivity>
+</im:sbml></annotation>
+  <model name="{name}">
+<annotation><im:model xmlns:im="{IMNS}"><im:gridWidth>{num(W)}</im:gridWidth><im:gridHeight>{num(W)}</im:gridHeight>
+<im:physicalWidth>{num(L)}</im:physicalWidth><im:physicalHeight>{num(L)}</im:physicalHeight></im:model></annotation>
+    <listOfCompartments>
+{cs}
+    </listOfCompartments>
+    <listOfSpecies>
+{chr(10).join(ss)}
+    </listOfSpecies>
+    <listOfParameters>
+{ps}
+    </listOfParameters>
+    <listOfReactions>
+{chr(10).join(rs)}
+    </listOfReactions>
+  </model>
+</sbml>
+'''
+
+
+def times(*xs):
+    return "<apply><times/>" + "".join(xs) + "</apply>"
+
+
+def ci(n):
+    return f"<ci>{n}</ci>"
+
+
+def cn(v):
+    return f"<cn>{v}</cn>"
+
+
+def minus(a, b):
+    return f"<apply><minus/>{a}{b}</apply>"
+
+
+def plus(a, b):
+    return f"<apply><plus/>{a}{b}</apply>"
+
+
+def divide(a, b):
+    return f"<apply><divide/>{a}{b}</apply>"
+
+
+def main():
+    # A+B annihilation with drift, 2A annihilation, sources; mass-action laws
+    ab = document(
+        "AB drift", "stochastic_inhomogeneous", 24, 12.0, 0.3, 0.1, {"k1": 0.002, "k2": 0.02, "k3": 1.5},
+        {"World": (0, 0, 24, 24), "Left": (0, 0, 8, 24)},
+        {"A": (1.0, {"World": 24 * 24 * 20 + 7}), "B": (0.5, {"Left": 3000})},
+        {"AA": ({"A": 2}, {}, times(times(ci("k1"), ci("A")), minus(ci("A"), cn("1.0")))),
+         "AB": ({"A": 1, "B": 1}, {}, times(times(ci("k2"), ci("A")), ci("B"))),
+         "Asrc": ({}, {"A": 1}, ci("k3"))},
+        method="All->DiffusivityX = 1.;\nAll->DiffusivityY = 0.5;\nAll->DriftX = 0.4;\nB->DriftX = -0.2;\n"
+               "All->DriftY = -0.1;")
+    # saturating production (a custom law): 0 -> P at vmax S / (km + S), S -> 0
+    mm = document(
+        "Saturating production", "stochastic_homogeneous", 8, 8.0, 0.5, 0.25, {"vmax": 40.0, "km": 25.0, "kd": 0.3},
+        {"World": (0, 0, 8, 8)},
+        {"S": (0.5, {"World": 64 * 30}), "P": (0.2, {})},
+        {"prod": ({}, {"P": 1}, divide(times(ci("vmax"), ci("S")), plus(ci("km"), ci("S")))),
+         "deg": ({"S": 1}, {}, times(ci("kd"), ci("S")))})
+    for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm)):
+        with open(os.path.join(HERE, name), "w") as f:
+            f.write(text)
+
+
+if __name__ == "__main__":
+    main()
