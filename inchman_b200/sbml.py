@@ -88,7 +88,11 @@ def mathml(e: ET.Element):
             return ("num", mant * 10.0 ** ex)
         return ("num", float((e.text or "").strip()))
     if tag == "ci":
-        return ("id", (e.text or "").strip())
+        name = (e.text or "").strip()
+        try:
+            return ("num", float(name))          # editors write some numbers as <ci>
+        except ValueError:
+            return ("id", name)
     if tag in ("true", "false"):
         return ("num", 1.0 if tag == "true" else 0.0)
     if tag in ("exponentiale",):
