@@ -30,6 +30,7 @@ constexpr uint32_t PH_DIFF = 0x03000000u;
 constexpr uint32_t PH_SOURCE = 0x04000000u;
 constexpr uint32_t PH_PART = 0x05000000u;
 constexpr uint32_t PH_PAIR = 0x06000000u;
+constexpr uint32_t PH_POP = 0x07000000u;    // population bookkeeping (individuals)
 
 constexpr int SSA_EVENT_CAP = 1 << 22;
 constexpr int SIM_EVENT_CAP = 1;

@@ -7,6 +7,7 @@ tensors of the same bits):
     sort_pairs_u32(keys, vals, bits) -> stable sort by the low `bits` key bits
     cell_offsets(sorted_keys, ncells) -> (start, count)
     cell_indices(start, count)        -> the reference's (left, right) ranges
+    maintain_population(...)          -> the individual list brought to new counts
 Particles(capacity, grid, ...) wraps the move/bin/react/compact step.
 """
 from __future__ import annotations
@@ -28,6 +29,9 @@ _SIGS = {
     "gpgmp_cell_offsets": (C.c_int, [vp, i64, i64, vp, vp, vp, C.c_size_t, vp]),
     "gpgmp_cell_indices": (C.c_int, [vp, vp, i64, vp, vp, vp]),
     "gpgmp_scratch_status": (C.c_int, [vp, i32, i64, i32, P(i32)]),
+    "gpgmp_population_scratch_bytes": (C.c_int, [i64, i64, P(C.c_size_t)]),
+    "gpgmp_population_maintain": (C.c_int, [vp, vp, i64, vp, vp, vp, i64, vp, i64, u32, u32, vp, vp, i64, vp, i64,
+                                            vp, P(i64), P(i64), vp, C.c_size_t, vp]),
     "gpgmp_particles_create": (C.c_int, [i64, i32, f32, f32, f32, f32, f32, u32, P(vp)]),
     "gpgmp_particles_destroy": (C.c_int, [vp]),
     "gpgmp_particles_set_stream": (C.c_int, [vp, vp]),
@@ -122,6 +126,32 @@ def cell_indices(start, count):
     right = torch.empty_like(start)
     _call("gpgmp_cell_indices", _ptr(start), _ptr(count), start.numel(), _ptr(left), _ptr(right), _stream())
     return left, right
+
+
+def maintain_population(keys, ids, start, count, goal, pool, seed: int, step: int, capacity: int = None,
+                        pool_capacity: int = None):
+    """IndividualSolver::maintainPopulation: rebuild the cell-sorted individual list
+    (keys = cell, ids, with start / count from cell_offsets) so that cell c holds
+    goal[c] individuals.  Returns (keys, ids, start, pool) of the new list and pool
+    (int32 tensors of uint32 bits; counts are goal)."""
+    import torch
+    dev = goal.device
+    n, ncells, npool = keys.numel(), goal.numel(), pool.numel()
+    cap = capacity if capacity is not None else n + npool
+    pcap = pool_capacity if pool_capacity is not None else n + npool
+    b = C.c_size_t(0)
+    _call("gpgmp_population_scratch_bytes", n, ncells, C.byref(b))
+    scratch = torch.empty(max(1, b.value), dtype=torch.uint8, device=dev)
+    ko = torch.empty(max(1, cap), dtype=torch.int32, device=dev)
+    io = torch.empty_like(ko)
+    po = torch.empty(max(1, pcap), dtype=torch.int32, device=dev)
+    so = torch.empty(ncells, dtype=torch.int32, device=dev)
+    na, npo = C.c_int64(0), C.c_int64(0)
+    _call("gpgmp_population_maintain", _ptr(keys) if n else None, _ptr(ids) if n else None, n, _ptr(start),
+          _ptr(count), _ptr(goal), ncells, _ptr(pool) if npool else None, npool, seed & 0xFFFFFFFF,
+          step & 0xFFFFFFFF, _ptr(ko), _ptr(io), cap, _ptr(po), pcap, _ptr(so), C.byref(na), C.byref(npo),
+          _ptr(scratch), scratch.numel(), _stream())
+    return ko[:na.value], io[:na.value], so, po[:npo.value]
 
 
 class Particles:

@@ -242,6 +242,29 @@ int gpgmp_cell_offsets(const uint32_t* sorted_keys, int64_t n, int64_t ncells, u
 int gpgmp_cell_indices(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left, uint32_t* right,
                        void* stream);
 int gpgmp_scratch_status(const void* scratch, int32_t kind, int64_t n, int32_t key_bits, int32_t* status);
+
+/* ---- individual particles: population bookkeeping -------------------------------
+ * IndividualSolver::maintainPopulation (IndividualSolver.cpp:458-671,
+ * IndividualSolver.cl:1017-1882, doc/source/individual.rst).  After a reaction window
+ * changed the per-cell counts goal[c], the cell-sorted list (keys = cell index, ids)
+ * with its cell_start / cell_count (gpgmp_cell_offsets) is rebuilt so that cell c
+ * holds goal[c] individuals: a cell's surplus is removed, chosen uniformly without
+ * replacement by a random stream keyed by (seed, step, cell), and the removed ids are
+ * put at the front of the new pool in list order, followed by the unused old pool;
+ * a cell's missing individuals take ids from the front of the old pool, in cell
+ * order, and come first in their cell, before its survivors (in their old order).
+ * Outputs: keys_out / ids_out (n_active_out entries, at most capacity_out), pool_out
+ * (n_pool_out ids, at most pool_capacity), start_out (optional, ncells entries: the
+ * new cell starts; the new counts are goal).  Device pointers; returns after the
+ * work is done (the totals are read back).  GPGMP_ERR_INVALID when the pool has
+ * fewer free ids than births or an output is too small. */
+int gpgmp_population_scratch_bytes(int64_t n_active, int64_t ncells, size_t* bytes);
+int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n_active,
+                              const uint32_t* cell_start, const uint32_t* cell_count, const int32_t* goal,
+                              int64_t ncells, const uint32_t* pool, int64_t n_pool, uint32_t seed, uint32_t step,
+                              uint32_t* keys_out, uint32_t* ids_out, int64_t capacity_out, uint32_t* pool_out,
+                              int64_t pool_capacity, uint32_t* start_out, int64_t* n_active_out,
+                              int64_t* n_pool_out, void* scratch, size_t scratch_bytes, void* stream);
 /* gpgmp_exclusive_scan_u32 for callers that may not allocate device memory: code
  * whose device memory is owned and accounted by another allocator (a framework's
  * memory pool), or that cannot take cudaMalloc's implicit synchronisation or its

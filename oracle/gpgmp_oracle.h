@@ -118,6 +118,10 @@ int orc_aqss(const orc_model* m, float* state, float dtg, int literal);
 void orc_sort_pairs_u32(uint32_t* keys, uint32_t* vals, int64_t n);
 void orc_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n);
 void orc_cell_indices_ref(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* left, uint32_t* right);
+int orc_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n, const uint32_t* start,
+                            const uint32_t* count, const int32_t* goal, int64_t ncells, const uint32_t* pool,
+                            int64_t npool, uint32_t seed, uint32_t step, uint32_t* keys_out, uint32_t* ids_out,
+                            uint32_t* pool_out, int64_t* n_out, int64_t* npool_out);
 void orc_cell_offsets(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count);
 int64_t orc_particles_run(int64_t n, float* px, float* py, uint8_t* species, int grid, float D, float vx, float vy,
                           float dt, float p_react, uint32_t seed, int step0, int nsteps);

@@ -76,6 +76,8 @@ def orc():
             "orc_aqss_cell": (C.c_int, [vp, vp, f32, C.c_int]),
             "orc_aqss": (C.c_int, [vp, vp, f32, C.c_int]),
             "orc_set_custom_hazard": (None, [vp]),
+            "orc_population_maintain": (C.c_int, [vp, vp, i64, vp, vp, vp, i64, vp, i64, u32, u32, vp, vp, vp,
+                                                  P(i64), P(i64)]),
             "orc_sort_pairs_u32": (None, [vp, vp, i64]),
             "orc_exclusive_scan_u32": (None, [vp, vp, i64]),
             "orc_cell_indices_ref": (None, [vp, i64, i64, vp, vp]),

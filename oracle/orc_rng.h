@@ -99,5 +99,6 @@ static inline uint32_t orc_stream_next(orc_stream* s) {
 #define ORC_PH_SOURCE 0x04000000u
 #define ORC_PH_PART   0x05000000u
 #define ORC_PH_PAIR   0x06000000u
+#define ORC_PH_POP    0x07000000u
 
 #endif

@@ -160,3 +160,48 @@ int64_t orc_particles_run(int64_t n, float* px, float* py, uint8_t* sp, int G, f
     free(keys); free(vals); free(start); free(count); free(alive); free(nx); free(ny); free(nsp);
     return n;
 }
+
+/* IndividualSolver::maintainPopulation (IndividualSolver.cpp:458-671,
+ * IndividualSolver.cl:1017-1882), restated as the CUDA path lays it out: per cell the
+ * surplus is chosen by selection sampling (candidate i taken with probability
+ * k_rem / (is - i), one Philox draw each, stream (seed, 0, step, cell, POP)); the new
+ * list has, per cell in order, the births (ids from the front of the pool) and then
+ * the survivors in their old order; the new pool is the removed ids in list order
+ * followed by the unused old pool.  Returns -1 if the pool is too small. */
+int orc_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n, const uint32_t* start,
+                            const uint32_t* count, const int32_t* goal, int64_t ncells, const uint32_t* pool,
+                            int64_t npool, uint32_t seed, uint32_t step, uint32_t* keys_out, uint32_t* ids_out,
+                            uint32_t* pool_out, int64_t* n_out, int64_t* npool_out) {
+    uint8_t* dead = (uint8_t*)calloc(n > 0 ? n : 1, 1);
+    int64_t births = 0;
+    for (int64_t c = 0; c < ncells; ++c) {
+        uint32_t is = count[c], g = goal[c] > 0 ? (uint32_t)goal[c] : 0u;
+        if (g > is) births += g - is;
+        if (is > g) {
+            orc_stream st;
+            orc_stream_init(&st, seed, 0u, step, (uint32_t)c, ORC_PH_POP);
+            uint32_t krem = is - g;
+            for (uint32_t i = 0; i < is && krem > 0; ++i) {
+                double u = (double)orc_stream_next(&st) * (1.0 / 4294967296.0);
+                if ((double)(is - i) * u < (double)krem) { dead[start[c] + i] = 1; --krem; }
+            }
+        }
+    }
+    if (births > npool) { free(dead); return -1; }
+    int64_t o = 0, b = 0, k = 0;
+    for (int64_t c = 0; c < ncells; ++c) {
+        uint32_t is = count[c], g = goal[c] > 0 ? (uint32_t)goal[c] : 0u;
+        for (uint32_t j = g > is ? g - is : 0; j > 0; --j) { keys_out[o] = (uint32_t)c; ids_out[o] = pool[b++]; ++o; }
+        for (uint32_t i = 0; i < is; ++i) {
+            int64_t q = start[c] + i;
+            if (!dead[q]) { keys_out[o] = (uint32_t)c; ids_out[o] = ids[q]; ++o; }
+        }
+    }
+    for (int64_t q = 0; q < n; ++q) if (dead[q]) pool_out[k++] = ids[q];
+    for (int64_t t = b; t < npool; ++t) pool_out[k++] = pool[t];
+    (void)keys;
+    *n_out = o;
+    *npool_out = k;
+    free(dead);
+    return 0;
+}
