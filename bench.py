@@ -167,6 +167,41 @@ def bench_gray_scott(args, rank, world):
     t_total = max_over_ranks(sum(per), world)
     value = cell_steps * args.steps * world / t_total
     t_launch = sum(per) / len(per)
+    # ---- batched: the nine solves of the central finite-difference check (base and
+    # +-h in F, k, Du, Dv), one 16-CTA cluster each in one launch, against the same
+    # nine solved one after another
+    h = 1e-3
+    members = [[cfg.F, cfg.k, cfg.Du, cfg.Dv, 0.0, 0.0]]
+    for q in range(4):
+        for sgn in (1.0, -1.0):
+            m_ = list(members[0])
+            m_[q] += sgn * h
+            members.append(m_)
+    B = len(members)
+    U0 = u0.unsqueeze(0).repeat(B, 1, 1).contiguous()
+    V0 = v0.unsqueeze(0).repeat(B, 1, 1).contiguous()
+    gs.forward_batch(U0, V0, p, member_params=members)
+    torch.cuda.synchronize()
+    flush_l2(l2)
+    ba, bb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ba.record(stream)
+    gs.forward_batch(U0, V0, p, member_params=members)
+    bb.record(stream)
+    torch.cuda.synchronize()
+    t_batch = ba.elapsed_time(bb) / 1e3
+    singles = [gs.GrayScottConfig(F=m_[0], k=m_[1], Du=m_[2], Dv=m_[3]).params() for m_ in members]
+    flush_l2(l2)
+    sa, sb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sa.record(stream)
+    for ps in singles:
+        gs.forward(u0, v0, ps)
+    sb.record(stream)
+    torch.cuda.synchronize()
+    t_plain9 = sa.elapsed_time(sb) / 1e3
+    batched = {"members": B, "what": "central FD check: base and +-1e-3 in F, k, Du, Dv",
+               "lattices_at_once": gs.batch_capacity(n),
+               "value": B * cell_steps / t_batch, "unit": "cell-steps/s", "seconds": t_batch,
+               "plain_seconds": t_plain9, "batched_over_plain": t_plain9 / t_batch}
     # ---- end to end through the C ABI with pinned host buffers
     pu = torch.from_numpy(u0h).pin_memory()
     pv = torch.from_numpy(v0h).pin_memory()
@@ -233,13 +268,14 @@ def bench_gray_scott(args, rank, world):
                    "l2": "flushed between timed iterations (256 MB write)",
                    "parallelism": f"replicas x{world}"},
         "adjoint_forward_ratio": ratio,
+        "batched": batched,
         "gradient_ms": t_grad * 1e3,
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": 2 * n * n * 4},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "note": "16 B/cell-step algorithmic; the lattice stays in cluster shared memory"},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps,   # one k_gs_forward_rr launch per timed solve
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1:

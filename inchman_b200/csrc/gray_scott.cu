@@ -21,6 +21,7 @@
 #include <cooperative_groups.h>
 #include <cstdint>
 #include <cstdio>
+#include <vector>
 #include <cuda_runtime.h>
 #include "gs_kernels.h"
 
@@ -675,7 +676,9 @@ cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, 
         size_t smem = 0;
         int wpc = p.variant > 10 ? p.variant - 10 : 0;
         const void* rk = rr_kernel(p.n, &wpc, p.vx != 0.0 || p.vy != 0.0, &smem);
-        if (rk) return launch_cluster<T>(rk, p.n, cl, smem, st, args, dim3(32 * wpc, 1, 1));
+        const GSArgs<float>* no_batch = nullptr;
+        void* rargs[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every, &no_batch};
+        if (rk) return launch_cluster<T>(rk, p.n, cl, smem, st, rargs, dim3(32 * wpc, 1, 1));
         if (p.variant != 0) return cudaErrorInvalidValue;
     }
     const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl);
@@ -704,6 +707,74 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     const size_t smem = smem_bytes<T>(p.n, cl) * (sizeof(T) == 4 ? 2 : 1);
     if (blk.x != 0 && ak && p.variant != 1) return launch_cluster<T>(ak, p.n, cl, smem, st, args, blk);
     return launch_cluster<T>((const void*)k_gs_adjoint<T>, p.n, cl, smem_bytes<T>(p.n, cl), st, args);
+}
+
+cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMember* members, const float* u0,
+                                 const float* v0, float* u, float* v, cudaStream_t st) {
+    if (batch <= 0 || !members) return cudaErrorInvalidValue;
+    bool drift = false;
+    std::vector<GSArgs<float>> h(batch);
+    for (int b = 0; b < batch; ++b) {
+        const GSBatchMember& m = members[b];
+        h[b] = GSArgs<float>{p.n, p.steps, (float)m.F, (float)m.k, (float)m.Du, (float)m.Dv, (float)m.vx, (float)m.vy,
+                             (float)p.dt};
+        drift = drift || m.vx != 0.0 || m.vy != 0.0;
+    }
+    size_t smem = 0;
+    int wpc = p.variant > 10 ? p.variant - 10 : 0;
+    const void* rk = rr_kernel(p.n, &wpc, drift, &smem);
+    if (!rk) return cudaErrorInvalidValue;
+    GSArgs<float>* d = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d, sizeof(GSArgs<float>) * batch, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(d, h.data(), sizeof(GSArgs<float>) * batch, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        GSArgs<float> a = h[0];
+        float* no_trace = nullptr;
+        int every = 1;
+        void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &no_trace, &every, &d};
+        e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(rk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(kRRCluster * batch, 1, 1);
+            cfg.blockDim = dim3(32 * wpc, 1, 1);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = kRRCluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            e = cudaLaunchKernelExC(&cfg, rk, args);
+        }
+    }
+    cudaError_t e2 = cudaFreeAsync(d, st);
+    return e != cudaSuccess ? e : e2;
+}
+
+cudaError_t gs_batch_capacity(int n, int* clusters) {
+    size_t smem = 0;
+    int wpc = 0;
+    const void* rk = rr_kernel(n, &wpc, false, &smem);
+    if (!rk) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(rk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kRRCluster, 1, 1);
+    cfg.blockDim = dim3(32 * wpc, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kRRCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(clusters, rk, &cfg);
 }
 
 cudaError_t gs_forward_status(int* out, bool clear) {

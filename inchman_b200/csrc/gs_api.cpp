@@ -190,6 +190,36 @@ int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* ck, const doubl
     return adjoint<double>(p, ck, lu, lv, gu, gv, grad6, work, stream);
 }
 
+int gpgmp_gs_forward_batch_f32(const gpgmp_gs_params* p, int32_t batch, const double* member_params,
+                               const float* u0, const float* v0, float* u, float* v, void* stream) {
+    int rc = check(p, 4);
+    if (rc) return rc;
+    if (batch <= 0 || !u0 || !v0 || !u || !v) return set_error(GPGMP_ERR_INVALID, "bad argument");
+    if ((p->cluster != 0 && p->cluster != 16) || (p->variant != 0 && p->variant != 3 && p->variant <= 10))
+        return set_error(GPGMP_ERR_UNSUPPORTED, "batched solves use the register-resident kernel");
+    std::vector<GSBatchMember> m(batch);
+    for (int b = 0; b < batch; ++b) {
+        const double* q = member_params ? member_params + 6 * (size_t)b : nullptr;
+        m[b] = GSBatchMember{q ? q[0] : p->F, q ? q[1] : p->k, q ? q[2] : p->Du, q ? q[3] : p->Dv,
+                             q ? q[4] : p->vx, q ? q[5] : p->vy};
+    }
+    cudaError_t e = gs_forward_batch_f32(to_params(p), batch, m.data(), u0, v0, u, v, (cudaStream_t)stream);
+    if (e == cudaErrorInvalidValue)
+        return set_error(GPGMP_ERR_UNSUPPORTED, "lattice %d has no register-resident kernel", p->n);
+    CK(e);
+    return GPGMP_OK;
+}
+
+int gpgmp_gs_batch_capacity(int32_t n, int32_t* lattices) {
+    if (!lattices) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    int c = 0;
+    cudaError_t e = gs_batch_capacity(n, &c);
+    if (e == cudaErrorInvalidValue) return set_error(GPGMP_ERR_UNSUPPORTED, "lattice %d", n);
+    CK(e);
+    *lattices = c;
+    return GPGMP_OK;
+}
+
 int gpgmp_gs_status(int32_t* flags) {
     if (!flags) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     CK(cudaDeviceSynchronize());

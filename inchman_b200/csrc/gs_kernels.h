@@ -13,6 +13,20 @@ struct GSParams {
                    // 3 register-resident (float32), 10 + w register-resident with w warps per CTA
 };
 
+// per-lattice parameters of a batched forward solve
+struct GSBatchMember {
+    double F, k, Du, Dv, vx, vy;
+};
+// batch independent float32 n x n lattices (u0/v0/u/v: [batch][n][n]) with their own
+// parameters (p.n, p.steps, p.dt shared), one 16-CTA cluster each, in one launch of
+// the register-resident kernel
+cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMember* members, const float* u0,
+                                 const float* v0, float* u, float* v, cudaStream_t st);
+
+// how many lattices of side n a batched launch runs at the same time on this device
+// (16-CTA clusters that fit at once)
+cudaError_t gs_batch_capacity(int n, int* clusters);
+
 // reads (and with clear, resets) the device word that the register-resident forward
 // kernel sets when one of its bounded waits gave up; synchronous
 cudaError_t gs_forward_status(int* out, bool clear);

@@ -276,10 +276,20 @@ __device__ __forceinline__ void rr_step(const RRCtx<N, WPC>& c, const GSCoef2& k
 template <int N, int WPC, int DRIFT>
 __global__ void __launch_bounds__(32 * WPC, 1)
     k_gs_forward_rr(GSArgs<float> a, const float* __restrict__ u0, const float* __restrict__ v0,
-                    float* __restrict__ uo, float* __restrict__ vo, float* __restrict__ trace, int trace_every) {
+                    float* __restrict__ uo, float* __restrict__ vo, float* __restrict__ trace, int trace_every,
+                    const GSArgs<float>* __restrict__ batch_args) {
     using S = RRShape<N, WPC>;
     constexpr int R = S::R, H = S::H;
     constexpr int NN = N * N;
+    // a batched launch runs one lattice per cluster: member m = cluster index, with
+    // its own state slice and parameters (trace is single-lattice only)
+    const int member = (int)blockIdx.x / kRRCluster;
+    if (batch_args) {
+        const size_t moff = (size_t)member * NN;
+        u0 += moff; v0 += moff; uo += moff; vo += moff;
+        a = batch_args[member];
+        trace = nullptr;
+    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RRCtx<N, WPC> c;
     c.smem = smem_raw;

@@ -38,6 +38,8 @@ _SIGS = {
     "gpgmp_gs_forward_host": (C.c_int, [C.POINTER(GSParams)] + [C.c_void_p] * 4),
     "gpgmp_gs_loss_grad_host": (C.c_int, [C.POINTER(GSParams)] + [C.c_void_p] * 6),
     "gpgmp_gs_status": (C.c_int, [C.POINTER(C.c_int32)]),
+    "gpgmp_gs_forward_batch_f32": (C.c_int, [C.POINTER(GSParams), C.c_int32, C.c_void_p] + [C.c_void_p] * 5),
+    "gpgmp_gs_batch_capacity": (C.c_int, [C.c_int32, C.POINTER(C.c_int32)]),
 }
 _lib.SIGNATURES.update(_SIGS)
 
@@ -117,6 +119,32 @@ def forward(u0, v0, p: GSParams, checkpoints=None):
     _lib.check(_fn(name)(C.byref(p), C.c_void_p(u0.data_ptr()), C.c_void_p(v0.data_ptr()), C.c_void_p(u.data_ptr()),
                          C.c_void_p(v.data_ptr()), ck, _stream_ptr(torch, u0.device)), name)
     return u, v
+
+
+def forward_batch(u0, v0, p: GSParams, member_params=None):
+    """Independent float32 lattices u0, v0 [batch][n][n] in one launch (one 16-CTA
+    cluster each); member_params: optional [batch][6] (F, k, Du, Dv, vx, vy)."""
+    import torch
+    u0 = u0.contiguous()
+    v0 = v0.contiguous()
+    u = torch.empty_like(u0)
+    v = torch.empty_like(v0)
+    mp = None
+    if member_params is not None:
+        mp = np.ascontiguousarray(member_params, dtype=np.float64).reshape(-1, 6)
+    _lib.check(_fn("gpgmp_gs_forward_batch_f32")(C.byref(p), u0.shape[0],
+                                                 mp.ctypes.data_as(C.c_void_p) if mp is not None else None,
+                                                 C.c_void_p(u0.data_ptr()), C.c_void_p(v0.data_ptr()),
+                                                 C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                                 _stream_ptr(torch, u0.device)), "gpgmp_gs_forward_batch_f32")
+    return u, v
+
+
+def batch_capacity(n: int) -> int:
+    """Lattices of side n that forward_batch runs at the same time on this GPU."""
+    c = C.c_int32(0)
+    _lib.check(_fn("gpgmp_gs_batch_capacity")(n, C.byref(c)), "gpgmp_gs_batch_capacity")
+    return int(c.value)
 
 
 def status() -> int:

@@ -203,6 +203,16 @@ int gpgmp_gs_adjoint_f32(const gpgmp_gs_params* p, const float* checkpoints, con
 int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* checkpoints, const double* lam_u,
                          const double* lam_v, double* grad_u0, double* grad_v0, double* grad6, void* work,
                          void* stream);
+/* batch independent float32 lattices in one launch, one 16-CTA cluster each (on a B200
+ * nine run at once): u0, v0, u, v are [batch][n][n]; member_params (host, may be NULL
+ * = all use p) holds per member F, k, Du, Dv, vx, vy; n, steps and dt are p's.  No
+ * checkpoints.  Each member's result is bit-identical to its own gpgmp_gs_forward_f32.
+ * No counterpart in the reference (one model per run). */
+int gpgmp_gs_forward_batch_f32(const gpgmp_gs_params* p, int32_t batch, const double* member_params,
+                               const float* u0, const float* v0, float* u, float* v, void* stream);
+/* how many lattices of side n gpgmp_gs_forward_batch_f32 runs at the same time on the
+ * current device (its 16-CTA clusters that are resident at once) */
+int gpgmp_gs_batch_capacity(int32_t n, int32_t* lattices);
 /* Status of the forward kernels on the current device: *flags != 0 if a bounded wait
  * inside a register-resident forward solve gave up since the last call (that solve's
  * output is NaN).  Synchronises the device and clears the flags.  No counterpart in

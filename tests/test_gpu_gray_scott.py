@@ -96,6 +96,28 @@ def test_register_resident_forward_bit_exact(gpgmp, n, steps, drift, every):
         assert torch.equal(ru, tu) and torch.equal(rv, tv)
 
 
+def test_batched_forward_equals_single_solves(gpgmp):
+    """Nine lattices with their own (F, k, drift) in one launch, one cluster each,
+    give the bits of nine separate solves."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=256, steps=400)
+    u0, v0 = _init(cfg, np.float32)
+    rng = np.random.default_rng(8)
+    B = 9
+    U0 = np.stack([u0 + 0.01 * rng.random(u0.shape, np.float32) for _ in range(B)]).astype(np.float32)
+    V0 = np.stack([v0] * B).astype(np.float32)
+    mp = np.array([[0.04 + 0.002 * b, 0.06 - 0.001 * b, 0.16, 0.08, 0.05 if b % 3 == 0 else 0.0, 0.0]
+                   for b in range(B)])
+    tu, tv = torch.tensor(U0, device="cuda"), torch.tensor(V0, device="cuda")
+    bu, bv = gs.forward_batch(tu, tv, cfg.params(), member_params=mp)
+    for b in range(B):
+        p = cfg.params(F=mp[b, 0], k=mp[b, 1], vx=mp[b, 4])
+        su, sv = gs.forward(tu[b], tv[b], p)
+        assert torch.equal(bu[b], su) and torch.equal(bv[b], sv), b
+    assert gs.status() == 0
+
+
 _RR_ADJ_WARPS = {64: [1, 2, 4], 128: [2, 4, 8], 256: [4, 8]}
 
 
