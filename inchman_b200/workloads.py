@@ -4,6 +4,7 @@ Each returns one JSON-ready dict in bench.py's format.  Inputs are synthetic and
 seeded.  Units:
   cell-steps/s      lattice cells x realisations x event-loop steps per second
   particle-steps/s  particles x steps per second
+  individuals/s     individuals in the list x bookkeeping calls per second
 """
 from __future__ import annotations
 
@@ -187,9 +188,101 @@ def particles(args, rank, world):
                  {"particles_left": len(x1), "dtype": "f32+u32"})
 
 
+def population(args, rank, world):
+    """Individual bookkeeping (maintainPopulation): 1024 x 1024 cells holding Poisson(4)
+    individuals (about 4.2e6) sorted by cell, a free-id pool of 2^21; every step each
+    cell's target count moves by -1, 0 or +1.  Timed: one gpgmp_population_maintain
+    call per step on resident buffers (the list alternates between two buffer sets).
+
+    Roofline: the bytes the operation must move at least once -- read keys and ids,
+    write the new keys and ids (16 B per individual), read start, count and goal and
+    write the new start (16 B per cell), read and write the pool (8 B per entry)."""
+    import ctypes as C
+    import os
+    import sys
+    import torch
+    from .individual import _call, _ptr, _stream
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import load_peaks
+    G, mean, npool0 = 1024, 4.0, 1 << 21
+    ncells = G * G
+    rng = np.random.default_rng(1234)
+    counts = rng.poisson(mean, ncells).astype(np.uint32)
+    n = int(counts.sum())
+    keys = np.repeat(np.arange(ncells, dtype=np.uint32), counts)
+    perm = rng.permutation(n + npool0).astype(np.uint32)
+    start = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.uint32)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cap = n + npool0
+    tot = lambda a: torch.from_numpy(a.view(np.int32)).to(dev)
+    bufs = []
+    for _ in range(2):
+        bufs.append({"keys": torch.empty(cap, dtype=torch.int32, device=dev),
+                     "ids": torch.empty(cap, dtype=torch.int32, device=dev),
+                     "pool": torch.empty(cap, dtype=torch.int32, device=dev),
+                     "start": torch.empty(ncells, dtype=torch.int32, device=dev)})
+    bufs[0]["keys"][:n] = tot(keys)
+    bufs[0]["ids"][:n] = tot(perm[:n].copy())
+    bufs[0]["pool"][:npool0] = tot(perm[n:].copy())
+    bufs[0]["start"][:] = tot(start)
+    count = tot(counts)
+    nsteps = args.warmup + args.steps
+    goals = []
+    g = counts.astype(np.int64)
+    for _ in range(nsteps):
+        g = np.maximum(g + rng.integers(-1, 2, ncells), 0)
+        goals.append(tot(g.astype(np.int32)))
+    sb = C.c_size_t(0)
+    _call("gpgmp_population_scratch_bytes", cap, ncells, C.byref(sb))
+    scratch = torch.empty(sb.value, dtype=torch.uint8, device=dev)
+    state = {"n": n, "npool": npool0, "count": count}
+    na, npo = C.c_int64(0), C.c_int64(0)
+    moved = []
+
+    def step(k):
+        src, dst = bufs[k % 2], bufs[(k + 1) % 2]
+        _call("gpgmp_population_maintain", _ptr(src["keys"]), _ptr(src["ids"]), state["n"], _ptr(src["start"]),
+              _ptr(state["count"]), _ptr(goals[k]), ncells, _ptr(src["pool"]), state["npool"], 1234, k,
+              _ptr(dst["keys"]), _ptr(dst["ids"]), cap, _ptr(dst["pool"]), cap, _ptr(dst["start"]),
+              C.byref(na), C.byref(npo), _ptr(scratch), scratch.numel(), _stream())
+        moved.append(16 * (state["n"] + na.value) // 2 + 16 * ncells + 8 * (state["npool"] + npo.value) // 2)
+        state["n"], state["npool"], state["count"] = na.value, npo.value, goals[k]
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    moved.clear()
+    n_before = state["n"]
+    a, b = _events()
+    a.record()
+    for k in range(args.warmup, nsteps):
+        step(k)
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    # the last list must hold exactly the last goal, still sorted by cell
+    last = bufs[nsteps % 2]
+    kk = last["keys"][:state["n"]].cpu().numpy().view(np.uint32)
+    ok = bool(np.all(np.diff(kk.astype(np.int64)) >= 0) and
+              np.array_equal(np.bincount(kk, minlength=ncells), goals[-1].cpu().numpy()))
+    inds = (n_before + state["n"]) / 2 * args.steps
+    launches_per_call = 7     # decide, three scans, scatter, births, pool tail
+    alg = sum(moved) / args.steps
+    peak, peak_kind = load_peaks()
+    ach = alg / (t / args.steps) / 1e9
+    return _base(args, world, inds / t, "individuals/s", "population_1024x1024_poisson4_pool2^21",
+                 {"grid": [G, G], "individuals": n, "pool": npool0, "goal_change": "U{-1,0,1} per cell per step",
+                  "l2": "inputs larger than L2 (about 70 MB read + 70 MB written per step, ping-pong buffers)"},
+                 t / args.steps * 1e3,
+                 {"dtype": "u32", "invariants_ok": ok, "gpu_launches": launches_per_call * args.steps,
+                  "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                               "peak_kind": peak_kind, "traffic": None,
+                               "algorithmic_bytes_per_step": alg}})
+
+
 def run(args, rank, world):
     table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles,
-             "ensemble": ensemble}
+             "ensemble": ensemble, "population": population}
     if args.workload not in table:
         raise SystemExit(f"unknown workload {args.workload}; one of gray_scott, {', '.join(table)}")
     return table[args.workload](args, rank, world)
