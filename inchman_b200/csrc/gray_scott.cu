@@ -24,6 +24,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "gs_kernels.h"
+#include "host_common.h"
 
 namespace cg = cooperative_groups;
 
@@ -725,7 +726,7 @@ cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMemb
     const void* rk = rr_kernel(p.n, &wpc, drift, &smem);
     if (!rk) return cudaErrorInvalidValue;
     GSArgs<float>* d = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&d, sizeof(GSArgs<float>) * batch, st);
+    cudaError_t e = pool_alloc((void**)&d, sizeof(GSArgs<float>) * batch, st);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d, h.data(), sizeof(GSArgs<float>) * batch, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
@@ -751,7 +752,7 @@ cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMemb
             e = cudaLaunchKernelExC(&cfg, rk, args);
         }
     }
-    cudaError_t e2 = cudaFreeAsync(d, st);
+    cudaError_t e2 = pool_free(d, st);
     return e != cudaSuccess ? e : e2;
 }
 

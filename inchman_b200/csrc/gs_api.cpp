@@ -229,14 +229,34 @@ int gpgmp_gs_status(int32_t* flags) {
     return GPGMP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Device buffers of one host-buffer call, returned to the pool in stream order on
+// every exit path.
+template <int N>
+struct PoolBuffers {
+    explicit PoolBuffers(cudaStream_t s) : st(s) {}
+    ~PoolBuffers() {
+        for (void* q : p) gpgmp::pool_free(q, st);
+    }
+    cudaStream_t st;
+    void* p[N] = {};
+};
+}  // namespace
+
+extern "C" {
+
 int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v) {
     int rc = check(p, 4);
     if (rc) return rc;
     if (!u0 || !v0 || !u || !v) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     const size_t nn = (size_t)p->n * p->n, bytes = nn * sizeof(float);
     cudaStream_t st = nullptr;
+    PoolBuffers<1> buf(st);
     float* d = nullptr;
-    CK(cudaMallocAsync((void**)&d, 4 * bytes, st));
+    CK(pool_alloc((void**)&d, 4 * bytes, st));
+    buf.p[0] = d;
     CK(cudaMemcpyAsync(d, u0, bytes, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d + nn, v0, bytes, cudaMemcpyHostToDevice, st));
     rc = forward<float>(p, d, d + nn, d + 2 * nn, d + 3 * nn, nullptr, st);
@@ -244,7 +264,6 @@ int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float
         CK(cudaMemcpyAsync(u, d + 2 * nn, bytes, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(v, d + 3 * nn, bytes, cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaFreeAsync(d, st));
     CK(cudaStreamSynchronize(st));
     if (rc == GPGMP_OK) {
         int bad = 0;
@@ -263,12 +282,17 @@ int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const flo
     size_t ckb = 0, wb = 0;
     gpgmp_gs_buffer_sizes(p, 4, &ckb, &wb);
     cudaStream_t st = nullptr;
+    PoolBuffers<4> buf(st);
     float *d = nullptr, *ck = nullptr, *work = nullptr;
     double* dg = nullptr;
-    CK(cudaMallocAsync((void**)&d, 8 * bytes, st));
-    CK(cudaMallocAsync((void**)&ck, ckb, st));
-    CK(cudaMallocAsync((void**)&work, wb, st));
-    CK(cudaMallocAsync((void**)&dg, 6 * sizeof(double), st));
+    CK(pool_alloc((void**)&d, 8 * bytes, st));
+    buf.p[0] = d;
+    CK(pool_alloc((void**)&ck, ckb, st));
+    buf.p[1] = ck;
+    CK(pool_alloc((void**)&work, wb, st));
+    buf.p[2] = work;
+    CK(pool_alloc((void**)&dg, 6 * sizeof(double), st));
+    buf.p[3] = dg;
     CK(cudaMemcpyAsync(d, u0, bytes, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d + nn, v0, bytes, cudaMemcpyHostToDevice, st));
     rc = forward<float>(p, d, d + nn, d + 2 * nn, d + 3 * nn, ck, st);
@@ -292,10 +316,6 @@ int gpgmp_gs_loss_grad_host(const gpgmp_gs_params* p, const float* u0, const flo
     int err = 0;
     CK(cudaMemcpyAsync(grad6, dg, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&err, (char*)work + wb - 16, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaFreeAsync(d, st));
-    CK(cudaFreeAsync(ck, st));
-    CK(cudaFreeAsync(work, st));
-    CK(cudaFreeAsync(dg, st));
     CK(cudaStreamSynchronize(st));
     if (err) return set_error(GPGMP_ERR_TIMEOUT, "a bounded wait for a TMA copy in the adjoint gave up");
     CK(gs_forward_status(&err, true));
