@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <mutex>
 #include <cuda_runtime.h>
+#include "lookback.cuh"
 #include "sort_kernels.h"
 #include "host_common.h"
 #include "../../include/gpgmp_c.h"
@@ -30,26 +31,6 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;   // 4096
-constexpr uint64_t kScanFlagA = 1ull << 32;
-constexpr uint64_t kScanFlagP = 2ull << 32;
-constexpr uint32_t kSpinLimit = 1u << 24;
-
-__device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t* p) {
-    uint64_t v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
-}
 
 // ---- exclusive scan ------------------------------------------------------------
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
@@ -107,38 +88,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
     const uint32_t aggregate = s_warp[kScanThreads / 32 - 1];
     // decoupled look-back by warp 0
     if (warp == 0) {
-        uint32_t exclusive = 0;
-        if (tile == 0) {
-            if (lane == 0) st_release_u64(&status[0], kScanFlagP | aggregate);
-        } else {
-            if (lane == 0) st_release_u64(&status[tile], kScanFlagA | aggregate);
-            int64_t look = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            bool done = false;
-            while (!done) {
-                const int64_t idx = look - lane;
-                uint64_t w = idx >= 0 ? ld_volatile_u64(&status[idx]) : kScanFlagP;
-                uint32_t flag = (uint32_t)(w >> 32);
-                // wait until every lane of the window has at least an aggregate
-                if (__any_sync(0xffffffffu, flag == 0)) {
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0) atomicExch(err, 1);
-                        break;
-                    }
-                    continue;
-                }
-                const unsigned pmask = __ballot_sync(0xffffffffu, flag == 2);
-                // lanes up to and including the first inclusive prefix contribute
-                const int first_p = pmask ? __ffs(pmask) - 1 : 32;
-                uint32_t val = lane <= first_p ? (uint32_t)w : 0u;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-                exclusive += val;
-                if (pmask) done = true;
-                else look -= 32;
-            }
-            if (lane == 0) st_release_u64(&status[tile], kScanFlagP | (uint32_t)(exclusive + aggregate));
-        }
+        const uint32_t exclusive = warp_lookback_u32(status, tile, aggregate, err);
         if (lane == 0) s_prefix = exclusive;
     }
     __syncthreads();

@@ -266,7 +266,7 @@ def population(args, rank, world):
     ok = bool(np.all(np.diff(kk.astype(np.int64)) >= 0) and
               np.array_equal(np.bincount(kk, minlength=ncells), goals[-1].cpu().numpy()))
     inds = (n_before + state["n"]) / 2 * args.steps
-    launches_per_call = 7     # decide, three scans, scatter, births, pool tail
+    launches_per_call = 2     # k_pop_plan, k_pop_move
     alg = sum(moved) / args.steps
     peak, peak_kind = load_peaks()
     ach = alg / (t / args.steps) / 1e9

@@ -69,7 +69,8 @@ def test_oracle_reports_a_short_pool():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("ncells,mean,extra,change", [(1, 6.0, 10, 4), (97, 3.0, 400, 3), (4096, 0.5, 20000, 2),
-                                                      (200_000, 5.0, 400_000, 2), (50, 0.0, 100, 3)])
+                                                      (6145, 3.0, 20000, 3), (200_000, 5.0, 400_000, 2),
+                                                      (50, 0.0, 100, 3)])
 def test_gpu_matches_oracle(gpgmp, ncells, mean, extra, change):
     import torch
     from inchman_b200.individual import maintain_population
@@ -99,3 +100,56 @@ def test_gpu_reports_a_short_pool(gpgmp):
                             torch.zeros(2, dtype=torch.int32, device="cuda"),
                             torch.tensor([3, 2], dtype=torch.int32, device="cuda"),
                             torch.arange(4, dtype=torch.int32, device="cuda"), 1, 1)
+
+
+def _gpu_vs_oracle(keys, ids, start, count, goal, pool, seed, step):
+    import torch
+    from inchman_b200.individual import maintain_population
+    rc, ko, io, po = _oracle(keys, ids, start, count, goal, pool, seed, step)
+    assert rc == 0
+    t = lambda a: torch.tensor(a.view(np.int32) if a.dtype == np.uint32 else a, dtype=torch.int32, device="cuda")
+    gk, gi, gs, gp = maintain_population(t(keys), t(ids), t(start), t(count), t(goal), t(pool), seed, step)
+    assert np.array_equal(gk.cpu().numpy().view(np.uint32), ko)
+    assert np.array_equal(gi.cpu().numpy().view(np.uint32), io)
+    assert np.array_equal(gp.cpu().numpy().view(np.uint32), po)
+
+
+@pytest.mark.gpu
+def test_gpu_heavy_cells(gpgmp):
+    """One cell loses 15,000 of 20,000 individuals, another gains 29,997; the rest
+    are ordinary: the per-cell loops and the individual-parallel moves agree with
+    the oracle bit for bit."""
+    rng = np.random.default_rng(7)
+    ncells = 3000
+    counts = rng.poisson(2.0, ncells).astype(np.uint32)
+    counts[17] = 20000
+    counts[2500] = 3
+    n = int(counts.sum())
+    keys = np.repeat(np.arange(ncells, dtype=np.uint32), counts)
+    allids = rng.permutation(n + 40000).astype(np.uint32)
+    ids, pool = allids[:n].copy(), allids[n:].copy()
+    start = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.uint32)
+    goal = np.maximum(counts.astype(np.int64) + rng.integers(-2, 3, ncells), 0).astype(np.int32)
+    goal[17] = 5000
+    goal[2500] = 30000
+    goal[5] = -4                      # negative goals count as 0
+    _gpu_vs_oracle(keys, ids, start, counts, goal, pool, 99, 2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["list", "pool"])
+def test_gpu_reports_full_outputs(gpgmp, which):
+    import torch
+    from inchman_b200 import _lib
+    from inchman_b200.individual import maintain_population
+    rng = np.random.default_rng(3)
+    keys, ids, start, count, goal, pool = _case(rng, 500, 4.0, 3000, 3)
+    t = lambda a: torch.tensor(a.view(np.int32) if a.dtype == np.uint32 else a, dtype=torch.int32, device="cuda")
+    n_new = int(goal.sum())
+    kw = {"capacity": n_new - 1} if which == "list" else {"pool_capacity": 10}
+    with pytest.raises(_lib.GpgmpError):
+        maintain_population(t(keys), t(ids), t(start), t(count), t(goal), t(pool), 1, 1, **kw)
+    # exactly enough room succeeds
+    gk, gi, gs, gp = maintain_population(t(keys), t(ids), t(start), t(count), t(goal), t(pool), 1, 1,
+                                         capacity=n_new)
+    assert gk.numel() == n_new
