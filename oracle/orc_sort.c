@@ -164,7 +164,8 @@ int64_t orc_particles_run(int64_t n, float* px, float* py, uint8_t* sp, int G, f
 /* IndividualSolver::maintainPopulation (IndividualSolver.cpp:458-671,
  * IndividualSolver.cl:1017-1882), restated as the CUDA path lays it out: per cell the
  * surplus is chosen by selection sampling (candidate i taken with probability
- * k_rem / (is - i), one Philox draw each, stream (seed, 0, step, cell, POP)); the new
+ * k_rem / (is - i): draw x, taken iff x (is - i) < k_rem 2^32; one Philox draw per
+ * candidate while removals remain, stream (seed, 0, step, cell, POP)); the new
  * list has, per cell in order, the births (ids from the front of the pool) and then
  * the survivors in their old order; the new pool is the removed ids in list order
  * followed by the unused old pool.  Returns -1 if the pool is too small. */
@@ -182,8 +183,9 @@ int orc_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n
             orc_stream_init(&st, seed, 0u, step, (uint32_t)c, ORC_PH_POP);
             uint32_t krem = is - g;
             for (uint32_t i = 0; i < is && krem > 0; ++i) {
-                double u = (double)orc_stream_next(&st) * (1.0 / 4294967296.0);
-                if ((double)(is - i) * u < (double)krem) { dead[start[c] + i] = 1; --krem; }
+                /* u (is - i) < krem with u = x / 2^32, exactly in 64-bit integers */
+                uint32_t x = orc_stream_next(&st);
+                if ((uint64_t)(is - i) * x < ((uint64_t)krem << 32)) { dead[start[c] + i] = 1; --krem; }
             }
         }
     }
