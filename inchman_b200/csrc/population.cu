@@ -38,9 +38,9 @@
 namespace gpgmp {
 namespace {
 
-constexpr int kPlanThreads = 256;
+constexpr int kPlanThreads = 512;
 constexpr int kPlanItems = 8;
-constexpr int kPlanTile = kPlanThreads * kPlanItems;   // 2048 cells
+constexpr int kPlanTile = kPlanThreads * kPlanItems;   // 4096 cells
 constexpr int kMoveThreads = 256;
 constexpr int kMoveUnroll = 4;   // independent loads in flight per thread
 constexpr uint32_t kMaskCell = 32;     // cells of at most this many individuals get a removal mask
@@ -110,9 +110,9 @@ __device__ __forceinline__ void warp_masks(const uint32_t* list, uint32_t* mask,
 }
 
 // Cells are read and written warp-striped (item q of lane l of warp w is cell
-// tile_base + 256 w + 32 q + l), so every access is one coalesced 128-byte row; the
+// tile_base + 256 w + 32 q + l for 8 items), so every access is one coalesced 128-byte row; the
 // scans run in that order: a warp scan per item row, carried across the rows.
-__global__ void __launch_bounds__(kPlanThreads, 4)
+__global__ void __launch_bounds__(kPlanThreads, 2)
     k_pop_plan(const uint32_t* __restrict__ start, const uint32_t* __restrict__ count,
                const int32_t* __restrict__ goal, int64_t ncells, uint32_t seed, uint32_t step,
                uint32_t* __restrict__ new_start, uint32_t* __restrict__ birth_off, CellPlan* __restrict__ plan,
