@@ -204,7 +204,7 @@ int gpgmp_gs_adjoint_f64(const gpgmp_gs_params* p, const double* checkpoints, co
                          const double* lam_v, double* grad_u0, double* grad_v0, double* grad6, void* work,
                          void* stream);
 /* batch independent float32 lattices in one launch, one 16-CTA cluster each (on a B200
- * nine run at once): u0, v0, u, v are [batch][n][n]; member_params (host, may be NULL
+ * seven or eight run at once, gpgmp_gs_batch_capacity): u0, v0, u, v are [batch][n][n]; member_params (host, may be NULL
  * = all use p) holds per member F, k, Du, Dv, vx, vy; n, steps and dt are p's.  No
  * checkpoints.  Each member's result is bit-identical to its own gpgmp_gs_forward_f32.
  * No counterpart in the reference (one model per run). */
@@ -219,7 +219,8 @@ int gpgmp_gs_batch_capacity(int32_t n, int32_t* lattices);
  * the reference (its kernels have no waits). */
 int gpgmp_gs_status(int32_t* flags);
 /* Host buffers in and out: copies (u0, v0) to the device, runs the forward solve,
- * copies (u, v) back.  Allocates its device buffers from the stream-ordered pool. */
+ * copies (u, v) back.  Its device buffers come from a memory pool per device that the
+ * library keeps (freed memory stays mapped for the next call, until the process exits). */
 int gpgmp_gs_forward_host(const gpgmp_gs_params* p, const float* u0, const float* v0, float* u, float* v);
 /* Host buffers: loss L = sum (u_N - ut)^2 + (v_N - vt)^2 and its gradient with
  * respect to (F, k, Du, Dv, vx, vy) by the adjoint. */
