@@ -244,6 +244,9 @@ class LoadedModel:
     runs: int = 1
     parameters: Dict[str, float] = field(default_factory=dict)
     notes: List[str] = field(default_factory=list)
+    # named compartments as inclusive rectangles (x0, y0, x1, y1), in file order
+    compartments: Dict[str, Tuple[int, int, int, int]] = field(default_factory=dict)
+    source: str = ""          # the model file's text
 
 
 def _text(e: Optional[ET.Element]) -> str:
@@ -263,9 +266,12 @@ def _num(parent: Optional[ET.Element], name: str, env: Dict[str, float]) -> Opti
     return evaluate(mathml(m), env)
 
 
-def load(source: str, *, ignore_scripts: bool = False) -> LoadedModel:
+def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[str, float]] = None) -> LoadedModel:
     """source: a file path or the XML text.  ignore_scripts: load a model whose init
-    or event scripts are non-empty without them (the reference runs them as Python)."""
+    or event scripts are non-empty without them (the reference runs them as Python).
+    overrides: parameter values that replace (or add to) the file's, before any
+    expression is evaluated (the executable's --p name=value,
+    InchmanDiffusionModel.cpp:100-118)."""
     text = source if source.lstrip().startswith("<") else open(source, encoding="utf-8").read()
     root = ET.fromstring(text)
     model_e = root.find(SB + "model")
@@ -282,6 +288,8 @@ def load(source: str, *, ignore_scripts: bool = False) -> LoadedModel:
         if domain != "single":
             raise Unsupported(f"parameter domain {domain!r}")
         params[p.get("id")] = float(p.get("value", "0"))
+    for k, v in (overrides or {}).items():
+        params[k] = float(v)
     sb = root.find(f"{SB}annotation/{IM}sbml")
     m = DiffusionModel()
     runs = 1
@@ -417,4 +425,4 @@ def load(source: str, *, ignore_scripts: bool = False) -> LoadedModel:
         m.code_defines = "\n".join(defines)
     elif m.custom_laws is not None:
         m.code_defines = "\n".join(f"#define {k} {c_float(v)}" for k, v in params.items())
-    return LoadedModel(model=m, runs=runs, parameters=params, notes=notes)
+    return LoadedModel(model=m, runs=runs, parameters=params, notes=notes, compartments=comps, source=text)

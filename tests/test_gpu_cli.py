@@ -1,0 +1,77 @@
+"""The reference's executable end to end (exec/src/inchman/main.cpp:67-160): a model
+file in, the reference's HDF5 layout out (inchman_b200.cli), with the same numbers as
+the solver run directly on the same model, seed and initial state."""
+import os
+
+import numpy as np
+import pytest
+
+from inchman_b200 import _lib, cli, h5, sbml
+from inchman_b200.solver import Solver
+
+MODELS = os.path.join(os.path.dirname(__file__), "golden", "models")
+
+
+def _variant(tmp_path, name, runs=None, solver=None):
+    text = open(os.path.join(MODELS, name), encoding="utf-8").read()
+    if runs is not None:
+        old = '<im:runs><math:math xmlns:math="http://www.w3.org/1998/Math/MathML"><math:cn>1</math:cn>'
+        assert old in text
+        text = text.replace(old, old.replace("<math:cn>1</math:cn>", f"<math:cn>{runs}</math:cn>"))
+    if solver is not None:
+        a = text.index("<im:solver>") + len("<im:solver>")
+        b = text.index("</im:solver>")
+        text = text[:a] + solver + text[b:]
+    p = tmp_path / name
+    p.write_text(text, encoding="utf-8")
+    return str(p)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,runs,solver,override", [
+    ("saturating.xml", 3, None, None),
+    ("ab_drift.xml", 2, None, ("k2", 0.02)),
+    ("ab_drift.xml", 1, "deterministic_inhomogeneous_RK4", None),
+])
+def test_cli_writes_the_solver_results(gpgmp, tmp_path, name, runs, solver, override):
+    path = _variant(tmp_path, name, runs, solver)
+    out = str(tmp_path / "out.h5")
+    args = [path, "--output", out, "--seed", "11"]
+    overrides = {}
+    if override:
+        args += ["--p", f"{override[0]}={override[1]}"]
+        overrides[override[0]] = override[1]
+    assert cli.main(args) == 0
+    # the same model run directly
+    lm = sbml.load(path, overrides=overrides)
+    m = lm.model
+    det = m.solver in _lib.DETERMINISTIC_TYPES
+    R = 1 if det else runs
+    init = m.initial_state(np.random.default_rng(11), R)
+    with Solver(m, realisations=R, seed=11) as s:
+        s.set_state(init.astype(np.float32) if det else init)
+        snaps, times, _ = s.solve(max_snapshots=64)
+    f = h5.read(out)
+    assert f["Model"].attrs["numRuns"].tolist() == [R]
+    assert f["Model/Species"].value == [sp.id for sp in m.species]
+    assert f["Model/InchmanFile"].value == open(path, encoding="utf-8").read()
+    if override:
+        assert f["Parameters"].attrs[override[0]].tolist() == [np.float32(override[1])]
+    names = []
+    for t in times:
+        if cli.dump_name(t) not in names:
+            names.append(cli.dump_name(t))
+    assert sorted(names) == list(f["Runs/0"]) and "Dump_0" in names
+    for r in range(R):
+        seen = set()
+        for k, t in enumerate(times):
+            nm = cli.dump_name(t)
+            if nm in seen:
+                continue                       # a repeated name keeps the first dump
+            seen.add(nm)
+            d = f[f"Runs/{r}/{nm}"]
+            assert d.attrs["time"].tolist() == [t]
+            for si, sp in enumerate(m.species):
+                v = d[sp.id].value
+                assert v.dtype == (np.float32 if det else np.int32)
+                assert np.array_equal(v.reshape(-1), snaps[k, r, si].reshape(-1))
