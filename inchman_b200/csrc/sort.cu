@@ -114,11 +114,15 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
 }
 
 // ---- radix sort ------------------------------------------------------------------
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = 512;
 constexpr int kSortItems = 15;
-constexpr int kSortTile = kSortThreads * kSortItems;   // 3840
+constexpr int kSortTile = kSortThreads * kSortItems;   // 7680: fewer tiles, a shorter look-back chain
+constexpr int kDigitWarps = 256 / 32;                  // threads 0-255 own one digit each in the digit phases
+static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "one thread per digit");
+constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
 constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
+constexpr int kLookWindow = 8;   // predecessor tiles read per look-back step
 
 // one pass over the keys counts every digit position: hist[pass][256]
 __global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n, int passes,
@@ -155,102 +159,133 @@ __global__ void k_radix_bin_offsets(uint32_t* __restrict__ hist) {
 // One onesweep pass.  Warp w of a tile owns keys [w*32*IT, (w+1)*32*IT) of the tile
 // in a warp-striped layout (item j of lane l is key j*32 + l), so processing items in
 // order and lanes in order is index order: the ranks are stable.
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ kin,
+__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin,
                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            int64_t n, int shift, const uint32_t* __restrict__ bins,
                                                            uint32_t* __restrict__ look, unsigned int* tile_counter,
                                                            int* err) {
     __shared__ uint32_t s_warp_hist[kWarps][256];
+    __shared__ uint32_t s_count[256];        // the tile's count of each digit
     __shared__ uint32_t s_tile_off[256];     // exclusive offset of each digit inside the tile
     __shared__ uint32_t s_global[256];       // global start of each digit's run of this tile
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
+    extern __shared__ uint32_t s_staging[];  // keys then values in tile-sorted order (dynamic: 60 KB)
+    uint32_t* s_keys = s_staging;
+    uint32_t* s_vals = s_staging + kSortTile;
     __shared__ uint32_t s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int i = threadIdx.x; i < kWarps * 256; i += kSortThreads) (&s_warp_hist[0][0])[i] = 0;
+    if (threadIdx.x < 256) s_count[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const int64_t tbase = (int64_t)tile * kSortTile;
     const int64_t wbase = tbase + (int64_t)warp * 32 * kSortItems;
-    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+    // values stay in memory until the staging step (fewer registers, more warps per SM)
+    uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t idx = wbase + j * 32 + lane;
-        const bool ok = idx < n;
-        key[j] = ok ? kin[idx] : 0xffffffffu;
-        val[j] = ok ? vin[idx] : 0u;
+        key[j] = idx < n ? kin[idx] : 0xffffffffu;
     }
-    // warp-level ranking (stable)
+    // the tile's digit counts first (order-free shared-memory atomics), published
+    // before the ranking so that the look-back of later tiles can start early
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j)
+        if (wbase + j * 32 + lane < n) atomicAdd(&s_count[(key[j] >> shift) & 0xffu], 1u);
+    __syncthreads();
+    const int d = threadIdx.x;   // the digit of threads 0-255
+    const bool digit_thread = d < 256;
+    const uint32_t tile_count = digit_thread ? s_count[d] : 0u;
+    uint32_t* lk = look + (size_t)tile * 256;
+    if (digit_thread) st_release_u32(&lk[d], (tile == 0 ? kFlagP : kFlagA) | tile_count);
+    // warp-level ranking (stable): the lanes holding the same digit, from eight ballots
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t idx = wbase + j * 32 + lane;
         const bool ok = idx < n;
-        const unsigned active = __ballot_sync(0xffffffffu, ok);
-        const uint32_t d = (key[j] >> shift) & 0xffu;
-        unsigned peers = __match_any_sync(0xffffffffu, ok ? d : 0x100u + lane);
-        peers &= active;
+        const uint32_t dj = (key[j] >> shift) & 0xffu;
+        unsigned peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const unsigned bal = __ballot_sync(0xffffffffu, (dj >> b) & 1u);
+            peers &= ((dj >> b) & 1u) ? bal : ~bal;
+        }
         uint32_t prior = 0;
         if (ok) {
             const int leader = __ffs(peers) - 1;
             const uint32_t cnt = __popc(peers);
-            if (lane == leader) prior = s_warp_hist[warp][d], s_warp_hist[warp][d] = prior + cnt;
+            if (lane == leader) prior = s_warp_hist[warp][dj], s_warp_hist[warp][dj] = prior + cnt;
             prior = __shfl_sync(peers, prior, leader);
             rank[j] = prior + __popc(peers & lt);
         }
         __syncwarp();
     }
     __syncthreads();
-    // per digit: counts over warps -> warp offsets (in place) and the tile count
-    const int d = threadIdx.x;   // 256 threads = 256 digits
-    uint32_t tile_count = 0;
+    // per digit: counts over warps -> warp offsets (in place)
+    if (digit_thread) {
+        uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-        const uint32_t c = s_warp_hist[w][d];
-        s_warp_hist[w][d] = tile_count;
-        tile_count += c;
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = s_warp_hist[w][d];
+            s_warp_hist[w][d] = run;
+            run += c;
+        }
     }
-    // publish the tile count, then look back for the prefix of this digit
-    uint32_t* lk = look + (size_t)tile * 256;
-    if (tile == 0) st_release_u32(&lk[d], kFlagP | tile_count);
-    else st_release_u32(&lk[d], kFlagA | tile_count);
+    // look back for the prefix of this digit
     uint32_t excl = 0;
-    if (tile > 0) {
+    if (digit_thread && tile > 0) {
+        // look back kLookWindow tiles at a time (their loads in flight together): sum
+        // the counts up to and including the nearest inclusive prefix
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
-        while (t >= 0) {
-            const uint32_t w = ld_acquire_u32(&look[(size_t)t * 256 + d]);
-            const uint32_t f = w & ~kValMask;
-            if (f == 0) {
+        bool done = false;
+        while (!done) {
+            uint32_t w[kLookWindow];
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j)
+                w[j] = t - j >= 0 ? ld_acquire_u32(&look[(size_t)(t - j) * 256 + d]) : kFlagP;
+            bool ready = true;
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j) ready = ready && (w[j] & ~kValMask) != 0;
+            if (!ready) {
                 if (++spins > kSpinLimit) {
                     atomicExch(err, 1);
                     break;
                 }
                 continue;
             }
-            excl += w & kValMask;
-            if (f == kFlagP) break;
-            --t;
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j) {
+                if (!done) {
+                    excl += w[j] & kValMask;
+                    done = (w[j] & ~kValMask) == kFlagP;
+                }
+            }
+            t -= kLookWindow;
         }
         st_release_u32(&lk[d], kFlagP | ((excl + tile_count) & kValMask));
     }
     // tile-local digit offsets (exclusive scan of tile_count over digits)
     {
+        __shared__ uint32_t s_w[kDigitWarps];
         uint32_t incl = tile_count;
+        if (digit_thread) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane == 31) s_w[warp] = incl;
         }
-        __shared__ uint32_t s_w[kWarps];
-        if (lane == 31) s_w[warp] = incl;
         __syncthreads();
-        uint32_t wo = 0;
-        for (int w = 0; w < warp; ++w) wo += s_w[w];
-        s_tile_off[d] = wo + incl - tile_count;
-        s_global[d] = bins[d] + excl;
+        if (digit_thread) {
+            uint32_t wo = 0;
+            for (int w = 0; w < warp; ++w) wo += s_w[w];
+            s_tile_off[d] = wo + incl - tile_count;
+            s_global[d] = bins[d] + excl;
+        }
     }
     __syncthreads();
     // stage keys and values in tile-sorted order
@@ -261,7 +296,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __res
             const uint32_t dd = (key[j] >> shift) & 0xffu;
             const uint32_t lp = s_tile_off[dd] + s_warp_hist[warp][dd] + rank[j];
             s_keys[lp] = key[j];
-            s_vals[lp] = val[j];
+            s_vals[lp] = vin[idx];
         }
     }
     __syncthreads();
@@ -346,7 +381,9 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     uint32_t* look = (uint32_t*)(base + L.off_look);
     uint32_t* ak = (uint32_t*)(base + L.off_alt_keys);
     uint32_t* av = (uint32_t*)(base + L.off_alt_vals);
-    cudaError_t e = cudaMemsetAsync(base, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortStagingBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(base, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
     if (e != cudaSuccess) return e;
     k_radix_histogram<<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
     k_radix_bin_offsets<<<L.passes, 256, 0, st>>>(hist);
@@ -359,7 +396,7 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
         uint32_t* dk = to_out ? kout : ak;
         uint32_t* dv = to_out ? vout : av;
         (void)last;
-        k_onesweep<<<(unsigned)L.tiles, kSortThreads, 0, st>>>(sk, sv, dk, dv, n, 8 * p, hist + 256 * p,
+        k_onesweep<<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(sk, sv, dk, dv, n, 8 * p, hist + 256 * p,
                                                                look + (size_t)256 * L.tiles * p, counters + p,
                                                                (int*)(counters + 4));
         e = cudaGetLastError();
