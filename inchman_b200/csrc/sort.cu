@@ -212,14 +212,16 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
             const unsigned bal = __ballot_sync(0xffffffffu, (dj >> b) & 1u);
             peers &= ((dj >> b) & 1u) ? bal : ~bal;
         }
+        // the lowest lane of each group adds the group to the warp's digit count; the
+        // count before it comes back to the whole group by one full-warp shuffle
+        const int leader = peers ? __ffs(peers) - 1 : lane;
         uint32_t prior = 0;
-        if (ok) {
-            const int leader = __ffs(peers) - 1;
-            const uint32_t cnt = __popc(peers);
-            if (lane == leader) prior = s_warp_hist[warp][dj], s_warp_hist[warp][dj] = prior + cnt;
-            prior = __shfl_sync(peers, prior, leader);
-            rank[j] = prior + __popc(peers & lt);
+        if (ok && lane == leader) {
+            prior = s_warp_hist[warp][dj];
+            s_warp_hist[warp][dj] = prior + __popc(peers);
         }
+        prior = __shfl_sync(0xffffffffu, prior, leader);
+        rank[j] = prior + __popc(peers & lt);
         __syncwarp();
     }
     __syncthreads();
