@@ -75,6 +75,9 @@ class ModelDesc(C.Structure):
         ("code_defines", C.c_char_p),
         ("drift_code", C.c_char_p),
         ("custom_laws", C.POINTER(C.c_char_p)),
+        ("individual", C.POINTER(C.c_uint8)),
+        ("individual_capacity", C.c_int64),
+        ("new_individuals_code", C.c_char_p),
     ]
 
 
@@ -112,6 +115,9 @@ SIGNATURES = {
     "gpgmp_synchronize": (C.c_int, [vp]),
     "gpgmp_device_state": (vp, [vp]),
     "gpgmp_timesteps": (C.c_int, [vp, P(f32), P(f32)]),
+    "gpgmp_individual_count": (C.c_int, [vp, i32, P(i64)]),
+    "gpgmp_get_individuals": (C.c_int, [vp, i32, vp, vp, vp, i64, P(i64)]),
+    "gpgmp_set_individual_properties": (C.c_int, [vp, i32, vp, i64, i64]),
 }
 
 

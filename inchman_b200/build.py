@@ -27,6 +27,7 @@ EXTRA = {
     "stochastic.cu": ["-fmad=false"],
     "ensemble.cu": ["-fmad=false"],
     "particles.cu": ["-fmad=false"],
+    "individual.cu": ["-fmad=false"],
 }
 
 
@@ -38,6 +39,7 @@ def _sources():
 # string literals in the generated csrc/_jit_sources.h
 JIT_HEADERS = [("common.cuh", os.path.join(CSRC, "common.cuh")),
                ("stoch_device.cuh", os.path.join(CSRC, "stoch_device.cuh")),
+               ("individual_device.cuh", os.path.join(CSRC, "individual_device.cuh")),
                ("../../include/gpgmp_c.h", os.path.join(HERE, "..", "include", "gpgmp_c.h"))]
 JIT_OUT = os.path.join(CSRC, "_jit_sources.h")
 

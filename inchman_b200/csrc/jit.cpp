@@ -10,6 +10,7 @@
 #include <cuda.h>
 #include <nvrtc.h>
 #include "host_common.h"
+#include "individual.h"
 #include "_jit_sources.h"
 
 namespace gpgmp {
@@ -87,23 +88,42 @@ typedef unsigned char uint8_t;
 #define INFINITY __int_as_float(0x7f800000)
 )GPGMPJIT";
 
+int compile_module(const std::string& src, const std::vector<const char*>& names, std::vector<CUfunction>* outs);
+
 // Compiles `src` for the current device (sm_100a) and returns kernel `name`.
 int compile(const std::string& src, const char* name, CUfunction* out) {
+    std::vector<CUfunction> fns;
+    int rc = compile_module(src, {name}, &fns);
+    if (rc == GPGMP_OK) *out = fns[0];
+    return rc;
+}
+
+// Compiles `src` once and returns each of the kernels `names`.
+int compile_module(const std::string& src, const std::vector<const char*>& names_in, std::vector<CUfunction>* outs) {
     std::string why;
     if (!load_api(&why)) return set_error(GPGMP_ERR_UNSUPPORTED, "run-time compilation unavailable: %s", why.c_str());
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaFree(nullptr) != cudaSuccess)
         return set_error(GPGMP_ERR_CUDA, "no CUDA context for run-time compilation");
-    const std::string key = std::to_string(dev) + '\0' + name + '\0' + src;
-    auto it = g_cache.find(key);
-    if (it != g_cache.end()) {
-        *out = it->second;
-        return GPGMP_OK;
+    std::string key = std::to_string(dev) + '\0';
+    for (const char* nm : names_in) key += std::string(nm) + '\0';
+    key += src;
+    outs->clear();
+    bool cached = true;
+    for (const char* nm : names_in) {
+        auto it = g_cache.find(key + '\0' + nm);
+        if (it == g_cache.end()) {
+            cached = false;
+            break;
+        }
+        outs->push_back(it->second);
     }
+    if (cached) return GPGMP_OK;
+    outs->clear();
     std::vector<const char*> names(kJitHeaderNames, kJitHeaderNames + kJitHeaderCount);
     std::vector<const char*> texts(kJitHeaderSources, kJitHeaderSources + kJitHeaderCount);
     names.push_back("gpgmp_rtc_prelude.h");
-    texts.push_back(kPrelude);
+    texts.push_back(kPrelude);   // header names (the kernels' names are names_in)
     nvrtcProgram prog = nullptr;
     if (g_api.createProgram(&prog, src.c_str(), "gpgmp_model.cu", (int)names.size(), texts.data(), names.data()) !=
         NVRTC_SUCCESS)
@@ -127,11 +147,13 @@ int compile(const std::string& src, const char* name, CUfunction* out) {
     CUmodule mod = nullptr;
     CUresult cr = g_api.moduleLoadData(&mod, cubin.data());
     if (cr != CUDA_SUCCESS) return set_error(GPGMP_ERR_CUDA, "cuModuleLoadData: error %d", (int)cr);
-    CUfunction fn = nullptr;
-    cr = g_api.moduleGetFunction(&fn, mod, name);
-    if (cr != CUDA_SUCCESS) return set_error(GPGMP_ERR_CUDA, "cuModuleGetFunction(%s): error %d", name, (int)cr);
-    g_cache[key] = fn;
-    *out = fn;
+    for (const char* nm : names_in) {
+        CUfunction fn = nullptr;
+        cr = g_api.moduleGetFunction(&fn, mod, nm);
+        if (cr != CUDA_SUCCESS) return set_error(GPGMP_ERR_CUDA, "cuModuleGetFunction(%s): error %d", nm, (int)cr);
+        g_cache[key + '\0' + nm] = fn;
+        outs->push_back(fn);
+    }
     return GPGMP_OK;
 }
 
@@ -260,6 +282,69 @@ cudaError_t launch_drift_jit(JitFunction fn, const GridDesc& g, int species, flo
     void* args[] = {&W, &H, &S, &species, &L, &sim_time, &dx, &dy, &rx, &ry, (void*)&state};
     std::lock_guard<std::mutex> lk(g_mu);
     return launch((CUfunction)fn, blocks, 256, 0, st, args);
+}
+
+// Individual species with model code (individual_device.cuh): the drift/diffusivity
+// method and the new-individuals method inside the reference's environment -- the
+// individual as All, every other species a zero dummy (IndividualSolver.cpp:210-238,
+// 258-300), parameters and species names from `defines`, RANDOM a uniform draw.
+int jit_ind_kernels(const std::string& defines, const std::string& drift_code, const std::string& newborn_code,
+                    int num_species, IndKernels* out) {
+    auto env = [&](std::ostringstream& s) {
+        s << "    IndSpecies _d[" << (num_species > 0 ? num_species : 1) << "] = {};\n"
+          << "    IndSpecies* All = &_me;\n"
+          << "    const int GridX = _p.GridX, GridY = _p.GridY;\n"
+          << "    const Real PhysicalX = _p.PhysicalX, PhysicalY = _p.PhysicalY, PhysicalSimTime = _p.PhysicalSimTime;\n"
+          << "    const int GridModelWidth = _a.W, GridModelHeight = _a.H;\n"
+          << "    const Real PhysicalModelWidth = _a.L, PhysicalModelHeight = _a.L;\n"
+          << "    const Real PhysicalCellWidth = _a.L / (float)_a.W, PhysicalCellHeight = _a.L / (float)_a.H;\n"
+          << "    (void)_d; (void)All; (void)GridX; (void)GridY; (void)PhysicalX; (void)PhysicalY;\n"
+          << "    (void)PhysicalSimTime; (void)GridModelWidth; (void)GridModelHeight; (void)PhysicalModelWidth;\n"
+          << "    (void)PhysicalModelHeight; (void)PhysicalCellWidth; (void)PhysicalCellHeight;\n"
+          << "#define SP(i) ((i) == _a.species ? &_me : &_d[(i)])\n";
+    };
+    std::ostringstream s;
+    s << "#include \"individual_device.cuh\"\n"
+      << defines << "\n"
+      << "typedef float Real;\n"
+      << "typedef gpgmp::IndSpecies _species_t;\n"
+      << "namespace gpgmp {\n"
+      << "struct ModelIndDrift {\n"
+      << "  __device__ __forceinline__ void operator()(IndSpecies& _me, const IndArgs& _a, const IndPos& _p) const {\n";
+    env(s);
+    s << "    {\n" << drift_code << "\n    }\n#undef SP\n  }\n};\n"
+      << "struct ModelNewborn {\n"
+      << "  __device__ __forceinline__ void operator()(IndSpecies& _me, const IndArgs& _a, const IndPos& _p,\n"
+      << "                                             Stream& _st) const {\n";
+    env(s);
+    s << "#define RANDOM (::gpgmp::u01(_st.next()))\n"
+      << "    {\n" << newborn_code << "\n    }\n#undef RANDOM\n#undef SP\n  }\n};\n"
+      << "}  // namespace gpgmp\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) gpgmp_ind_sweep(gpgmp::IndArgs a) {\n"
+      << "  gpgmp::ind_sweep_body(a, gpgmp::ModelIndDrift());\n}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) gpgmp_ind_fields(gpgmp::IndArgs a) {\n"
+      << "  gpgmp::ind_fields_body(a, gpgmp::ModelIndDrift());\n}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) gpgmp_ind_newborn(gpgmp::IndArgs a) {\n"
+      << "  gpgmp::ind_newborn_body(a, gpgmp::ModelNewborn());\n}\n";
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::vector<CUfunction> fns;
+    int rc = compile_module(s.str(), {"gpgmp_ind_sweep", "gpgmp_ind_fields", "gpgmp_ind_newborn"}, &fns);
+    if (rc) return rc;
+    out->sweep = (JitFunction)fns[0];
+    out->fields = (JitFunction)fns[1];
+    out->newborn = (JitFunction)fns[2];
+    out->newborn_active = !newborn_code.empty();
+    return GPGMP_OK;
+}
+
+cudaError_t launch_ind_jit(JitFunction fn, const IndArgs& a, long long work, cudaStream_t st) {
+    long long b = (work + 255) / 256;
+    if (b < 1) b = 1;
+    if (b > 148 * 8) b = 148 * 8;
+    IndArgs copy = a;
+    void* args[] = {&copy};
+    std::lock_guard<std::mutex> lk(g_mu);
+    return launch((CUfunction)fn, (unsigned)b, 256, 0, st, args);
 }
 
 }  // namespace gpgmp

@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "host_common.h"
 #include "lookback.cuh"
+#include "sort_kernels.h"
 #include "../../include/gpgmp_c.h"
 
 namespace gpgmp {
@@ -411,6 +412,21 @@ int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t
                               int64_t capacity_out, uint32_t* pool_out, int64_t pool_capacity, uint32_t* start_out,
                               int64_t* n_active_out, int64_t* n_pool_out, void* scratch, size_t scratch_bytes,
                               void* stream) {
+    return gpgmp::population_maintain(keys, ids, n_active, cell_start, cell_count, goal, ncells, pool, n_pool, seed,
+                                      step, keys_out, ids_out, capacity_out, pool_out, pool_capacity, start_out,
+                                      n_active_out, n_pool_out, nullptr, scratch, scratch_bytes, stream);
+}
+
+}  // extern "C"
+
+namespace gpgmp {
+
+int population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n_active, const uint32_t* cell_start,
+                        const uint32_t* cell_count, const int32_t* goal, int64_t ncells, const uint32_t* pool,
+                        int64_t n_pool, uint32_t seed, uint32_t step, uint32_t* keys_out, uint32_t* ids_out,
+                        int64_t capacity_out, uint32_t* pool_out, int64_t pool_capacity, uint32_t* start_out,
+                        int64_t* n_active_out, int64_t* n_pool_out, int64_t* births_out, void* scratch,
+                        size_t scratch_bytes, void* stream) {
     if (n_active < 0 || n_pool < 0 || ncells <= 0 || n_active >= ((int64_t)1 << 31) || ncells >= ((int64_t)1 << 31) ||
         n_pool >= ((int64_t)1 << 31))
         return set_error(GPGMP_ERR_INVALID, "bad sizes");
@@ -456,7 +472,8 @@ int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t
                          (long long)(n_pool - B + K));
     *n_active_out = n_new;
     *n_pool_out = n_pool - B + K;
+    if (births_out) *births_out = B;
     return GPGMP_OK;
 }
 
-}  // extern "C"
+}  // namespace gpgmp

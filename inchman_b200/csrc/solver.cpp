@@ -17,6 +17,7 @@
 #include "kernels.h"
 #include "host_common.h"
 #include "jit.h"
+#include "individual.h"
 
 using namespace gpgmp;
 
@@ -57,6 +58,13 @@ struct gpgmp_solver {
     std::vector<float> dt, next;
     std::vector<float> nextX, nextY, smallX, smallY, ddX, ddY;
     float pi = 0.f, pmove = 0.f, h = 1.f, det_dt = 0.f, stay = 0.f;
+    // individual species (individual.h): one list per flagged species
+    std::vector<uint8_t> is_ind;
+    std::vector<IndList> ind;           // indexed by species (species == -1: not individual)
+    IndKernels ind_k;
+    std::string newind_code;
+    long long ind_cap = 0;
+    float sim_time = 0.f;               // the time of the last diffusion event (the methods' PhysicalSimTime)
 };
 
 namespace {
@@ -134,6 +142,7 @@ void free_all(gpgmp_solver* h) {
                     h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (IndList& l : h->ind) ind_free(l);
 }
 
 int validate(const gpgmp_model_desc* m, int R) {
@@ -168,6 +177,98 @@ int validate(const gpgmp_model_desc* m, int R) {
         if (m->drift_method == GPGMP_DRIFT_CODE && !m->drift_code)
             return set_error(GPGMP_ERR_INVALID, "GPGMP_DRIFT_CODE needs drift_code");
         if (m->flags & 1) return set_error(GPGMP_ERR_UNSUPPORTED, "nonlinear diffusivity recompute");
+    }
+    if (m->individual) {
+        bool any = false;
+        for (int s = 0; s < m->num_species; ++s) any = any || m->individual[s];
+        if (any && m->solver_type != GPGMP_STOCHASTIC_INHOMOGENEOUS && m->solver_type != GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE)
+            return set_error(GPGMP_ERR_UNSUPPORTED, "individual species need a stochastic inhomogeneous solver");
+        if (any && (int64_t)m->width * m->height * R >= ((int64_t)1 << 31))
+            return set_error(GPGMP_ERR_INVALID, "individual species: realisations x cells must stay below 2^31");
+        if (m->individual_capacity < 0) return set_error(GPGMP_ERR_INVALID, "individual_capacity < 0");
+    }
+    return GPGMP_OK;
+}
+
+IndArgs ind_args(gpgmp_solver* h, int species, int dir, float dt, uint32_t step_seed) {
+    IndArgs a{};
+    a.W = h->g.W;
+    a.H = h->g.H;
+    a.S = h->g.S;
+    a.R = h->R;
+    a.species = species;
+    a.dir = dir;
+    a.L = h->m.physical_length;
+    a.dx = h->m.physical_length / (float)(dir == 0 ? h->m.width : h->m.height);
+    a.dt = dt;
+    a.sim_time = h->sim_time;
+    for (int b = 0; b < 4; ++b) a.bmask[b] = h->m.boundary_mask[b];
+    a.seed = h->seed;
+    a.step_seed = step_seed;
+    Planes p = planes_of(h);
+    for (int s = 0; s < h->g.S; ++s) a.planes[s] = p.p[s];
+    return a;
+}
+
+// The smallest time step over every cell of every realisation from a species'
+// individual fields (computeIndividualTimestepX/Y on the fields that
+// computeDiffusionConstants wrote, InhomogeneousSolver.cpp:468-500).
+int ind_timestep(gpgmp_solver* h, const IndList& l, int dir, float* out) {
+    const float dx = h->m.physical_length / (float)(dir == 0 ? h->m.width : h->m.height);
+    const float* D = l.fields + (dir == 0 ? 0 : l.ncells);
+    const float* r = l.fields + (dir == 0 ? 2 : 3) * l.ncells;
+    uint32_t key = 0;
+    CK(launch_timestep((int)l.ncells, D, r, dx, h->d_minkey, h->stream, h->ts_kind, h->stay));
+    CK(cudaMemcpyAsync(&key, h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = key_to_float(key);
+    return GPGMP_OK;
+}
+
+// (Re)builds the individual lists from the state (the caller set it) and takes the
+// first time steps from them (InhomogeneousSolver.cpp:190-211 for individual species).
+int ind_refresh(gpgmp_solver* h, const int32_t* host_state) {
+    if (h->ind.empty()) return GPGMP_OK;
+    const long long ncells = (long long)h->area * h->R;
+    for (int s = 0; s < h->g.S; ++s) {
+        IndList& l = h->ind[s];
+        if (l.species < 0) continue;
+        long long cap = h->ind_cap;
+        if (cap <= 0) {
+            long long n0 = 0;
+            if (host_state) {
+                for (int r = 0; r < h->R; ++r) {
+                    const int32_t* p = host_state + ((size_t)r * h->g.S + s) * h->area;
+                    for (size_t c = 0; c < h->area; ++c) n0 += p[c] > 0 ? p[c] : 0;
+                }
+            } else {
+                std::vector<int32_t> st((size_t)h->area * h->g.S * h->R);
+                int rc = gather_state(h, h->d_stage);
+                if (rc) return rc;
+                CK(cudaMemcpyAsync(st.data(), h->d_stage, st.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                for (int r = 0; r < h->R; ++r)
+                    for (size_t c = 0; c < h->area; ++c) n0 += st[((size_t)r * h->g.S + s) * h->area + c];
+            }
+            cap = 4 * n0 > 65536 ? 4 * n0 : 65536;
+            if (cap >= ((long long)1 << 31)) cap = ((long long)1 << 31) - 1;
+        }
+        if (l.cap != cap || l.ncells != ncells || !l.keys[0]) {
+            int rc = ind_alloc(l, s, cap, ncells);
+            if (rc) return rc;
+        }
+        int rc = ind_build(l, ind_args(h, s, 0, 0.f, 0u), h->ind_k, h->stream);
+        if (rc) return rc;
+        rc = ind_timestep(h, l, 0, &h->smallX[s]);
+        if (rc) return rc;
+        rc = ind_timestep(h, l, 1, &h->smallY[s]);
+        if (rc) return rc;
+        h->ddX[s] = h->smallX[s];
+        h->ddY[s] = h->smallY[s];
+        h->nextX[s] = h->smallX[s];
+        h->nextY[s] = h->smallY[s];
+        h->next[s] = h->nextX[s] < h->nextY[s] ? h->nextX[s] : h->nextY[s];
     }
     return GPGMP_OK;
 }
@@ -266,8 +367,35 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
                 custom = true;
             }
     }
+    h->is_ind.assign(model->num_species, 0);
+    bool any_ind = false;
+    if (model->individual)
+        for (int s = 0; s < model->num_species; ++s) {
+            h->is_ind[s] = model->individual[s] ? 1 : 0;
+            any_ind = any_ind || h->is_ind[s];
+        }
+    if (model->new_individuals_code) h->newind_code = model->new_individuals_code;
+    h->ind_cap = model->individual_capacity;
     h->m.code_defines = h->m.drift_code = nullptr;
     h->m.custom_laws = nullptr;
+    h->m.individual = nullptr;
+    h->m.new_individuals_code = nullptr;
+    if (any_ind) {
+        h->ind.resize(model->num_species);
+        for (int s = 0; s < model->num_species; ++s) h->ind[s].species = h->is_ind[s] ? s : -1;
+        const bool code = model->drift_method == GPGMP_DRIFT_CODE && !h->drift_code.empty();
+        if (code || !h->newind_code.empty()) {
+            // the reference compiles its individual kernels with the model's methods
+            // (IndividualSolver.cpp:188-330)
+            int rc2 = jit_ind_kernels(h->code_defines, code ? h->drift_code : std::string(), h->newind_code,
+                                      model->num_species, &h->ind_k);
+            if (rc2) {
+                delete h;
+                return rc2;
+            }
+            if (!code) h->ind_k.sweep = h->ind_k.fields = nullptr;   // properties as stored
+        }
+    }
     const int ty = model->solver_type;
     h->deterministic = ty == GPGMP_DETERMINISTIC_RK4 || ty == GPGMP_DETERMINISTIC_AQSS ||
                        ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_RK4 || ty == GPGMP_DETERMINISTIC_INHOMOGENEOUS_AQSS;
@@ -401,7 +529,9 @@ int gpgmp_set_state(gpgmp_solver* h, const void* host) {
         std::fill(h->cur.begin(), h->cur.end(), 0);
     }
     CK(cudaStreamSynchronize(h->stream));
-    return refresh_code_fields(h);
+    int rc = refresh_code_fields(h);
+    if (rc) return rc;
+    return h->deterministic ? GPGMP_OK : ind_refresh(h, (const int32_t*)host);
 }
 
 int gpgmp_get_state(gpgmp_solver* h, void* host) {
@@ -431,7 +561,9 @@ int gpgmp_init_poisson(gpgmp_solver* h, const float* lambda) {
     std::fill(h->cur.begin(), h->cur.end(), 0);
     int rc = after_launch(h, launch_init_poisson(h->g, planes_of(h), h->seed, h->d_lambda, h->stream));
     if (rc) return rc;
-    return refresh_code_fields(h);
+    rc = refresh_code_fields(h);
+    if (rc) return rc;
+    return ind_refresh(h, nullptr);
 }
 
 int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
@@ -451,7 +583,15 @@ int gpgmp_do_reactions(gpgmp_solver* h, float deltat, int32_t* seed) {
                                         : launch_ssa(h->g, planes_of(h), h->d_reactions, (int)h->reactions.size(),
                                                      h->seed, (uint32_t)*seed, deltat, h->d_status, h->stream));
     (*seed)++;
-    return rc;
+    if (rc) return rc;
+    // the individual species follow the new counts (Solver.cpp:240-247: one seed each)
+    for (IndList& l : h->ind) {
+        if (l.species < 0) continue;
+        rc = ind_maintain(l, ind_args(h, l.species, 0, 0.f, (uint32_t)*seed), h->ind_k, h->stream);
+        (*seed)++;
+        if (rc) return rc;
+    }
+    return GPGMP_OK;
 }
 
 int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
@@ -506,6 +646,28 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
         h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
         return GPGMP_OK;
     }
+    if (!h->ind.empty() && h->ind[i].species >= 0) {
+        // InhomogeneousSolver::diffuse for an individual species (:264-269, :303-335):
+        // move the individuals, then new fields and a new time step of that direction
+        h->sim_time = t;
+        for (int dir = 0; dir < 2; ++dir) {
+            float& nxt = dir == 0 ? h->nextX[i] : h->nextY[i];
+            if (!(nxt <= t)) continue;
+            float& dd = dir == 0 ? h->ddX[i] : h->ddY[i];
+            float& small = dir == 0 ? h->smallX[i] : h->smallY[i];
+            const float dxd = h->m.physical_length / (float)(dir == 0 ? h->m.width : h->m.height);
+            float ndt = 0.f;
+            int rc = ind_sweep(h->ind[i], ind_args(h, i, dir, dd, (uint32_t)*seed), h->ind_k, dxd, h->ts_kind, h->stay,
+                               h->d_minkey, &ndt, h->stream);
+            if (rc) return rc;
+            (*seed)++;
+            small = ndt;
+            nxt += small;
+            dd = small;
+        }
+        h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
+        return GPGMP_OK;
+    }
     if (h->nextX[i] <= t) {
         const int c = h->cur[i];
         int rc = after_launch(h, launch_sweep(h->g, h->d_buf[c], h->d_buf[1 - c], i, 0, h->seed, (uint32_t)*seed,
@@ -540,6 +702,67 @@ int gpgmp_timesteps(gpgmp_solver* h, float* dtx, float* dty) {
     if (!h || !dtx || !dty) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (!h->inhom) return set_error(GPGMP_ERR_INVALID, "time steps per direction exist for the inhomogeneous solver");
     for (int i = 0; i < h->g.S; ++i) { dtx[i] = h->smallX[i]; dty[i] = h->smallY[i]; }
+    return GPGMP_OK;
+}
+
+int gpgmp_individual_count(gpgmp_solver* h, int32_t species, int64_t* n) {
+    if (!h || !n) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (species < 0 || species >= h->g.S || h->ind.empty() || h->ind[species].species < 0)
+        return set_error(GPGMP_ERR_INVALID, "species %d is not an individual species", species);
+    *n = h->ind[species].n;
+    return GPGMP_OK;
+}
+
+int gpgmp_get_individuals(gpgmp_solver* h, int32_t species, uint32_t* keys, uint32_t* ids, float* props,
+                          int64_t capacity, int64_t* n) {
+    int rc = gpgmp_individual_count(h, species, n);
+    if (rc) return rc;
+    const IndList& l = h->ind[species];
+    const long long m = l.n < capacity ? l.n : (capacity > 0 ? capacity : 0);
+    if (m > 0 && keys)
+        CK(cudaMemcpyAsync(keys, l.keys[l.cur], sizeof(uint32_t) * m, cudaMemcpyDeviceToHost, h->stream));
+    if (m > 0 && (ids || props)) {
+        std::vector<uint32_t> hid(m);
+        CK(cudaMemcpyAsync(hid.data(), l.ids[l.cur], sizeof(uint32_t) * m, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (ids) std::memcpy(ids, hid.data(), sizeof(uint32_t) * m);
+        if (props) {
+            std::vector<float> all((size_t)4 * l.cap);
+            CK(cudaMemcpyAsync(all.data(), l.props, sizeof(float) * all.size(), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (int q = 0; q < 4; ++q)
+                for (long long i = 0; i < m; ++i) props[q * capacity + i] = all[(size_t)q * l.cap + hid[i]];
+        }
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+int gpgmp_set_individual_properties(gpgmp_solver* h, int32_t species, const float* props, int64_t first_id,
+                                    int64_t count) {
+    int64_t n = 0;
+    int rc = gpgmp_individual_count(h, species, &n);
+    if (rc) return rc;
+    IndList& l = h->ind[species];
+    if (!props || first_id < 0 || count < 0 || first_id + count > l.cap)
+        return set_error(GPGMP_ERR_INVALID, "ids %lld..%lld outside the capacity %lld", (long long)first_id,
+                         (long long)(first_id + count - 1), (long long)l.cap);
+    for (int q = 0; q < 4; ++q)
+        CK(cudaMemcpyAsync(l.props + (size_t)q * l.cap + first_id, props + (size_t)q * count, sizeof(float) * count,
+                           cudaMemcpyHostToDevice, h->stream));
+    // the fields and the next time steps follow the properties (as after the
+    // reference's init script)
+    rc = ind_fields(l, ind_args(h, species, 0, 0.f, 0u), h->ind_k, h->stream);
+    if (rc) return rc;
+    rc = ind_timestep(h, l, 0, &h->smallX[species]);
+    if (rc) return rc;
+    rc = ind_timestep(h, l, 1, &h->smallY[species]);
+    if (rc) return rc;
+    h->ddX[species] = h->smallX[species];
+    h->ddY[species] = h->smallY[species];
+    h->nextX[species] = h->sim_time + h->smallX[species];
+    h->nextY[species] = h->sim_time + h->smallY[species];
+    h->next[species] = h->nextX[species] < h->nextY[species] ? h->nextX[species] : h->nextY[species];
     return GPGMP_OK;
 }
 

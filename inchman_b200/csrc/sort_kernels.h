@@ -29,4 +29,13 @@ cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t nce
 cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t ncells, uint32_t* left,
                            uint32_t* right, cudaStream_t st);
 
+// gpgmp_population_maintain with the number of individuals created (births_out,
+// may be NULL): they took the first births_out ids of the old pool (population.cu)
+int population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n_active, const uint32_t* cell_start,
+                        const uint32_t* cell_count, const int32_t* goal, int64_t ncells, const uint32_t* pool,
+                        int64_t n_pool, uint32_t seed, uint32_t step, uint32_t* keys_out, uint32_t* ids_out,
+                        int64_t capacity_out, uint32_t* pool_out, int64_t pool_capacity, uint32_t* start_out,
+                        int64_t* n_active_out, int64_t* n_pool_out, int64_t* births_out, void* scratch,
+                        size_t scratch_bytes, void* stream);
+
 }  // namespace gpgmp

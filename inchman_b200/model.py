@@ -27,6 +27,7 @@ class Species:
     id: str
     diffusion: float = 0.0
     initial: float = 0.0          # mean initial count per cell (Poisson) or amount
+    individual: bool = False      # molecules tracked one by one (IndividualSolver)
 
 
 @dataclass
@@ -83,10 +84,14 @@ class DiffusionModel:
     code_defines: Optional[str] = None
     drift_code: Optional[str] = None
     custom_laws: Optional[List[Optional[str]]] = None
+    # individual species (gpgmp_model_desc.individual_capacity / new_individuals_code)
+    individual_capacity: int = 0
+    new_individuals_code: Optional[str] = None
 
     # -- builders (DiffusionModel.cpp:426-493) --------------------------------
-    def add_species(self, id: str, diffusion: float = 0.0, initial: float = 0.0) -> "DiffusionModel":
-        self.species.append(Species(id, diffusion, initial))
+    def add_species(self, id: str, diffusion: float = 0.0, initial: float = 0.0,
+                    individual: bool = False) -> "DiffusionModel":
+        self.species.append(Species(id, diffusion, initial, individual))
         return self
 
     def add_reaction(self, id: str, reactants: Dict[str, int], products: Dict[str, int], rate: float):
@@ -169,6 +174,15 @@ class DiffusionModel:
             b = self.drift_code.encode()
             keep.append(b)
             d.drift_code = b
+        if any(sp.individual for sp in self.species):
+            flags = np.ascontiguousarray([1 if sp.individual else 0 for sp in self.species], dtype=np.uint8)
+            keep.append(flags)
+            d.individual = flags.ctypes.data_as(C.POINTER(C.c_uint8))
+            d.individual_capacity = int(self.individual_capacity)
+            if self.new_individuals_code:
+                b = self.new_individuals_code.encode()
+                keep.append(b)
+                d.new_individuals_code = b
         if self.custom_laws is not None:
             if len(self.custom_laws) != len(self.reactions):
                 raise ValueError("custom_laws needs one entry (or None) per reaction")

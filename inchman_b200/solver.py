@@ -107,6 +107,33 @@ class Solver:
                   dy.ctypes.data_as(C.POINTER(C.c_float)))
         return dx, dy
 
+    # -- individual species (IndividualSolver) --------------------------------------
+    def individual_count(self, species: int) -> int:
+        n = C.c_int64(0)
+        _lib.call("gpgmp_individual_count", self._h, int(species), C.byref(n))
+        return n.value
+
+    def get_individuals(self, species: int):
+        """(keys, ids, props): keys r * area + cell in list order (sorted), ids, and
+        props [4][n] = DiffusivityX, DiffusivityY, DriftX, DriftY."""
+        n = self.individual_count(species)
+        keys = np.empty(n, np.uint32)
+        ids = np.empty(n, np.uint32)
+        props = np.empty((4, n), np.float32)
+        got = C.c_int64(0)
+        _lib.call("gpgmp_get_individuals", self._h, int(species), keys.ctypes.data_as(C.c_void_p),
+                  ids.ctypes.data_as(C.c_void_p), props.ctypes.data_as(C.c_void_p), n, C.byref(got))
+        return keys, ids, props
+
+    def set_individual_properties(self, species: int, props, first_id: int = 0):
+        """props [4][count] for ids first_id ..: DiffusivityX, DiffusivityY, DriftX, DriftY
+        (what the reference's init scripts set through individualProperties)."""
+        a = np.ascontiguousarray(props, dtype=np.float32)
+        if a.ndim != 2 or a.shape[0] != 4:
+            raise ValueError("props must be [4][count]")
+        _lib.call("gpgmp_set_individual_properties", self._h, int(species), a.ctypes.data_as(C.c_void_p),
+                  int(first_id), a.shape[1])
+
     def status(self) -> np.ndarray:
         out = np.zeros(self.R, dtype=np.int32)
         _lib.call("gpgmp_get_status", self._h, out.ctypes.data_as(C.POINTER(C.c_int32)))

@@ -123,6 +123,21 @@ typedef struct gpgmp_model_desc {
     const char* code_defines;
     const char* drift_code;
     const char* const* custom_laws;
+    /* Individual species (IndividualSolver.cpp, IndividualSolver.cl): individual[s] != 0
+     * tracks the molecules of species s one by one -- a cell-sorted list of
+     * individuals, each with an id and four properties (DiffusivityX, DiffusivityY,
+     * DriftX, DriftY) -- in the stochastic inhomogeneous solvers.  NULL: none.
+     *  individual_capacity: the most individuals one species may have over all
+     *                       realisations (0: four times the initial count, at least
+     *                       65,536);
+     *  new_individuals_code: statements setting All->... of an individual a reaction
+     *                       window created (the newIndividualsMethod; RANDOM is a
+     *                       uniform draw), or NULL to keep the properties its id has.
+     * With GPGMP_DRIFT_CODE the drift method runs per individual on its properties;
+     * with a built-in method the individuals move with their properties as stored. */
+    const uint8_t* individual;
+    int64_t individual_capacity;
+    const char* new_individuals_code;
 } gpgmp_model_desc;
 
 typedef struct gpgmp_solver gpgmp_solver;
@@ -165,6 +180,21 @@ int gpgmp_synchronize(gpgmp_solver* h);
 void* gpgmp_device_state(gpgmp_solver* h);
 /* computeTimestepX/Y + reduceBlocks + readback -- InhomogeneousSolver.cpp:468-500 */
 int gpgmp_timesteps(gpgmp_solver* h, float* dt_x, float* dt_y);
+/* Individual species.  Keys are r * width * height + cell (realisation r), sorted;
+ * the reference's output pairs are key | id << 32 (IndividualSolver.h:6-9,
+ * getPositionList, IndividualSolver.cpp:1295-1318).
+ *  gpgmp_individual_count: the individuals of species s now (all realisations);
+ *  gpgmp_get_individuals:  up to capacity of them in list order -- keys, ids and the
+ *                          properties [4][capacity] (any output may be NULL);
+ *  gpgmp_set_individual_properties: properties [4][count] of ids first_id ..
+ *                          first_id + count - 1 (the initial individuals are ids 0..
+ *                          in cell order, as the reference's init scripts set them);
+ *                          the next time steps follow the new properties. */
+int gpgmp_individual_count(gpgmp_solver* h, int32_t species, int64_t* n);
+int gpgmp_get_individuals(gpgmp_solver* h, int32_t species, uint32_t* keys, uint32_t* ids, float* props,
+                          int64_t capacity, int64_t* n);
+int gpgmp_set_individual_properties(gpgmp_solver* h, int32_t species, const float* props, int64_t first_id,
+                                    int64_t count);
 
 
 /* ---- deterministic reaction-diffusion: Gray-Scott, forward and adjoint ----------

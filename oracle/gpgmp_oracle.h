@@ -57,6 +57,9 @@ typedef struct orc_model {
     const char* code_defines;          /* run-time model code (the product compiles it with NVRTC; */
     const char* drift_code;            /* the oracle takes custom hazards through orc_set_custom_hazard) */
     const char* const* custom_laws;
+    const uint8_t* individual;         /* individual species (the product's lists; the oracle restates */
+    int64_t individual_capacity;       /* their steps in orc_individual.c) */
+    const char* new_individuals_code;
 } orc_model;
 
 /* ---- generators and elementary functions ---------------------------------- */
@@ -95,6 +98,10 @@ void orc_rep_inhomog_sweep(const orc_model* m, int32_t* state, int R, uint32_t s
 float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float* dfield, const float* rfield);
 void orc_rep_diffusivity_drift(const orc_model* m, int species, float* dx, float* dy, float* rx, float* ry);
 void orc_set_custom_hazard(float (*fn)(int r, const int32_t* x));
+int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int dir, float dt,
+                          uint32_t step_seed, uint32_t* keys, uint32_t* ids, int64_t n, const float* props,
+                          int64_t cap, float* fields, uint32_t* killed_ids, int64_t* n_killed);
+float orc_rep_timestep_cells(const float* D, const float* r, int64_t n, float dx);
 int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
                   int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots,
                   int64_t* steps, int32_t* status);

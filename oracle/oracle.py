@@ -65,6 +65,9 @@ def orc():
             "orc_rep_homog_diffuse": (None, [vp, vp, C.c_int, u32, C.c_int, u32]),
             "orc_rep_inhomog_sweep": (None, [vp, vp, C.c_int, u32, C.c_int, C.c_int, u32, f32, vp, vp]),
             "orc_rep_timestep": (f32, [vp, C.c_int, C.c_int, vp, vp]),
+            "orc_rep_ind_sweep": (C.c_int64, [vp, vp, C.c_int, C.c_uint32, C.c_int, C.c_int, f32, C.c_uint32, vp, vp,
+                                              C.c_int64, vp, C.c_int64, vp, vp, vp]),
+            "orc_rep_timestep_cells": (f32, [vp, vp, C.c_int64, f32]),
             "orc_rep_diffusivity_drift": (None, [vp, C.c_int, vp, vp, vp, vp]),
             "orc_rep_solve": (C.c_int, [vp, vp, C.c_int, u32, vp, vp, C.c_int, P(C.c_int), P(i64), vp]),
             "orc_gs_forward_f32": (None, [C.c_int, C.c_int, f32, f32, f32, f32, f32, f32, f32, vp, vp]),

@@ -435,3 +435,92 @@ int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
     free(Fdx); free(Fdy); free(Frx); free(Fry);
     return 0;
 }
+
+/* ---- individual species ------------------------------------------------------------
+ * One sweep of an individual species with the properties as stored (no model code),
+ * restating individual_device.cuh (ind_sweep_body, ind_fields_body, ind_counts_body)
+ * and individual.cu (ind_sweep) after the reference's individual_diffuseX/Y,
+ * computeDiffusionConstants and computeCellIndices (IndividualSolver.cl:654-1015,
+ * IndividualSolver.cpp:1083-1153): every individual draws once (stream (seed, r),
+ * counter (step_seed, id, PH_INDIV | species << 8 | dir)) and moves one cell with the
+ * inhomogeneous sweep's probabilities of its own D and r, reflecting walls cancel the
+ * move, absorbing walls remove it; then the stable sort by key, the counts into the
+ * species' planes and the fields [4][R*area] (largest D x, D y, |r x|, |r y| per cell).
+ * keys/ids: the list (sorted by key = r*area + cell), updated in place; removed ids are
+ * written to killed_ids (list order).  Returns the new list length. */
+int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int dir, float dt,
+                          uint32_t step_seed, uint32_t* keys, uint32_t* ids, int64_t n, const float* props,
+                          int64_t cap, float* fields, uint32_t* killed_ids, int64_t* n_killed) {
+    const int W = m->width, H = m->height, S = m->num_species;
+    const int64_t area = (int64_t)W * H, ncells = area * R;
+    const float dx = m->physical_length / (float)(dir == 0 ? W : H);
+    const uint32_t killed = (uint32_t)ncells;
+    for (int64_t i = 0; i < n; ++i) {
+        const uint32_t key = keys[i], id = ids[i];
+        const int r = (int)(key / area);
+        const int cell = (int)(key - (int64_t)r * area);
+        const int gx = cell % W, gy = cell / W;
+        const float D = props[(dir == 0 ? 0 : 1) * cap + id];
+        const float v = props[(dir == 0 ? 2 : 3) * cap + id];
+        float Pp, Pm;
+        rep_sweep_probs(D, v, dt, dx, &Pp, &Pm);
+        orc_stream s;
+        orc_stream_init(&s, seed, (uint32_t)r, step_seed, id, ORC_PH_INDIV | ((uint32_t)species << 8) | (uint32_t)dir);
+        const float u = orc_u01(orc_stream_next(&s));
+        const int mv = u < Pp ? 1 : (u < Pp + Pm ? -1 : 0);
+        if (mv == 0) continue;
+        const int c = dir == 0 ? gx : gy, lim = dir == 0 ? W : H, nc = c + mv;
+        if (nc < 0 || nc >= lim) {
+            const int wall = (dir == 0 ? 0 : 2) + (mv > 0 ? 1 : 0);
+            if (m->boundary_mask[wall] == 0) continue;
+            keys[i] = killed;
+        } else {
+            const int ncell = dir == 0 ? gy * W + nc : nc * W + gx;
+            keys[i] = (uint32_t)((int64_t)r * area + ncell);
+        }
+    }
+    /* stable sort by key: counting sort over ncells + 1 bins */
+    int64_t* cnt = (int64_t*)calloc((size_t)ncells + 2, sizeof(int64_t));
+    uint32_t* k2 = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    uint32_t* i2 = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    for (int64_t i = 0; i < n; ++i) cnt[keys[i] + 1]++;
+    for (int64_t b = 0; b <= ncells; ++b) cnt[b + 1] += cnt[b];
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t o = cnt[keys[i]]++;
+        k2[o] = keys[i];
+        i2[o] = ids[i];
+    }
+    int64_t alive = 0, nk = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (k2[i] == killed) killed_ids[nk++] = i2[i];
+        else { keys[alive] = k2[i]; ids[alive] = i2[i]; ++alive; }
+    }
+    *n_killed = nk;
+    /* fields (State before the counts change is not used without model code) and counts */
+    for (int64_t k = 0; k < ncells; ++k) fields[k] = fields[ncells + k] = fields[2 * ncells + k] = fields[3 * ncells + k] = 0.f;
+    for (int64_t k = 0; k < ncells; ++k) {
+        const int r = (int)(k / area);
+        state[((int64_t)r * S + species) * area + (k - (int64_t)r * area)] = 0;
+    }
+    for (int64_t i = 0; i < alive; ++i) {
+        const uint32_t k = keys[i], id = ids[i];
+        const int r = (int)(k / area);
+        state[((int64_t)r * S + species) * area + (k - (int64_t)r * area)] += 1;
+        fields[k] = fmaxf(fields[k], props[id]);
+        fields[ncells + k] = fmaxf(fields[ncells + k], props[cap + id]);
+        fields[2 * ncells + k] = fmaxf(fields[2 * ncells + k], fabsf(props[2 * cap + id]));
+        fields[3 * ncells + k] = fmaxf(fields[3 * ncells + k], fabsf(props[3 * cap + id]));
+    }
+    free(cnt); free(k2); free(i2);
+    return alive;
+}
+
+/* the smallest time step over n cells of fields D, r (the stochastic formula) */
+float orc_rep_timestep_cells(const float* D, const float* r, int64_t n, float dx) {
+    float best = INFINITY;
+    for (int64_t c = 0; c < n; ++c) {
+        float ts = orc_cell_timestep(D[c], r[c], dx);
+        if (ts == ts) best = fminf(best, ts);
+    }
+    return best;
+}

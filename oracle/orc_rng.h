@@ -100,5 +100,7 @@ static inline uint32_t orc_stream_next(orc_stream* s) {
 #define ORC_PH_PART   0x05000000u
 #define ORC_PH_PAIR   0x06000000u
 #define ORC_PH_POP    0x07000000u
+#define ORC_PH_INDIV  0x08000000u
+#define ORC_PH_NEWIND 0x09000000u
 
 #endif
