@@ -81,6 +81,10 @@ class ModelDesc(C.Structure):
     ]
 
 
+# int (*)(void* user, int32_t index, float time)
+DUMP_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_float)
+
+
 class GpgmpError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         super().__init__(f"{func} failed ({ERRORS.get(code, code)}): {msg}")
@@ -116,6 +120,7 @@ SIGNATURES = {
     "gpgmp_device_state": (vp, [vp]),
     "gpgmp_timesteps": (C.c_int, [vp, P(f32), P(f32)]),
     "gpgmp_individual_count": (C.c_int, [vp, i32, P(i64)]),
+    "gpgmp_solve_with_callback": (C.c_int, [vp, vp, P(f32), i32, P(i32), P(i64), vp, vp]),
     "gpgmp_get_individuals": (C.c_int, [vp, i32, vp, vp, vp, i64, P(i64)]),
     "gpgmp_set_individual_properties": (C.c_int, [vp, i32, vp, i64, i64]),
 }

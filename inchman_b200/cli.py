@@ -15,7 +15,9 @@ InchmanDiffusionModel.cpp:240-274, doc/source/hdf5.rst) with inchman_b200.h5:
   /Runs/<run>/Dump_<time>     attribute time (float32[1]); one dataset per species,
                               dims [gridWidth, gridHeight] over the state buffer
                               (int32 counts, float32 for deterministic solvers);
-                              an empty Individuals group
+                              an Individuals group: per individual species its
+                              (cell | id << 32) uint64 list and four float32
+                              property lists (empty without individual species)
 
 Dumps are named by the time printed with 9 significant digits (the reference's
 boost::lexical_cast of a float): Dump_0, Dump_1, Dump_0.100000001, ...  They are taken
@@ -45,8 +47,15 @@ def dump_name(t: float) -> str:
     return "Dump_" + ("%.9g" % float(np.float32(t)))
 
 
-def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray) -> h5.Group:
-    """The reference's file layout for snapshots [n][runs][S][H][W] at times [n]."""
+PROPERTY_NAMES = ("DiffusivityX", "DiffusivityY", "DriftX", "DriftY")
+
+
+def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray, individuals=None) -> h5.Group:
+    """The reference's file layout for snapshots [n][runs][S][H][W] at times [n].
+    individuals[k][species] = (keys, ids, props [4][n]) of dump k (keys r * area + cell):
+    written per run as /Individuals/<species> (uint64 cell | id << 32, the reference's
+    getPositionList) and <species>.DiffusivityX/Y, .DriftX/Y (float32, in the same
+    order as the positions)."""
     m = lm.model
     S, H, W = m.num_species, m.height, m.width
     runs = snaps.shape[1]
@@ -75,12 +84,25 @@ def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray) -> h
                 # the state buffer of one species as the reference hands it to HDF5:
                 # dims [gridWidth, gridHeight] over the bytes of the [H][W] plane
                 d.create_dataset(sp.id, np.ascontiguousarray(snaps[k, r, s]).reshape(W, H))
-            d.create_group("Individuals")
+            ig = d.create_group("Individuals")
+            if individuals is None:
+                continue
+            area = W * H
+            for s_idx, (keys, ids, props) in individuals[k].items():
+                sel = (keys // area) == r
+                if not sel.any():
+                    continue
+                sid = m.species[s_idx].id
+                pairs = (keys[sel] % area).astype(np.uint64) | (ids[sel].astype(np.uint64) << np.uint64(32))
+                ig.create_dataset(sid, pairs)
+                for q, pname in enumerate(PROPERTY_NAMES):
+                    ig.create_dataset(f"{sid}.{pname}", np.ascontiguousarray(props[q][sel], dtype=np.float32))
     return root
 
 
 def run(lm: sbml.LoadedModel, seed: int):
-    """Runs the model; returns (snapshots [n][runs][S][H][W], times [n], steps)."""
+    """Runs the model; returns (snapshots [n][runs][S][H][W], times [n], steps,
+    individuals per dump or None)."""
     from .solver import Solver
     m = lm.model
     det = m.solver in _lib.DETERMINISTIC_TYPES
@@ -92,10 +114,17 @@ def run(lm: sbml.LoadedModel, seed: int):
         nmax = int(np.floor(m.max_time / m.output_interval)) + 4
     else:
         nmax = 4
+    ind_species = [i for i, sp in enumerate(m.species) if sp.individual]
+    individuals = []
     with Solver(m, realisations=R, seed=seed) as s:
         s.set_state(state)
-        snaps, times, steps = s.solve(max_snapshots=nmax)
-    return snaps, times, steps
+        if ind_species:
+            def on_dump(index, t):
+                individuals.append({i: s.get_individuals(i) for i in ind_species})
+            snaps, times, steps = s.solve(max_snapshots=nmax, on_dump=on_dump)
+        else:
+            snaps, times, steps = s.solve(max_snapshots=nmax)
+    return snaps, times, steps, (individuals[:len(times)] if ind_species else None)
 
 
 def main(argv: Optional[list] = None) -> int:
@@ -123,9 +152,9 @@ def main(argv: Optional[list] = None) -> int:
     for n in lm.notes:
         print(f"note: {n}", file=sys.stderr)
     t0 = time.perf_counter()
-    snaps, times, steps = run(lm, seed)
+    snaps, times, steps, individuals = run(lm, seed)
     t1 = time.perf_counter()
-    h5.write(args.output, output_tree(lm, snaps, times))
+    h5.write(args.output, output_tree(lm, snaps, times, individuals))
     print(f"{args.model_file}: {snaps.shape[1]} run(s), {len(times)} dumps, {steps} steps in {t1 - t0:.3f} s "
           f"-> {args.output}", file=sys.stderr)
     return 0

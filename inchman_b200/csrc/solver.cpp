@@ -785,6 +785,11 @@ int gpgmp_synchronize(gpgmp_solver* h) {
 // reference does.  Output events take two passes of the loop (the first only
 // re-arms, :1555-1571), and ties between events go to diffusion.
 int gpgmp_solve(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_snaps, int32_t* nsnap, int64_t* steps) {
+    return gpgmp_solve_with_callback(h, snaps, snap_times, max_snaps, nsnap, steps, nullptr, nullptr);
+}
+
+int gpgmp_solve_with_callback(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_snaps, int32_t* nsnap,
+                              int64_t* steps, gpgmp_dump_callback on_dump, void* user) {
     if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
     const int S = h->g.S;
     const size_t elem = h->deterministic ? sizeof(float) : sizeof(int32_t);
@@ -803,6 +808,10 @@ int gpgmp_solve(gpgmp_solver* h, void* snaps, float* snap_times, int32_t max_sna
             CK(cudaStreamSynchronize(h->stream));
         }
         if (snap_times && ns < max_snaps) snap_times[ns] = t;
+        if (on_dump) {
+            CK(cudaStreamSynchronize(h->stream));
+            if (on_dump(user, ns, t) != 0) return set_error(GPGMP_ERR_INVALID, "the dump callback failed");
+        }
         ns++;
         return GPGMP_OK;
     };

@@ -20,9 +20,13 @@ as a C expression and compiled into the SSA kernel at run time (custom_laws).  T
 drift/diffusivity method is C code; it is compiled at run time as well (DRIFT_CODE),
 with the parameters as defines and every species id bound to SP(i).
 
+Individual species (<im:individual/>) become individual species of the solver, with the
+newIndividualsMethod compiled at run time; their properties start at zero, as the
+reference's do without an init script.
+
 Not supported (raises Unsupported): init and event scripts (Python run by the
-reference's executable), individual species, field parameters, reactions localised to
-part of the grid, nonlinear drift methods that read the state, time or moments.
+reference's executable), field parameters, reactions localised to part of the grid,
+nonlinear drift methods that read the state, time or moments.
 """
 from __future__ import annotations
 
@@ -232,7 +236,7 @@ _IDENT = re.compile(r"[A-Za-z_][A-Za-z0-9_]*")
 
 def drift_identifiers(code: str) -> set:
     c = _COMMENT.sub(" ", code)
-    c = re.sub(r"\d+\.?\d*([eE][-+]?\d+)?[fF]?", " ", c)
+    c = re.sub(r"(?<![A-Za-z_0-9])\.?\d+\.?\d*([eE][-+]?\d+)?[fF]?", " ", c)   # numbers, not B00's digits
     return set(_IDENT.findall(c))
 
 
@@ -326,6 +330,8 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
         sf = sb.find(f"{IM}setField/{IM}method")
         if sf is not None and _text(sf):
             raise Unsupported("setField method (field parameters)")
+        ni = sb.find(f"{IM}newIndividualsMethod/{IM}method")
+        newind = _text(ni) if ni is not None else ""
     ma = model_e.find(f"{SB}annotation/{IM}model")
     if ma is not None:
         for name, attr in (("gridWidth", "width"), ("gridHeight", "height")):
@@ -359,7 +365,8 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
         m.add_species(sid, float(D or 0.0))
         if a is not None:
             if a.find(IM + "individual") is not None:
-                raise Unsupported(f"individual species {sid!r}")
+                # InchmanDiffusionModel.cpp:345-350: the molecules become individuals
+                m.species[-1].individual = True
             lst = a.find(IM + "listOfCompartmentParameters")
             for cp in (lst if lst is not None else []):
                 cid = cp.get("compartment")
@@ -425,4 +432,10 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
         m.code_defines = "\n".join(defines)
     elif m.custom_laws is not None:
         m.code_defines = "\n".join(f"#define {k} {c_float(v)}" for k, v in params.items())
+    if any(sp.individual for sp in m.species):
+        if m.solver not in (_lib.STOCHASTIC_INHOMOGENEOUS, _lib.STOCHASTIC_INHOMOGENEOUS_FPE):
+            raise Unsupported("individual species with a solver other than stochastic_inhomogeneous(_fpe)")
+        if newind and _COMMENT.sub(" ", newind).strip():
+            m.new_individuals_code = newind
+        notes.append("individual species: " + ", ".join(sp.id for sp in m.species if sp.individual))
     return LoadedModel(model=m, runs=runs, parameters=params, notes=notes, compartments=comps, source=text)

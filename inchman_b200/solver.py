@@ -142,8 +142,36 @@ class Solver:
     def synchronize(self):
         _lib.call("gpgmp_synchronize", self._h)
 
-    def solve(self, max_snapshots: int = 0, count_only: bool = False):
-        """Runs the oclSolve event loop; returns (snapshots, times, steps)."""
+    def solve(self, max_snapshots: int = 0, count_only: bool = False, on_dump=None):
+        """Runs the oclSolve event loop; returns (snapshots, times, steps).  on_dump(index,
+        time) is called at every dump, when the solver's state and individual lists are
+        those of the dump (the reference's writeAllSpecies)."""
+        if on_dump is not None:
+            snaps = np.zeros((max(1, max_snapshots),) + self.shape, dtype=self.dtype)
+            times = np.zeros(max(1, max_snapshots), dtype=np.float32)
+            ns = C.c_int32(0)
+            steps = C.c_int64(0)
+            errors = []
+
+            def cb(_user, index, t):
+                try:
+                    on_dump(int(index), float(t))
+                    return 0
+                except Exception as e:       # reported after the run
+                    errors.append(e)
+                    return 1
+
+            fn = _lib.DUMP_CALLBACK(cb)
+            try:
+                _lib.call("gpgmp_solve_with_callback", self._h, snaps.ctypes.data_as(C.c_void_p),
+                          times.ctypes.data_as(C.POINTER(C.c_float)), max_snapshots, C.byref(ns), C.byref(steps),
+                          C.cast(fn, C.c_void_p), None)
+            except _lib.GpgmpError:
+                if errors:
+                    raise errors[0]
+                raise
+            n = min(ns.value, max_snapshots)
+            return snaps[:n], times[:n], steps.value
         if count_only or max_snapshots == 0:
             ns = C.c_int32(0)
             steps = C.c_int64(0)

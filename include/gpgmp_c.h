@@ -172,6 +172,13 @@ int gpgmp_next_diffusion_time(gpgmp_solver* h, float* out_per_species);
  * final state; snapshots has room for max_snapshots states (NULL to count only). */
 int gpgmp_solve(gpgmp_solver* h, void* snapshots, float* snapshot_times, int32_t max_snapshots,
                 int32_t* num_snapshots, int64_t* steps);
+/* gpgmp_solve, calling on_dump(user, index, time) at every dump (after its snapshot
+ * is copied), where the caller may read the state or the individual lists (the
+ * reference's writeAllSpecies, DiffusionModel.cpp:1096-1260); a non-zero return ends
+ * the run with an error. */
+typedef int (*gpgmp_dump_callback)(void* user, int32_t index, float time);
+int gpgmp_solve_with_callback(gpgmp_solver* h, void* snapshots, float* snapshot_times, int32_t max_snapshots,
+                              int32_t* num_snapshots, int64_t* steps, gpgmp_dump_callback on_dump, void* user);
 /* per-realisation GPGMP_SIM_* bits; the reference's debug error buffer
  * (Gillespie.cl:86-98, Solver.cpp:274-295) turned into a status word */
 int gpgmp_get_status(gpgmp_solver* h, int32_t* status_per_realisation);

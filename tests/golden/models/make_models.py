@@ -14,7 +14,8 @@ def num(v):
     return f'<math:math xmlns:math="{MML}"><math:cn>{v}</math:cn></math:math>'
 
 
-def document(name, solver, W, L, time, out, params, comps, species, reactions, method=""):
+def document(name, solver, W, L, time, out, params, comps, species, reactions, method="", newind=None,
+             individual=()):
     ps = "\n".join(f'      <parameter id="{k}" value="{v}"><annotation><im:parameter xmlns:im="{IMNS}" '
                    f'type="float" domain="single"/></annotation></parameter>' for k, v in params.items())
     cs = "\n".join(f'      <compartment id="{cid}"><annotation><im:compartment xmlns:im="{IMNS}">'
@@ -28,6 +29,7 @@ def document(name, solver, W, L, time, out, params, comps, species, reactions, m
         ss.append(f'      <species id="{sid}" compartment="World"><annotation><im:species xmlns:im="{IMNS}">'
                   f'<im:diffusionConstant>{num(D)}</im:diffusionConstant>'
                   f'<im:listOfCompartmentParameters>{cp}</im:listOfCompartmentParameters>'
+                  + ('<im:individual/>' if sid in individual else '') +
                   f'</im:species></annotation></species>')
     rs = []
     for rid, (re_, pr, law) in reactions.items():
@@ -49,7 +51,7 @@ def document(name, solver, W, L, time, out, params, comps, species, reactions, m
   <im:init type="python"><im:script><![CDATA[]]></im:script></im:init>
   <im:events type="python"><im:script><![CDATA[]]></im:script><im:listOfTimeStamps/></im:events>
   <im:driftDiffusivity nonLinear="false" computeMoments=""><im:method><![CDATA[{method}]]></im:method></im:driftDiffusivity>
-</im:sbml></annotation>
+{"" if newind is None else f"  <im:newIndividualsMethod><im:method><![CDATA[{newind}]]></im:method></im:newIndividualsMethod>" + chr(10)}</im:sbml></annotation>
   <model name="{name}">
 <annotation><im:model xmlns:im="{IMNS}"><im:gridWidth>{num(W)}</im:gridWidth><im:gridHeight>{num(W)}</im:gridHeight>
 <im:physicalWidth>{num(L)}</im:physicalWidth><im:physicalHeight>{num(L)}</im:physicalHeight></im:model></annotation>
@@ -112,7 +114,18 @@ def main():
         {"S": (0.5, {"World": 64 * 30}), "P": (0.2, {})},
         {"prod": ({}, {"P": 1}, divide(times(ci("vmax"), ci("S")), plus(ci("km"), ci("S")))),
          "deg": ({"S": 1}, {}, times(ci("kd"), ci("S")))})
-    for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm)):
+    # individual species: A tracked one by one (decays, made from B), drift per
+    # individual, new individuals with a random drift
+    ind = document(
+        "Individual A", "stochastic_inhomogeneous", 16, 16.0, 0.6, 0.2, {"kd": 0.5, "km": 0.2},
+        {"World": (0, 0, 16, 16)},
+        {"A": (0.0, {"World": 16 * 16 * 6}), "B": (0.5, {"World": 16 * 16 * 3})},
+        {"decay": ({"A": 1}, {}, times(ci("kd"), ci("A"))),
+         "make": ({"B": 1}, {"A": 1, "B": 1}, times(ci("km"), ci("B")))},
+        method="A->DiffusivityX = 0.8;\nA->DiffusivityY = 0.6;\nA->DriftX = A->DriftX + 0.1;\nA->DriftY = 0.0;\n"
+               "B->DiffusivityX = 0.5;\nB->DiffusivityY = 0.5;\nB->DriftX = 0.0;\nB->DriftY = 0.0;",
+        newind="All->DriftX = 0.2 * RANDOM;", individual=("A",))
+    for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm), ("individual_a.xml", ind)):
         with open(os.path.join(HERE, name), "w") as f:
             f.write(text)
 

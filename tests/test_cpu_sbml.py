@@ -96,7 +96,11 @@ def test_reference_examples_load_or_name_what_is_missing():
     ab = ok["ABReaction.xml"]
     assert [r.rate for r in ab.reactions] == pytest.approx([1e-3, 1e-2, 1.2, 1.0])
     assert ab.reactions[0].reactants == {"SpeciesA": 2}
-    assert "individual" in unsupported["ABReactionIndividual.xml"]
+    ind = ok["ABReactionIndividual.xml"]
+    assert [sp.individual for sp in ind.species][:2] == [True, True]
+    assert "field parameter" in unsupported["Slit.xml"]
+    # a species name with digits (B00 ... B44) is not a number followed by a name
+    assert "RandomDrift.xml" not in unsupported or "script" in unsupported["RandomDrift.xml"]
     # without its (Python 2) init script the Calcium model loads, with custom laws
     ca = sbml.load(os.path.join(REF_EXAMPLES, "Calcium.xml"), ignore_scripts=True).model
     assert ca.custom_laws is not None and sum(l is not None for l in ca.custom_laws) >= 3

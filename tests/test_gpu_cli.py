@@ -16,7 +16,7 @@ def _variant(tmp_path, name, runs=None, solver=None):
     text = open(os.path.join(MODELS, name), encoding="utf-8").read()
     if runs is not None:
         old = '<im:runs><math:math xmlns:math="http://www.w3.org/1998/Math/MathML"><math:cn>1</math:cn>'
-        assert old in text
+        assert old in text, name
         text = text.replace(old, old.replace("<math:cn>1</math:cn>", f"<math:cn>{runs}</math:cn>"))
     if solver is not None:
         a = text.index("<im:solver>") + len("<im:solver>")
@@ -75,3 +75,36 @@ def test_cli_writes_the_solver_results(gpgmp, tmp_path, name, runs, solver, over
                 v = d[sp.id].value
                 assert v.dtype == (np.float32 if det else np.int32)
                 assert np.array_equal(v.reshape(-1), snaps[k, r, si].reshape(-1))
+
+
+@pytest.mark.gpu
+def test_cli_writes_individuals(gpgmp, tmp_path):
+    """A model file with an individual species: every dump holds the species' list
+    (cell | id << 32, the reference's getPositionList) whose cells count exactly the
+    dump's counts, with the properties of each listed individual."""
+    path = _variant(tmp_path, "individual_a.xml", runs=2)
+    out = str(tmp_path / "ind.h5")
+    assert cli.main([path, "--output", out, "--seed", "5"]) == 0
+    f = h5.read(out)
+    lm = sbml.load(path)
+    W, H = lm.model.width, lm.model.height
+    saw_new = False
+    for r in ("0", "1"):
+        for name in f[f"Runs/{r}"]:
+            d = f[f"Runs/{r}/{name}"]
+            counts = d["A"].value.reshape(-1)
+            ig = d["Individuals"]
+            if counts.sum() == 0:
+                assert "A" not in ig
+                continue
+            pairs = ig["A"].value
+            assert pairs.dtype == np.uint64 and len(pairs) == counts.sum()
+            cells = (pairs & np.uint64(0xFFFFFFFF)).astype(np.int64)
+            ids = (pairs >> np.uint64(32)).astype(np.int64)
+            assert np.array_equal(np.bincount(cells, minlength=W * H), counts)
+            assert np.all(np.diff(cells) >= 0) and len(np.unique(ids)) == len(ids)
+            drift = ig["A.DriftX"].value
+            assert len(drift) == len(pairs) and ig["A.DiffusivityY"].value.dtype == np.float32
+            assert np.all((drift >= 0) & (drift < 0.2))
+            saw_new = saw_new or bool((drift > 0).any())
+    assert saw_new                                       # the new-individuals method ran
