@@ -189,3 +189,42 @@ def test_individual_species_need_an_inhomogeneous_solver(gpgmp):
     h = C.c_void_p()
     rc = _lib.lib().gpgmp_solver_create(C.byref(d), 1, 0, 0, C.byref(h))
     assert rc == 4 and not h.value                      # GPGMP_ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+def test_individual_sweeps_match_count_sweeps_in_distribution(gpgmp):
+    """Individuals that all have the same D and r move like the molecules of the
+    count-based sweep (a binomial number leaves each cell): per-cell means over 512
+    realisations after 12 sweeps per direction agree within 5 standard errors, and so
+    does the spread of the cloud."""
+    W = 16
+    R = 512
+    D, r = 0.5, 0.15
+    st = np.zeros((R, 2, W, W), np.int32)
+    st[:, 0, 6:10, 6:10] = 25
+    means, spreads = [], []
+    for individual in (False, True):
+        m = DiffusionModel(width=W, height=W, physical_length=float(W), solver=_lib.STOCHASTIC_INHOMOGENEOUS)
+        m.add_species("A", 0.0, individual=individual)
+        m.add_species("B", 0.0)
+        m.drift_method = _lib.DRIFT_HOMOGENEOUS
+        m.drift_params = [D, D, r, 0.0] + [0.0] * 4
+        with Solver(m, realisations=R, seed=77) as s:
+            s.set_state(st)
+            if individual:
+                n = int(st[:, 0].sum())
+                s.set_individual_properties(0, np.array([[D], [D], [r], [0.0]], np.float32).repeat(n, axis=1))
+            dtx, dty = s.timesteps()
+            assert dtx[0] > 0 and dty[0] > 0
+            sd = 1
+            for k in range(12):
+                t = float(max(dtx[0], dty[0]) * (k + 1))
+                sd = s.diffuse(0, t, sd)
+            a = s.get_state()[:, 0].astype(np.float64)
+        means.append((a.mean(axis=0), a.var(axis=0)))
+        x = np.arange(W)
+        spreads.append(((a.sum(axis=1) * x).sum(axis=1) / a.sum(axis=(1, 2))).std())
+    (m0, v0), (m1, v1) = means
+    se = np.sqrt((v0 + v1) / R) + 1e-9
+    assert np.all(np.abs(m0 - m1) <= 5 * se + 1e-6)
+    assert abs(spreads[0] - spreads[1]) < 0.15 * spreads[0]
