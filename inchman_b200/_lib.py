@@ -33,6 +33,8 @@ DRIFT_MULTIPLICATIVE_NOISE = 1
 DRIFT_ORNSTEIN_UHLENBECK = 2
 DRIFT_CODE = 3
 
+FLAG_NONLINEAR = 1
+FLAG_COMPUTE_MOMENTS = 2
 FLAG_STOP_ON_ERROR = 4
 FLAG_LITERAL_REDIFFUSION = 8
 FLAG_AQSS_LITERAL = 16

@@ -114,6 +114,30 @@ def run(lm: sbml.LoadedModel, seed: int):
         nmax = int(np.floor(m.max_time / m.output_interval)) + 4
     else:
         nmax = 4
+    if R > 1 and (m.flags & _lib.FLAG_NONLINEAR):
+        # a nonlinear method's fields follow each run's state: one solver per run
+        parts = []
+        for r in range(R):
+            one = sbml.LoadedModel(model=m, runs=1, parameters=lm.parameters, notes=lm.notes,
+                                   compartments=lm.compartments, source=lm.source)
+            parts.append(run(one, seed + r))
+        n = min(len(p[1]) for p in parts)
+        snaps = np.concatenate([p[0][:n] for p in parts], axis=1)
+        inds = None
+        if parts[0][3] is not None:
+            area = m.width * m.height
+            inds = []
+            for k in range(n):
+                merged = {}
+                for r, p in enumerate(parts):
+                    for sp, (keys, ids, props) in p[3][k].items():
+                        prev = merged.get(sp)
+                        kk = keys + np.uint32(r * area)
+                        merged[sp] = (kk, ids, props) if prev is None else (
+                            np.concatenate([prev[0], kk]), np.concatenate([prev[1], ids]),
+                            np.concatenate([prev[2], props], axis=1))
+                inds.append(merged)
+        return snaps, parts[0][1][:n], sum(p[2] for p in parts), inds
     ind_species = [i for i, sp in enumerate(m.species) if sp.individual]
     individuals = []
     with Solver(m, realisations=R, seed=seed) as s:

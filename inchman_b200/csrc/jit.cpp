@@ -235,8 +235,10 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
       << "struct _species_t { int State; const int* SpeciesState; float MeanX;\n"
       << "                    float DiffusivityX; float DiffusivityY; float DriftX; float DriftY; };\n"
       << defines << "\n"
+      << "struct JitStatePlanes { const int* p[" << kMaxSpecies << "]; };\n"
       << "extern \"C\" __global__ void gpgmp_jit_drift(int _W, int _H, int _S, int _species, float _L,\n"
-      << "    float PhysicalSimTime, float* _dx, float* _dy, float* _rx, float* _ry, const int* _state) {\n"
+      << "    float PhysicalSimTime, float* _dx, float* _dy, float* _rx, float* _ry, JitStatePlanes _planes,\n"
+      << "    const float* _meanx) {\n"
       << "  const int _area = _W * _H;\n"
       << "  const int GridModelWidth = _W, GridModelHeight = _H;\n"
       << "  const Real PhysicalModelWidth = _L, PhysicalModelHeight = _L;\n"
@@ -248,9 +250,10 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
       << "    _species_t _sp[" << kMaxSpecies << "];\n"
       << "    for (int _s = 0; _s < _S; ++_s) {\n"
       << "      const long long _o = (long long)_s * _area + _c;\n"
-      << "      _sp[_s].State = _state ? _state[_o] : 0;\n"
-      << "      _sp[_s].SpeciesState = _state ? _state + (long long)_s * _area : nullptr;\n"
-      << "      _sp[_s].MeanX = 0.f;\n"
+      << "      const int* _pl = _planes.p[_s] ? _planes.p[_s] + (long long)_s * _area : nullptr;\n"
+      << "      _sp[_s].State = _pl ? _pl[_c] : 0;\n"
+      << "      _sp[_s].SpeciesState = _pl;\n"
+      << "      _sp[_s].MeanX = _meanx ? _meanx[_s] : 0.f;\n"
       << "      _sp[_s].DiffusivityX = _dx[_o]; _sp[_s].DiffusivityY = _dy[_o];\n"
       << "      _sp[_s].DriftX = _rx[_o]; _sp[_s].DriftY = _ry[_o];\n"
       << "    }\n"
@@ -275,11 +278,14 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
 }
 
 cudaError_t launch_drift_jit(JitFunction fn, const GridDesc& g, int species, float L, float sim_time, float* dx,
-                             float* dy, float* rx, float* ry, const int32_t* state, cudaStream_t st) {
+                             float* dy, float* rx, float* ry, const Planes* state, const float* meanx,
+                             cudaStream_t st) {
     int W = g.W, H = g.H, S = g.S;
     const int area = W * H;
     const unsigned blocks = (unsigned)((area + 255) / 256 < 148 * 8 ? (area + 255) / 256 : 148 * 8);
-    void* args[] = {&W, &H, &S, &species, &L, &sim_time, &dx, &dy, &rx, &ry, (void*)&state};
+    Planes planes{};
+    if (state) planes = *state;
+    void* args[] = {&W, &H, &S, &species, &L, &sim_time, &dx, &dy, &rx, &ry, &planes, (void*)&meanx};
     std::lock_guard<std::mutex> lk(g_mu);
     return launch((CUfunction)fn, blocks, 256, 0, st, args);
 }

@@ -29,8 +29,10 @@ cudaError_t launch_ssa_jit(JitFunction fn, const GridDesc& g, Planes planes, con
 // Drift/diffusivity kernel of the user method `code` (statements on All / SP(i)).
 int jit_drift_kernel(const std::string& defines, const std::string& code, JitFunction* out);
 // Evaluates the method for `species` over the grid: reads and writes the field
-// arrays [S][H][W]; state (realisation 0's [S][H][W] counts) may be NULL.
+// arrays [S][H][W].  state: the current plane base of each species (realisation 0's
+// counts are read), NULL for none; meanx: MeanX of each species (moments), NULL for 0.
 cudaError_t launch_drift_jit(JitFunction fn, const GridDesc& g, int species, float L, float sim_time, float* dx,
-                             float* dy, float* rx, float* ry, const int32_t* state, cudaStream_t st);
+                             float* dy, float* rx, float* ry, const Planes* state, const float* meanx,
+                             cudaStream_t st);
 
 }  // namespace gpgmp

@@ -36,6 +36,9 @@ cudaError_t launch_sweep(const GridDesc& g, const int32_t* in, int32_t* out, int
                          uint32_t seed, uint32_t step_seed, const float* d_D, const float* d_r, float dt, float dx,
                          cudaStream_t st, int fpe = 0);
 // kind: 0 stochastic drift-diffusion, 1 FPE (uses stay), 2 deterministic
+// MeanX of one species plane (the reference's moments): *d_meanx on the device
+cudaError_t launch_moments(const int32_t* plane, int W, int H, float L, unsigned long long* d_sums, float* d_meanx,
+                           cudaStream_t st);
 cudaError_t launch_timestep(int area, const float* d_D, const float* d_r, float dx, uint32_t* d_min_key,
                             cudaStream_t st, int kind = 0, float stay = 0.f);
 cudaError_t launch_diffusivity_drift(const GridDesc& g, int species, int method, const float* params, float L,

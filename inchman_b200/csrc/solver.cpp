@@ -65,6 +65,10 @@ struct gpgmp_solver {
     std::string newind_code;
     long long ind_cap = 0;
     float sim_time = 0.f;               // the time of the last diffusion event (the methods' PhysicalSimTime)
+    // nonlinear drift methods (GPGMP_FLAG_NONLINEAR / _COMPUTE_MOMENTS)
+    bool nonlinear = false, moments = false;
+    float* d_meanx = nullptr;               // [S]
+    unsigned long long* d_msums = nullptr;  // [2]
 };
 
 namespace {
@@ -139,7 +143,8 @@ int normalize(gpgmp_solver* h) {
 
 void free_all(gpgmp_solver* h) {
     void* ptrs[] = {h->d_buf[0], h->d_buf[1], h->d_fbuf[0], h->d_fbuf[1], h->d_reactions, h->d_status, h->d_diff,
-                    h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage};
+                    h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage, h->d_meanx,
+                    h->d_msums};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (IndList& l : h->ind) ind_free(l);
@@ -176,7 +181,13 @@ int validate(const gpgmp_model_desc* m, int R) {
             return set_error(GPGMP_ERR_UNSUPPORTED, "drift_method %d", m->drift_method);
         if (m->drift_method == GPGMP_DRIFT_CODE && !m->drift_code)
             return set_error(GPGMP_ERR_INVALID, "GPGMP_DRIFT_CODE needs drift_code");
-        if (m->flags & 1) return set_error(GPGMP_ERR_UNSUPPORTED, "nonlinear diffusivity recompute");
+        if ((m->flags & (GPGMP_FLAG_NONLINEAR | GPGMP_FLAG_COMPUTE_MOMENTS)) && m->drift_method == GPGMP_DRIFT_CODE) {
+            if (m->solver_type != GPGMP_STOCHASTIC_INHOMOGENEOUS && m->solver_type != GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE)
+                return set_error(GPGMP_ERR_UNSUPPORTED, "nonlinear drift methods with a deterministic solver");
+            if (R != 1)
+                return set_error(GPGMP_ERR_UNSUPPORTED,
+                                 "a nonlinear drift method needs one realisation per solver (its fields follow the state)");
+        }
     }
     if (m->individual) {
         bool any = false;
@@ -289,10 +300,15 @@ int inhom_init(gpgmp_solver* h) {
             int rc = jit_drift_kernel(h->code_defines, h->drift_code, &h->jit_drift);
             if (rc) return rc;
         }
-        const int32_t* st0 = h->deterministic ? nullptr : h->d_buf[h->cur.empty() ? 0 : h->cur[0]];
+        Planes planes{};
+        if (!h->deterministic) planes = planes_of(h);
+        if (h->moments)   // the reference computes the moments of every species first (:168-185)
+            for (int s = 0; s < h->g.S; ++s)
+                CK(launch_moments(planes.p[s] + (size_t)s * h->area, h->m.width, h->m.height, h->m.physical_length,
+                                  h->d_msums, h->d_meanx + s, h->stream));
         for (int s = 0; s < h->g.S; ++s)
             CK(launch_drift_jit(h->jit_drift, h->g, s, h->m.physical_length, 0.f, h->d_Dx, h->d_Dy, h->d_rx, h->d_ry,
-                                st0, h->stream));
+                                h->deterministic ? nullptr : &planes, h->moments ? h->d_meanx : nullptr, h->stream));
     } else if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
         CK(cudaMemcpyAsync(h->d_Dx, h->m.field_dx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_Dy, h->m.field_dy, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -321,6 +337,28 @@ int inhom_init(gpgmp_solver* h) {
         h->nextX[s] = h->smallX[s];
         h->nextY[s] = h->smallY[s];
     }
+    return GPGMP_OK;
+}
+
+// A nonlinear drift method after a sweep of species i in direction dir
+// (InhomogeneousSolver.cpp:288-335): the moments after an x sweep, the method on the
+// state and time now, the smallest time step of that direction.
+int nonlinear_update(gpgmp_solver* h, int i, int dir, float t) {
+    if (!h->nonlinear) return GPGMP_OK;
+    Planes planes = planes_of(h);
+    if (h->moments && dir == 0)
+        CK(launch_moments(planes.p[i] + (size_t)i * h->area, h->m.width, h->m.height, h->m.physical_length, h->d_msums,
+                          h->d_meanx + i, h->stream));
+    CK(launch_drift_jit(h->jit_drift, h->g, i, h->m.physical_length, t, h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, &planes,
+                        h->moments ? h->d_meanx : nullptr, h->stream));
+    const float dx = h->m.physical_length / (float)h->m.width;
+    uint32_t key = 0;
+    CK(launch_timestep((int)h->area, (dir == 0 ? h->d_Dx : h->d_Dy) + (size_t)i * h->area,
+                       (dir == 0 ? h->d_rx : h->d_ry) + (size_t)i * h->area, dx, h->d_minkey, h->stream, h->ts_kind,
+                       h->stay));
+    CK(cudaMemcpyAsync(&key, h->d_minkey, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    (dir == 0 ? h->smallX[i] : h->smallY[i]) = key_to_float(key);
     return GPGMP_OK;
 }
 
@@ -490,6 +528,12 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
         CKC(cudaMalloc(&h->d_rx, nf * sizeof(float)));
         CKC(cudaMalloc(&h->d_ry, nf * sizeof(float)));
         CKC(cudaMalloc(&h->d_minkey, sizeof(uint32_t)));
+        h->nonlinear = (model->flags & GPGMP_FLAG_NONLINEAR) && model->drift_method == GPGMP_DRIFT_CODE;
+        h->moments = (model->flags & GPGMP_FLAG_COMPUTE_MOMENTS) && model->drift_method == GPGMP_DRIFT_CODE &&
+                     !h->deterministic;
+        CKC(cudaMalloc(&h->d_meanx, sizeof(float) * S));
+        CKC(cudaMemset(h->d_meanx, 0, sizeof(float) * S));
+        CKC(cudaMalloc(&h->d_msums, 2 * sizeof(unsigned long long)));
         h->nextX.assign(S, 0.f); h->nextY.assign(S, 0.f);
         h->smallX.assign(S, 0.f); h->smallY.assign(S, 0.f);
         h->ddX.assign(S, 0.f); h->ddY.assign(S, 0.f);
@@ -675,6 +719,8 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
         if (rc) return rc;
         h->cur[i] ^= 1;
         (*seed)++;
+        rc = nonlinear_update(h, i, 0, t);
+        if (rc) return rc;
         h->nextX[i] += h->smallX[i];
         h->ddX[i] = h->smallX[i];
     }
@@ -685,6 +731,8 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
         if (rc) return rc;
         h->cur[i] ^= 1;
         (*seed)++;
+        rc = nonlinear_update(h, i, 1, t);
+        if (rc) return rc;
         h->nextY[i] += h->smallY[i];
         h->ddY[i] = h->smallY[i];
     }

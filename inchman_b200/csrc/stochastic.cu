@@ -553,6 +553,40 @@ cudaError_t launch_timestep(int area, const float* d_D, const float* d_r, float 
     return cudaGetLastError();
 }
 
+// inhomogeneous_computeMomentsX + reduceMomentsBlocks (StochasticInhomogeneousDriftDiffusion.cl:5-84)
+// and getMeanX (helpers.cl:18-21): MeanX = L / W * (sum x n / sum n - W / 2) of one
+// species plane, the sums taken exactly in 64-bit integers.
+__global__ void k_moments_sum(const int32_t* __restrict__ plane, int W, int area, unsigned long long* sums) {
+    unsigned long long mx = 0, n = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < area; c += gridDim.x * blockDim.x) {
+        const long long v = plane[c] > 0 ? plane[c] : 0;
+        mx += (unsigned long long)(v * (c % W));
+        n += (unsigned long long)v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx += __shfl_xor_sync(0xffffffffu, mx, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sums[0], mx);
+        atomicAdd(&sums[1], n);
+    }
+}
+__global__ void k_moments_finish(const unsigned long long* sums, int W, float L, float* meanx) {
+    const float tmp = (float)sums[0] / (float)sums[1];
+    *meanx = L / (float)W * (tmp - (float)W / 2.0f);
+}
+
+cudaError_t launch_moments(const int32_t* plane, int W, int H, float L, unsigned long long* d_sums, float* d_meanx,
+                           cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_sums, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    const int area = W * H;
+    k_moments_sum<<<grid_for(area, 256), 256, 0, st>>>(plane, W, area, d_sums);
+    k_moments_finish<<<1, 1, 0, st>>>(d_sums, W, L, d_meanx);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_diffusivity_drift(const GridDesc& g, int species, int method, const float* params, float L,
                                      float* dx, float* dy, float* rx, float* ry, cudaStream_t st) {
     DriftParams p;

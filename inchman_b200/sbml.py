@@ -24,9 +24,12 @@ Individual species (<im:individual/>) become individual species of the solver, w
 newIndividualsMethod compiled at run time; their properties start at zero, as the
 reference's do without an init script.
 
+A nonlinear drift method (nonLinear="true", or computeMoments="true") that reads the
+state, the time or MeanX is evaluated again after every sweep (GPGMP_FLAG_NONLINEAR,
+GPGMP_FLAG_COMPUTE_MOMENTS; one realisation per solver).
+
 Not supported (raises Unsupported): init and event scripts (Python run by the
-reference's executable), field parameters, reactions localised to part of the grid,
-nonlinear drift methods that read the state, time or moments.
+reference's executable), field parameters, reactions localised to part of the grid.
 """
 from __future__ import annotations
 
@@ -299,6 +302,7 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
     runs = 1
     method = ""
     nonlinear = False
+    moments = False
     if sb is not None:
         solver = _text(sb.find(IM + "solver")) or "stochastic_inhomogeneous"
         if solver not in SOLVERS:
@@ -325,8 +329,7 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
         if dd is not None:
             method = _text(dd.find(IM + "method"))
             nonlinear = dd.get("nonLinear", "false") == "true"
-            if dd.get("computeMoments", "") == "true":
-                raise Unsupported("drift methods with moments (computeMoments)")
+            moments = dd.get("computeMoments", "") == "true"
         sf = sb.find(f"{IM}setField/{IM}method")
         if sf is not None and _text(sf):
             raise Unsupported("setField method (field parameters)")
@@ -418,8 +421,12 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
     if m.solver in _lib.INHOMOGENEOUS_TYPES:
         used = drift_identifiers(method)
         dynamic = used & {"PhysicalSimTime", "State", "SpeciesState", "MeanX"}
-        if nonlinear and dynamic:
-            raise Unsupported(f"a nonlinear drift method that reads {sorted(dynamic)} (recomputed every sweep)")
+        if (nonlinear or moments) and dynamic:
+            # evaluated again after every sweep (InhomogeneousSolver.cpp:288-335)
+            if m.solver not in (_lib.STOCHASTIC_INHOMOGENEOUS, _lib.STOCHASTIC_INHOMOGENEOUS_FPE):
+                raise Unsupported(f"a nonlinear drift method that reads {sorted(dynamic)} with a deterministic solver")
+            m.flags |= _lib.FLAG_NONLINEAR | (_lib.FLAG_COMPUTE_MOMENTS if moments else 0)
+            notes.append("nonlinear drift method: one realisation per solver")
         unknown = used - DRIFT_NAMES - set(params) - spset - C_MATH
         declared = set(re.findall(r"\bReal\s+([A-Za-z_]\w*)", _COMMENT.sub(" ", method)))
         unknown -= declared

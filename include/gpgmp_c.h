@@ -62,6 +62,12 @@ extern "C" {
 #define GPGMP_DRIFT_CODE 3                 /* gpgmp_model_desc.drift_code, compiled at run time */
 
 /* gpgmp_model_desc.flags */
+#define GPGMP_FLAG_NONLINEAR 1             /* inhomogeneous, GPGMP_DRIFT_CODE: the method is evaluated again after
+                                              every sweep of a species, on the state and time then, and the next
+                                              time step of that direction follows (InhomogeneousSolver.cpp:303-335;
+                                              stochastic solvers of one realisation) */
+#define GPGMP_FLAG_COMPUTE_MOMENTS 2       /* with it, SP(i)->MeanX (the mean x of species i, helpers.cl:18-21)
+                                              is computed before the first evaluation and after every x sweep */
 #define GPGMP_FLAG_STOP_ON_ERROR 4         /* end a realisation's event loop once its status is set */
 #define GPGMP_FLAG_LITERAL_REDIFFUSION 8   /* deterministic: repeat the stencil per due species (reference) */
 #define GPGMP_FLAG_AQSS_LITERAL 16  /* alpha-QSS as the reference writes it: predictor from the current

@@ -15,7 +15,7 @@ def num(v):
 
 
 def document(name, solver, W, L, time, out, params, comps, species, reactions, method="", newind=None,
-             individual=()):
+             individual=(), nonlinear=False, moments=False):
     ps = "\n".join(f'      <parameter id="{k}" value="{v}"><annotation><im:parameter xmlns:im="{IMNS}" '
                    f'type="float" domain="single"/></annotation></parameter>' for k, v in params.items())
     cs = "\n".join(f'      <compartment id="{cid}"><annotation><im:compartment xmlns:im="{IMNS}">'
@@ -50,7 +50,7 @@ def document(name, solver, W, L, time, out, params, comps, species, reactions, m
   <im:outputInterval>{num(out)}</im:outputInterval>
   <im:init type="python"><im:script><![CDATA[]]></im:script></im:init>
   <im:events type="python"><im:script><![CDATA[]]></im:script><im:listOfTimeStamps/></im:events>
-  <im:driftDiffusivity nonLinear="false" computeMoments=""><im:method><![CDATA[{method}]]></im:method></im:driftDiffusivity>
+  <im:driftDiffusivity nonLinear="{"true" if nonlinear else "false"}" computeMoments="{"true" if moments else ""}"><im:method><![CDATA[{method}]]></im:method></im:driftDiffusivity>
 {"" if newind is None else f"  <im:newIndividualsMethod><im:method><![CDATA[{newind}]]></im:method></im:newIndividualsMethod>" + chr(10)}</im:sbml></annotation>
   <model name="{name}">
 <annotation><im:model xmlns:im="{IMNS}"><im:gridWidth>{num(W)}</im:gridWidth><im:gridHeight>{num(W)}</im:gridHeight>
@@ -125,7 +125,17 @@ def main():
         method="A->DiffusivityX = 0.8;\nA->DiffusivityY = 0.6;\nA->DriftX = A->DriftX + 0.1;\nA->DriftY = 0.0;\n"
                "B->DiffusivityX = 0.5;\nB->DiffusivityY = 0.5;\nB->DriftX = 0.0;\nB->DriftY = 0.0;",
         newind="All->DriftX = 0.2 * RANDOM;", individual=("A",))
-    for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm), ("individual_a.xml", ind)):
+    # a nonlinear method: drift towards the species' mean x (moments), diffusivity
+    # growing with the local count
+    nl = document(
+        "Nonlinear pull", "stochastic_inhomogeneous", 16, 16.0, 0.5, 0.25, {"pull": 0.4},
+        {"World": (0, 0, 16, 16), "Left": (0, 0, 5, 16)},
+        {"A": (0.0, {"Left": 5 * 16 * 12})}, {},
+        method="All->DiffusivityX = 0.3 + 0.02 * All->State;\nAll->DiffusivityY = 0.3;\n"
+               "All->DriftX = -pull * (PhysicalX - All->MeanX);\nAll->DriftY = 0.0;",
+        nonlinear=True, moments=True)
+    for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm), ("individual_a.xml", ind),
+                       ("nonlinear.xml", nl)):
         with open(os.path.join(HERE, name), "w") as f:
             f.write(text)
 

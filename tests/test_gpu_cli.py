@@ -108,3 +108,27 @@ def test_cli_writes_individuals(gpgmp, tmp_path):
             assert np.all((drift >= 0) & (drift < 0.2))
             saw_new = saw_new or bool((drift > 0).any())
     assert saw_new                                       # the new-individuals method ran
+
+
+@pytest.mark.gpu
+def test_cli_runs_a_nonlinear_model_one_solver_per_run(gpgmp, tmp_path):
+    """A nonlinear drift method (fields recomputed from each run's state after every
+    sweep) runs each run in its own solver; the file still holds every run, and
+    reflecting walls without reactions keep each run's total."""
+    path = _variant(tmp_path, "nonlinear.xml", runs=2)
+    out = str(tmp_path / "nl.h5")
+    assert cli.main([path, "--output", out, "--seed", "3"]) == 0
+    f = h5.read(out)
+    assert f["Model"].attrs["numRuns"].tolist() == [2]
+    total = 5 * 16 * 12
+    finals = []
+    for r in ("0", "1"):
+        names = list(f[f"Runs/{r}"])
+        assert "Dump_0" in names and len(names) >= 3
+        for nm in names:
+            assert int(f[f"Runs/{r}/{nm}/A"].value.sum()) == total
+        last = max(names, key=lambda nm: float(f[f"Runs/{r}/{nm}"].attrs["time"][0]))
+        finals.append(f[f"Runs/{r}/{last}/A"].value)
+    assert not np.array_equal(finals[0], finals[1])          # two different runs
+    # mass left the strip x < 5 it started in (the datasets hold the [y][x] buffer)
+    assert finals[0].reshape(16, 16)[:, 5:].sum() > 0
