@@ -80,6 +80,9 @@ class ModelDesc(C.Structure):
         ("individual", C.POINTER(C.c_uint8)),
         ("individual_capacity", C.c_int64),
         ("new_individuals_code", C.c_char_p),
+        ("num_fields", C.c_int32),
+        ("field_values", C.POINTER(C.c_float)),
+        ("set_field_code", C.c_char_p),
     ]
 
 
@@ -122,6 +125,9 @@ SIGNATURES = {
     "gpgmp_device_state": (vp, [vp]),
     "gpgmp_timesteps": (C.c_int, [vp, P(f32), P(f32)]),
     "gpgmp_individual_count": (C.c_int, [vp, i32, P(i64)]),
+    "gpgmp_update_fields": (C.c_int, [vp, f32, f32]),
+    "gpgmp_get_fields": (C.c_int, [vp, P(f32)]),
+    "gpgmp_set_fields": (C.c_int, [vp, P(f32)]),
     "gpgmp_solve_with_callback": (C.c_int, [vp, vp, P(f32), i32, P(i32), P(i64), vp, vp]),
     "gpgmp_get_individuals": (C.c_int, [vp, i32, vp, vp, vp, i64, P(i64)]),
     "gpgmp_set_individual_properties": (C.c_int, [vp, i32, vp, i64, i64]),

@@ -15,7 +15,9 @@ InchmanDiffusionModel.cpp:240-274, doc/source/hdf5.rst) with inchman_b200.h5:
   /Runs/<run>/Dump_<time>     attribute time (float32[1]); one dataset per species,
                               dims [gridWidth, gridHeight] over the state buffer
                               (int32 counts, float32 for deterministic solvers);
-                              an Individuals group: per individual species its
+                              a Fields group with the field parameters (when the
+                              model has them); an Individuals group: per individual
+                              species its
                               (cell | id << 32) uint64 list and four float32
                               property lists (empty without individual species)
 
@@ -50,12 +52,14 @@ def dump_name(t: float) -> str:
 PROPERTY_NAMES = ("DiffusivityX", "DiffusivityY", "DriftX", "DriftY")
 
 
-def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray, individuals=None) -> h5.Group:
+def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray, individuals=None,
+                fields=None) -> h5.Group:
     """The reference's file layout for snapshots [n][runs][S][H][W] at times [n].
     individuals[k][species] = (keys, ids, props [4][n]) of dump k (keys r * area + cell):
     written per run as /Individuals/<species> (uint64 cell | id << 32, the reference's
     getPositionList) and <species>.DiffusivityX/Y, .DriftX/Y (float32, in the same
-    order as the positions)."""
+    order as the positions).  fields[k] = [runs][F][H][W] field parameters of dump k,
+    written as /Fields/<name> (float32, dims [gridWidth, gridHeight])."""
     m = lm.model
     S, H, W = m.num_species, m.height, m.width
     runs = snaps.shape[1]
@@ -84,6 +88,10 @@ def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray, indi
                 # the state buffer of one species as the reference hands it to HDF5:
                 # dims [gridWidth, gridHeight] over the bytes of the [H][W] plane
                 d.create_dataset(sp.id, np.ascontiguousarray(snaps[k, r, s]).reshape(W, H))
+            if fields is not None and m.field_names:
+                fg = d.create_group("Fields")
+                for f, fname in enumerate(m.field_names):
+                    fg.create_dataset(fname, np.ascontiguousarray(fields[k][r][f]).reshape(W, H))
             ig = d.create_group("Individuals")
             if individuals is None:
                 continue
@@ -102,7 +110,7 @@ def output_tree(lm: sbml.LoadedModel, snaps: np.ndarray, times: np.ndarray, indi
 
 def run(lm: sbml.LoadedModel, seed: int):
     """Runs the model; returns (snapshots [n][runs][S][H][W], times [n], steps,
-    individuals per dump or None)."""
+    individuals per dump or None, fields per dump [runs][F][H][W] or None)."""
     from .solver import Solver
     m = lm.model
     det = m.solver in _lib.DETERMINISTIC_TYPES
@@ -114,7 +122,7 @@ def run(lm: sbml.LoadedModel, seed: int):
         nmax = int(np.floor(m.max_time / m.output_interval)) + 4
     else:
         nmax = 4
-    if R > 1 and (m.flags & _lib.FLAG_NONLINEAR):
+    if R > 1 and ((m.flags & _lib.FLAG_NONLINEAR) or m.set_field_code):
         # a nonlinear method's fields follow each run's state: one solver per run
         parts = []
         for r in range(R):
@@ -137,18 +145,25 @@ def run(lm: sbml.LoadedModel, seed: int):
                             np.concatenate([prev[0], kk]), np.concatenate([prev[1], ids]),
                             np.concatenate([prev[2], props], axis=1))
                 inds.append(merged)
-        return snaps, parts[0][1][:n], sum(p[2] for p in parts), inds
+        flds = None
+        if parts[0][4] is not None:
+            flds = [np.concatenate([p[4][k] for p in parts], axis=0) for k in range(n)]
+        return snaps, parts[0][1][:n], sum(p[2] for p in parts), inds, flds
     ind_species = [i for i, sp in enumerate(m.species) if sp.individual]
-    individuals = []
+    individuals, fields = [], []
     with Solver(m, realisations=R, seed=seed) as s:
         s.set_state(state)
-        if ind_species:
+        if ind_species or m.field_names:
             def on_dump(index, t):
-                individuals.append({i: s.get_individuals(i) for i in ind_species})
+                if ind_species:
+                    individuals.append({i: s.get_individuals(i) for i in ind_species})
+                if m.field_names:   # shared by the solver's realisations (no setField with R > 1)
+                    fields.append(np.repeat(s.get_fields()[None], R, axis=0))
             snaps, times, steps = s.solve(max_snapshots=nmax, on_dump=on_dump)
         else:
             snaps, times, steps = s.solve(max_snapshots=nmax)
-    return snaps, times, steps, (individuals[:len(times)] if ind_species else None)
+    return (snaps, times, steps, (individuals[:len(times)] if ind_species else None),
+            (fields[:len(times)] if m.field_names else None))
 
 
 def main(argv: Optional[list] = None) -> int:
@@ -176,9 +191,9 @@ def main(argv: Optional[list] = None) -> int:
     for n in lm.notes:
         print(f"note: {n}", file=sys.stderr)
     t0 = time.perf_counter()
-    snaps, times, steps, individuals = run(lm, seed)
+    snaps, times, steps, individuals, fields = run(lm, seed)
     t1 = time.perf_counter()
-    h5.write(args.output, output_tree(lm, snaps, times, individuals))
+    h5.write(args.output, output_tree(lm, snaps, times, individuals, fields))
     print(f"{args.model_file}: {snaps.shape[1]} run(s), {len(times)} dumps, {steps} steps in {t1 - t0:.3f} s "
           f"-> {args.output}", file=sys.stderr)
     return 0

@@ -236,9 +236,21 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
       << "                    float DiffusivityX; float DiffusivityY; float DriftX; float DriftY; };\n"
       << defines << "\n"
       << "struct JitStatePlanes { const int* p[" << kMaxSpecies << "]; };\n"
+      // helpers.cl:38-87: neighbour differences of a species' counts, mirrored at the
+      // edges (the reference bounds y by the grid width as well)
+      << "__device__ __forceinline__ float _gp_cdx(const _species_t* sp, int x, int y, int W) {\n"
+      << "  const int* d = sp->SpeciesState; if (!d) return 0.f;\n"
+      << "  const int l = x > 0 ? d[(x - 1) + y * W] : d[(x + 1) + y * W];\n"
+      << "  const int r = x < W - 1 ? d[(x + 1) + y * W] : d[(x - 1) + y * W];\n"
+      << "  return (float)(r - l);\n}\n"
+      << "__device__ __forceinline__ float _gp_cdy(const _species_t* sp, int x, int y, int W) {\n"
+      << "  const int* d = sp->SpeciesState; if (!d) return 0.f;\n"
+      << "  const int t = y > 0 ? d[x + (y - 1) * W] : d[x + (y + 1) * W];\n"
+      << "  const int b = y < W - 1 ? d[x + (y + 1) * W] : d[x + (y - 1) * W];\n"
+      << "  return (float)(b - t);\n}\n"
       << "extern \"C\" __global__ void gpgmp_jit_drift(int _W, int _H, int _S, int _species, float _L,\n"
       << "    float PhysicalSimTime, float* _dx, float* _dy, float* _rx, float* _ry, JitStatePlanes _planes,\n"
-      << "    const float* _meanx) {\n"
+      << "    const float* _meanx, const float* _fields) {\n"
       << "  const int _area = _W * _H;\n"
       << "  const int GridModelWidth = _W, GridModelHeight = _H;\n"
       << "  const Real PhysicalModelWidth = _L, PhysicalModelHeight = _L;\n"
@@ -258,12 +270,17 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
       << "      _sp[_s].DriftX = _rx[_o]; _sp[_s].DriftY = _ry[_o];\n"
       << "    }\n"
       << "#define SP(i) (&_sp[(i)])\n"
+      << "#define F(f) (_fields[(long long)(f) * _area + _c])\n"
+      << "#define getCentralDifferenceX(sp) _gp_cdx((sp), GridX, GridY, _W)\n"
+      << "#define getCentralDifferenceY(sp) _gp_cdy((sp), GridX, GridY, _W)\n"
+      << "#define getPhysicalX() (PhysicalX)\n#define getPhysicalY() (PhysicalY)\n"
       << "    _species_t* All = &_sp[_species];\n"
       << "    (void)GridX; (void)GridY; (void)PhysicalX; (void)PhysicalY; (void)PhysicalSimTime;\n"
       << "    (void)PhysicalModelWidth; (void)PhysicalModelHeight; (void)PhysicalCellWidth;\n"
       << "    (void)PhysicalCellHeight; (void)GridModelWidth; (void)GridModelHeight;\n"
       << "    {\n" << code << "\n    }\n"
-      << "#undef SP\n"
+      << "#undef SP\n#undef F\n#undef getCentralDifferenceX\n#undef getCentralDifferenceY\n"
+      << "#undef getPhysicalX\n#undef getPhysicalY\n"
       << "    const long long _o = (long long)_species * _area + _c;\n"
       << "    _dx[_o] = All->DiffusivityX; _dy[_o] = All->DiffusivityY;\n"
       << "    _rx[_o] = All->DriftX; _ry[_o] = All->DriftY;\n"
@@ -279,13 +296,60 @@ int jit_drift_kernel(const std::string& defines, const std::string& code, JitFun
 
 cudaError_t launch_drift_jit(JitFunction fn, const GridDesc& g, int species, float L, float sim_time, float* dx,
                              float* dy, float* rx, float* ry, const Planes* state, const float* meanx,
-                             cudaStream_t st) {
+                             const float* fields, cudaStream_t st) {
     int W = g.W, H = g.H, S = g.S;
     const int area = W * H;
     const unsigned blocks = (unsigned)((area + 255) / 256 < 148 * 8 ? (area + 255) / 256 : 148 * 8);
     Planes planes{};
     if (state) planes = *state;
-    void* args[] = {&W, &H, &S, &species, &L, &sim_time, &dx, &dy, &rx, &ry, &planes, (void*)&meanx};
+    void* args[] = {&W, &H, &S, &species, &L, &sim_time, &dx, &dy, &rx, &ry, &planes, (void*)&meanx, (void*)&fields};
+    std::lock_guard<std::mutex> lk(g_mu);
+    return launch((CUfunction)fn, blocks, 256, 0, st, args);
+}
+
+// The setField method (updateFields, Solver.cpp:583-653): per cell, X(i) is the count
+// of species i as a float (written back truncated), F(f) field f of the cell.
+int jit_field_kernel(const std::string& defines, const std::string& code, JitFunction* out) {
+    std::ostringstream s;
+    s << "#include \"gpgmp_rtc_prelude.h\"\n"
+      << "typedef float Real;\n"
+      << defines << "\n"
+      << "struct JitMutPlanes { int* p[" << kMaxSpecies << "]; };\n"
+      << "extern \"C\" __global__ void gpgmp_jit_fields(int _W, int _H, int _S, float _L, float deltat,\n"
+      << "    float simtime, float* _fields, JitMutPlanes _planes) {\n"
+      << "  const int _area = _W * _H;\n"
+      << "  const int GridModelWidth = _W, GridModelHeight = _H;\n"
+      << "  const Real PhysicalModelWidth = _L, PhysicalModelHeight = _L;\n"
+      << "  const Real PhysicalCellWidth = _L / (float)_W, PhysicalCellHeight = _L / (float)_H;\n"
+      << "  (void)GridModelWidth; (void)GridModelHeight; (void)PhysicalModelWidth; (void)PhysicalModelHeight;\n"
+      << "  (void)PhysicalCellWidth; (void)PhysicalCellHeight; (void)deltat; (void)simtime;\n"
+      << "  for (int _c = blockIdx.x * blockDim.x + threadIdx.x; _c < _area; _c += gridDim.x * blockDim.x) {\n"
+      << "    const int GridX = _c % _W, GridY = _c / _W;\n"
+      << "    (void)GridX; (void)GridY;\n"
+      << "    float _x[" << kMaxSpecies << "];\n"
+      << "    for (int _s = 0; _s < _S; ++_s) _x[_s] = (float)_planes.p[_s][(long long)_s * _area + _c];\n"
+      << "#define X(i) (_x[(i)])\n"
+      << "#define F(f) (_fields[(long long)(f) * _area + _c])\n"
+      << "    {\n" << code << "\n    }\n"
+      << "#undef X\n#undef F\n"
+      << "    for (int _s = 0; _s < _S; ++_s) _planes.p[_s][(long long)_s * _area + _c] = (int)_x[_s];\n"
+      << "  }\n"
+      << "}\n";
+    std::lock_guard<std::mutex> lk(g_mu);
+    CUfunction fn = nullptr;
+    int rc = compile(s.str(), "gpgmp_jit_fields", &fn);
+    if (rc) return rc;
+    *out = (JitFunction)fn;
+    return GPGMP_OK;
+}
+
+cudaError_t launch_field_jit(JitFunction fn, const GridDesc& g, float L, float deltat, float simtime, float* fields,
+                             const Planes& state, cudaStream_t st) {
+    int W = g.W, H = g.H, S = g.S;
+    const int area = W * H;
+    const unsigned blocks = (unsigned)((area + 255) / 256 < 148 * 8 ? (area + 255) / 256 : 148 * 8);
+    Planes planes = state;
+    void* args[] = {&W, &H, &S, &L, &deltat, &simtime, &fields, &planes};
     std::lock_guard<std::mutex> lk(g_mu);
     return launch((CUfunction)fn, blocks, 256, 0, st, args);
 }

@@ -30,9 +30,14 @@ cudaError_t launch_ssa_jit(JitFunction fn, const GridDesc& g, Planes planes, con
 int jit_drift_kernel(const std::string& defines, const std::string& code, JitFunction* out);
 // Evaluates the method for `species` over the grid: reads and writes the field
 // arrays [S][H][W].  state: the current plane base of each species (realisation 0's
-// counts are read), NULL for none; meanx: MeanX of each species (moments), NULL for 0.
+// counts are read), NULL for none; meanx: MeanX of each species (moments), NULL for 0;
+// fields: the field parameters [F][H][W] (F(f) in the code), NULL for none.
 cudaError_t launch_drift_jit(JitFunction fn, const GridDesc& g, int species, float L, float sim_time, float* dx,
                              float* dy, float* rx, float* ry, const Planes* state, const float* meanx,
-                             cudaStream_t st);
+                             const float* fields, cudaStream_t st);
+// The setField method (see jit.cpp): one pass over the grid of realisation 0.
+int jit_field_kernel(const std::string& defines, const std::string& code, JitFunction* out);
+cudaError_t launch_field_jit(JitFunction fn, const GridDesc& g, float L, float deltat, float simtime, float* fields,
+                             const Planes& state, cudaStream_t st);
 
 }  // namespace gpgmp

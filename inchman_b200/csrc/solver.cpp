@@ -69,6 +69,11 @@ struct gpgmp_solver {
     bool nonlinear = false, moments = false;
     float* d_meanx = nullptr;               // [S]
     unsigned long long* d_msums = nullptr;  // [2]
+    // field parameters (Solver.cpp:88-101) and the setField method
+    int nfields = 0;
+    float* d_fields = nullptr;              // [F][area]
+    std::string set_field_code;
+    JitFunction jit_fields = nullptr;
 };
 
 namespace {
@@ -144,7 +149,7 @@ int normalize(gpgmp_solver* h) {
 void free_all(gpgmp_solver* h) {
     void* ptrs[] = {h->d_buf[0], h->d_buf[1], h->d_fbuf[0], h->d_fbuf[1], h->d_reactions, h->d_status, h->d_diff,
                     h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage, h->d_meanx,
-                    h->d_msums};
+                    h->d_msums, h->d_fields};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (IndList& l : h->ind) ind_free(l);
@@ -188,6 +193,15 @@ int validate(const gpgmp_model_desc* m, int R) {
                 return set_error(GPGMP_ERR_UNSUPPORTED,
                                  "a nonlinear drift method needs one realisation per solver (its fields follow the state)");
         }
+    }
+    if (m->num_fields < 0) return set_error(GPGMP_ERR_INVALID, "num_fields %d", m->num_fields);
+    if (m->set_field_code && m->set_field_code[0]) {
+        if (m->num_fields <= 0) return set_error(GPGMP_ERR_INVALID, "set_field_code without fields");
+        const int ty = m->solver_type;
+        if (ty != GPGMP_STOCHASTIC_HOMOGENEOUS && ty != GPGMP_STOCHASTIC_INHOMOGENEOUS &&
+            ty != GPGMP_STOCHASTIC_INHOMOGENEOUS_FPE)
+            return set_error(GPGMP_ERR_UNSUPPORTED, "a setField method with a deterministic solver");
+        if (R != 1) return set_error(GPGMP_ERR_UNSUPPORTED, "a setField method needs one realisation per solver");
     }
     if (m->individual) {
         bool any = false;
@@ -308,7 +322,8 @@ int inhom_init(gpgmp_solver* h) {
                                   h->d_msums, h->d_meanx + s, h->stream));
         for (int s = 0; s < h->g.S; ++s)
             CK(launch_drift_jit(h->jit_drift, h->g, s, h->m.physical_length, 0.f, h->d_Dx, h->d_Dy, h->d_rx, h->d_ry,
-                                h->deterministic ? nullptr : &planes, h->moments ? h->d_meanx : nullptr, h->stream));
+                                h->deterministic ? nullptr : &planes, h->moments ? h->d_meanx : nullptr, h->d_fields,
+                                h->stream));
     } else if (h->m.drift_method == GPGMP_DRIFT_FIELD) {
         CK(cudaMemcpyAsync(h->d_Dx, h->m.field_dx, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_Dy, h->m.field_dy, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -350,7 +365,7 @@ int nonlinear_update(gpgmp_solver* h, int i, int dir, float t) {
         CK(launch_moments(planes.p[i] + (size_t)i * h->area, h->m.width, h->m.height, h->m.physical_length, h->d_msums,
                           h->d_meanx + i, h->stream));
     CK(launch_drift_jit(h->jit_drift, h->g, i, h->m.physical_length, t, h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, &planes,
-                        h->moments ? h->d_meanx : nullptr, h->stream));
+                        h->moments ? h->d_meanx : nullptr, h->d_fields, h->stream));
     const float dx = h->m.physical_length / (float)h->m.width;
     uint32_t key = 0;
     CK(launch_timestep((int)h->area, (dir == 0 ? h->d_Dx : h->d_Dy) + (size_t)i * h->area,
@@ -418,6 +433,8 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     h->m.custom_laws = nullptr;
     h->m.individual = nullptr;
     h->m.new_individuals_code = nullptr;
+    h->m.field_values = nullptr;
+    h->m.set_field_code = nullptr;
     if (any_ind) {
         h->ind.resize(model->num_species);
         for (int s = 0; s < model->num_species; ++s) h->ind[s].species = h->is_ind[s] ? s : -1;
@@ -493,6 +510,18 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     CKC(cudaMalloc(&h->d_diff, sizeof(float) * S));
     CKC(cudaMemcpy(h->d_diff, h->diffusion.data(), sizeof(float) * S, cudaMemcpyHostToDevice));
     CKC(cudaMalloc(&h->d_lambda, sizeof(float) * S));
+    if (model->num_fields > 0) {
+        const size_t fb = sizeof(float) * h->area * (size_t)model->num_fields;
+        h->nfields = model->num_fields;
+        CKC(cudaMalloc(&h->d_fields, fb));
+        if (model->field_values) CKC(cudaMemcpy(h->d_fields, model->field_values, fb, cudaMemcpyHostToDevice));
+        else CKC(cudaMemset(h->d_fields, 0, fb));
+    }
+    if (model->set_field_code && model->set_field_code[0]) {
+        h->set_field_code = model->set_field_code;
+        int rc2 = jit_field_kernel(h->code_defines, h->set_field_code, &h->jit_fields);
+        if (rc2) return fail(rc2);
+    }
     if (!h->reactions.empty()) {
         CKC(cudaMalloc(&h->d_reactions, sizeof(gpgmp_reaction) * h->reactions.size()));
         CKC(cudaMemcpy(h->d_reactions, h->reactions.data(), sizeof(gpgmp_reaction) * h->reactions.size(),
@@ -753,6 +782,32 @@ int gpgmp_timesteps(gpgmp_solver* h, float* dtx, float* dty) {
     return GPGMP_OK;
 }
 
+int gpgmp_update_fields(gpgmp_solver* h, float deltat, float simtime) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    if (!h->jit_fields) return GPGMP_OK;   // no setField method
+    return after_launch(h, launch_field_jit(h->jit_fields, h->g, h->m.physical_length, deltat, simtime, h->d_fields,
+                                            planes_of(h), h->stream));
+}
+
+int gpgmp_get_fields(gpgmp_solver* h, float* fields) {
+    if (!h || !fields) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (h->nfields <= 0) return GPGMP_OK;
+    CK(cudaMemcpyAsync(fields, h->d_fields, sizeof(float) * h->area * (size_t)h->nfields, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return GPGMP_OK;
+}
+
+int gpgmp_set_fields(gpgmp_solver* h, const float* fields) {
+    if (!h || !fields) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (h->nfields <= 0) return set_error(GPGMP_ERR_INVALID, "the model has no field parameters");
+    CK(cudaMemcpyAsync(h->d_fields, fields, sizeof(float) * h->area * (size_t)h->nfields, cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // the drift method reads the fields: like a state change, evaluate it again
+    return refresh_code_fields(h);
+}
+
 int gpgmp_individual_count(gpgmp_solver* h, int32_t species, int64_t* n) {
     if (!h || !n) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (species < 0 || species >= h->g.S || h->ind.empty() || h->ind[species].species < 0)
@@ -883,6 +938,10 @@ int gpgmp_solve_with_callback(gpgmp_solver* h, void* snaps, float* snap_times, i
         const float deltat = mindt - simTime;
         if (m.num_reactions > 0) {
             rc = gpgmp_do_reactions(h, deltat, &seed);
+            if (rc) return rc;
+        }
+        if (h->jit_fields && deltat > 0) {   // DiffusionModel.cpp:1536-1538
+            rc = gpgmp_update_fields(h, deltat, simTime);
             if (rc) return rc;
         }
         if (ev == 0) {

@@ -87,6 +87,11 @@ class DiffusionModel:
     # individual species (gpgmp_model_desc.individual_capacity / new_individuals_code)
     individual_capacity: int = 0
     new_individuals_code: Optional[str] = None
+    # field parameters: names (code reads field f as F(f); code_defines name them),
+    # initial values [F][H][W] (None: zeros) and the setField method
+    field_names: List[str] = field(default_factory=list)
+    field_values: Optional[np.ndarray] = None
+    set_field_code: Optional[str] = None
 
     # -- builders (DiffusionModel.cpp:426-493) --------------------------------
     def add_species(self, id: str, diffusion: float = 0.0, initial: float = 0.0,
@@ -183,6 +188,18 @@ class DiffusionModel:
                 b = self.new_individuals_code.encode()
                 keep.append(b)
                 d.new_individuals_code = b
+        if self.field_names:
+            d.num_fields = len(self.field_names)
+            if self.field_values is not None:
+                fv = np.ascontiguousarray(self.field_values, dtype=np.float32).reshape(-1)
+                if fv.size != len(self.field_names) * self.area:
+                    raise ValueError("field_values must hold [fields][height][width] values")
+                keep.append(fv)
+                d.field_values = fv.ctypes.data_as(C.POINTER(C.c_float))
+            if self.set_field_code:
+                b = self.set_field_code.encode()
+                keep.append(b)
+                d.set_field_code = b
         if self.custom_laws is not None:
             if len(self.custom_laws) != len(self.reactions):
                 raise ValueError("custom_laws needs one entry (or None) per reaction")

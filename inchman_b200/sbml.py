@@ -28,8 +28,12 @@ A nonlinear drift method (nonLinear="true", or computeMoments="true") that reads
 state, the time or MeanX is evaluated again after every sweep (GPGMP_FLAG_NONLINEAR,
 GPGMP_FLAG_COMPUTE_MOMENTS; one realisation per solver).
 
+Field parameters (domain "field") are per-cell values, zero until set (the reference's
+init scripts fill them): the model code reads them by name (F(f)), and the setField
+method, compiled at run time, updates them every step.
+
 Not supported (raises Unsupported): init and event scripts (Python run by the
-reference's executable), field parameters, reactions localised to part of the grid.
+reference's executable), reactions localised to part of the grid.
 """
 from __future__ import annotations
 
@@ -65,7 +69,8 @@ SOLVERS = {
 DRIFT_NAMES = {"All", "Real", "GridX", "GridY", "PhysicalX", "PhysicalY", "PhysicalModelWidth",
                "PhysicalModelHeight", "PhysicalCellWidth", "PhysicalCellHeight", "GridModelWidth",
                "GridModelHeight", "PhysicalSimTime", "DiffusivityX", "DiffusivityY", "DriftX", "DriftY", "State",
-               "MeanX", "SpeciesState"}
+               "MeanX", "SpeciesState", "getCentralDifferenceX", "getCentralDifferenceY", "getPhysicalX",
+               "getPhysicalY"}
 C_MATH = {"sin", "cos", "tan", "exp", "log", "sqrt", "pow", "fabs", "tanh", "sinh", "cosh", "atan", "atan2",
           "floor", "ceil", "fmin", "fmax", "asin", "acos", "if", "else", "return", "float", "int", "double",
           "sinf", "cosf", "expf", "logf", "sqrtf", "powf", "fabsf", "fminf", "fmaxf", "true", "false"}
@@ -287,14 +292,18 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
     notes: List[str] = []
     # parameters first: every MathML expression may refer to them
     params: Dict[str, float] = {}
+    fields: List[str] = []
     for p in model_e.iter(SB + "parameter"):
         a = p.find(f"{SB}annotation/{IM}parameter")
         domain = a.get("domain", "single") if a is not None else "single"
         if domain == "field":
-            raise Unsupported(f"field parameter {p.get('id')!r} (set by the model's scripts)")
+            # a per-cell value, zero until set (DiffusionModel.cpp:402-404, 778)
+            fields.append(p.get("id"))
+            continue
         if domain != "single":
             raise Unsupported(f"parameter domain {domain!r}")
         params[p.get("id")] = float(p.get("value", "0"))
+    fields.sort()      # the reference keeps them in a std::map: offsets in name order
     for k, v in (overrides or {}).items():
         params[k] = float(v)
     sb = root.find(f"{SB}annotation/{IM}sbml")
@@ -303,6 +312,7 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
     method = ""
     nonlinear = False
     moments = False
+    set_field = ""
     if sb is not None:
         solver = _text(sb.find(IM + "solver")) or "stochastic_inhomogeneous"
         if solver not in SOLVERS:
@@ -331,8 +341,7 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
             nonlinear = dd.get("nonLinear", "false") == "true"
             moments = dd.get("computeMoments", "") == "true"
         sf = sb.find(f"{IM}setField/{IM}method")
-        if sf is not None and _text(sf):
-            raise Unsupported("setField method (field parameters)")
+        set_field = _text(sf) if sf is not None else ""
         ni = sb.find(f"{IM}newIndividualsMethod/{IM}method")
         newind = _text(ni) if ni is not None else ""
     ma = model_e.find(f"{SB}annotation/{IM}model")
@@ -420,25 +429,35 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
     # drift / diffusivity method (inhomogeneous solvers)
     if m.solver in _lib.INHOMOGENEOUS_TYPES:
         used = drift_identifiers(method)
-        dynamic = used & {"PhysicalSimTime", "State", "SpeciesState", "MeanX"}
+        dynamic = used & {"PhysicalSimTime", "State", "SpeciesState", "MeanX", "getCentralDifferenceX",
+                          "getCentralDifferenceY"}
         if (nonlinear or moments) and dynamic:
             # evaluated again after every sweep (InhomogeneousSolver.cpp:288-335)
             if m.solver not in (_lib.STOCHASTIC_INHOMOGENEOUS, _lib.STOCHASTIC_INHOMOGENEOUS_FPE):
                 raise Unsupported(f"a nonlinear drift method that reads {sorted(dynamic)} with a deterministic solver")
             m.flags |= _lib.FLAG_NONLINEAR | (_lib.FLAG_COMPUTE_MOMENTS if moments else 0)
             notes.append("nonlinear drift method: one realisation per solver")
-        unknown = used - DRIFT_NAMES - set(params) - spset - C_MATH
+        unknown = used - DRIFT_NAMES - set(params) - set(fields) - spset - C_MATH
         declared = set(re.findall(r"\bReal\s+([A-Za-z_]\w*)", _COMMENT.sub(" ", method)))
         unknown -= declared
         if unknown:
             raise Unsupported(f"drift method uses {sorted(unknown)}")
-        defines = [f"#define {k} {c_float(v)}" for k, v in params.items()]
-        defines += [f"#define {sid} SP({i})" for i, sid in enumerate(species_ids)]
         m.drift_method = _lib.DRIFT_CODE
         m.drift_code = method
+    field_defines = [f"#define {f} F({i})" for i, f in enumerate(fields)]
+    if m.solver in _lib.INHOMOGENEOUS_TYPES:
+        defines = [f"#define {k} {c_float(v)}" for k, v in params.items()] + field_defines
+        defines += [f"#define {sid} SP({i})" for i, sid in enumerate(species_ids)]
         m.code_defines = "\n".join(defines)
-    elif m.custom_laws is not None:
-        m.code_defines = "\n".join(f"#define {k} {c_float(v)}" for k, v in params.items())
+    elif m.custom_laws is not None or fields:
+        m.code_defines = "\n".join([f"#define {k} {c_float(v)}" for k, v in params.items()] + field_defines)
+    if fields:
+        m.field_names = list(fields)
+        if set_field and _COMMENT.sub(" ", set_field).strip():
+            # in the setField method a species name is its count (Solver.cpp:606-612)
+            pre = "".join(f"#undef {sid}\n#define {sid} X({i})\n" for i, sid in enumerate(species_ids))
+            m.set_field_code = pre + set_field
+        notes.append("field parameters: " + ", ".join(fields) + " (zero until set)")
     if any(sp.individual for sp in m.species):
         if m.solver not in (_lib.STOCHASTIC_INHOMOGENEOUS, _lib.STOCHASTIC_INHOMOGENEOUS_FPE):
             raise Unsupported("individual species with a solver other than stochastic_inhomogeneous(_fpe)")

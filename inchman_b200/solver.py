@@ -107,6 +107,23 @@ class Solver:
                   dy.ctypes.data_as(C.POINTER(C.c_float)))
         return dx, dy
 
+    # -- field parameters ------------------------------------------------------------
+    def get_fields(self) -> np.ndarray:
+        """The field parameters [F][H][W] (synchronizeFieldBufferFromDevice)."""
+        m = self.model
+        out = np.zeros((len(m.field_names), m.height, m.width), np.float32)
+        if out.size:
+            _lib.call("gpgmp_get_fields", self._h, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def set_fields(self, fields):
+        a = np.ascontiguousarray(fields, dtype=np.float32)
+        _lib.call("gpgmp_set_fields", self._h, a.ctypes.data_as(C.POINTER(C.c_float)))
+
+    def update_fields(self, deltat: float, simtime: float):
+        """One pass of the setField method (Solver::updateFields)."""
+        _lib.call("gpgmp_update_fields", self._h, C.c_float(deltat), C.c_float(simtime))
+
     # -- individual species (IndividualSolver) --------------------------------------
     def individual_count(self, species: int) -> int:
         n = C.c_int64(0)

@@ -144,6 +144,20 @@ typedef struct gpgmp_model_desc {
     const uint8_t* individual;
     int64_t individual_capacity;
     const char* new_individuals_code;
+    /* Field parameters (DiffusionModel.cpp:402-404, Solver.cpp:88-101,736-747): per-cell
+     * values the model code reads as F(f) (field f of this cell); the caller's
+     * code_defines name them (e.g. "#define conc F(0)").
+     *  field_values:   [num_fields][H][W] initial values, NULL for zeros (the
+     *                  reference's init scripts fill them);
+     *  set_field_code: the setField method, statements run in every cell before the
+     *                  diffusion of every step with deltat > 0 (updateFields,
+     *                  Solver.cpp:269-272, the kernel of :583-653): F(f) and X(i) (the
+     *                  count of species i as a float, written back truncated) may be
+     *                  read and written; deltat and simtime are the step's.  One
+     *                  realisation per solver when it is set. */
+    int32_t num_fields;
+    const float* field_values;
+    const char* set_field_code;
 } gpgmp_model_desc;
 
 typedef struct gpgmp_solver gpgmp_solver;
@@ -193,6 +207,11 @@ int gpgmp_synchronize(gpgmp_solver* h);
 void* gpgmp_device_state(gpgmp_solver* h);
 /* computeTimestepX/Y + reduceBlocks + readback -- InhomogeneousSolver.cpp:468-500 */
 int gpgmp_timesteps(gpgmp_solver* h, float* dt_x, float* dt_y);
+/* Field parameters (Solver.h:59, :85-100): one setField pass (deltat, simtime), and
+ * the fields [num_fields][H][W] to and from the host. */
+int gpgmp_update_fields(gpgmp_solver* h, float deltat, float simtime);
+int gpgmp_get_fields(gpgmp_solver* h, float* fields);
+int gpgmp_set_fields(gpgmp_solver* h, const float* fields);
 /* Individual species.  Keys are r * width * height + cell (realisation r), sorted;
  * the reference's output pairs are key | id << 32 (IndividualSolver.h:6-9,
  * getPositionList, IndividualSolver.cpp:1295-1318).

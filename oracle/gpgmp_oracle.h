@@ -60,6 +60,9 @@ typedef struct orc_model {
     const uint8_t* individual;         /* individual species (the product's lists; the oracle restates */
     int64_t individual_capacity;       /* their steps in orc_individual.c) */
     const char* new_individuals_code;
+    int32_t num_fields;                /* field parameters (the product's F(f) in model code) */
+    const float* field_values;
+    const char* set_field_code;
 } orc_model;
 
 /* ---- generators and elementary functions ---------------------------------- */

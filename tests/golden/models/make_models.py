@@ -15,9 +15,12 @@ def num(v):
 
 
 def document(name, solver, W, L, time, out, params, comps, species, reactions, method="", newind=None,
-             individual=(), nonlinear=False, moments=False):
+             individual=(), nonlinear=False, moments=False, fields=(), set_field=None):
     ps = "\n".join(f'      <parameter id="{k}" value="{v}"><annotation><im:parameter xmlns:im="{IMNS}" '
                    f'type="float" domain="single"/></annotation></parameter>' for k, v in params.items())
+    if fields:
+        ps += "\n" + "\n".join(f'      <parameter id="{f}" value="0"><annotation><im:parameter xmlns:im="{IMNS}" '
+                                f'type="float" domain="field"/></annotation></parameter>' for f in fields)
     cs = "\n".join(f'      <compartment id="{cid}"><annotation><im:compartment xmlns:im="{IMNS}">'
                    f'<im:x>{num(x)}</im:x><im:y>{num(y)}</im:y><im:width>{num(w)}</im:width>'
                    f'<im:height>{num(h)}</im:height></im:compartment></annotation></compartment>'
@@ -51,7 +54,7 @@ def document(name, solver, W, L, time, out, params, comps, species, reactions, m
   <im:init type="python"><im:script><![CDATA[]]></im:script></im:init>
   <im:events type="python"><im:script><![CDATA[]]></im:script><im:listOfTimeStamps/></im:events>
   <im:driftDiffusivity nonLinear="{"true" if nonlinear else "false"}" computeMoments="{"true" if moments else ""}"><im:method><![CDATA[{method}]]></im:method></im:driftDiffusivity>
-{"" if newind is None else f"  <im:newIndividualsMethod><im:method><![CDATA[{newind}]]></im:method></im:newIndividualsMethod>" + chr(10)}</im:sbml></annotation>
+{"" if newind is None else f"  <im:newIndividualsMethod><im:method><![CDATA[{newind}]]></im:method></im:newIndividualsMethod>" + chr(10)}{"" if set_field is None else f"  <im:setField><im:method><![CDATA[{set_field}]]></im:method></im:setField>" + chr(10)}</im:sbml></annotation>
   <model name="{name}">
 <annotation><im:model xmlns:im="{IMNS}"><im:gridWidth>{num(W)}</im:gridWidth><im:gridHeight>{num(W)}</im:gridHeight>
 <im:physicalWidth>{num(L)}</im:physicalWidth><im:physicalHeight>{num(L)}</im:physicalHeight></im:model></annotation>
@@ -134,8 +137,17 @@ def main():
         method="All->DiffusivityX = 0.3 + 0.02 * All->State;\nAll->DiffusivityY = 0.3;\n"
                "All->DriftX = -pull * (PhysicalX - All->MeanX);\nAll->DriftY = 0.0;",
         nonlinear=True, moments=True)
+    # a field parameter: the setField method accumulates where A is, the drift method
+    # reads it
+    fd = document(
+        "Trace field", "stochastic_inhomogeneous", 12, 12.0, 0.4, 0.2, {"rate": 0.5},
+        {"World": (0, 0, 12, 12)},
+        {"A": (0.0, {"World": 12 * 12 * 8})}, {},
+        method="All->DiffusivityX = 0.4 + 0.0 * trace;\nAll->DiffusivityY = 0.4;\nAll->DriftX = 0.0;\n"
+               "All->DriftY = 0.0;",
+        fields=("trace",), set_field="trace = trace + rate * deltat * A;")
     for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm), ("individual_a.xml", ind),
-                       ("nonlinear.xml", nl)):
+                       ("nonlinear.xml", nl), ("field_trace.xml", fd)):
         with open(os.path.join(HERE, name), "w") as f:
             f.write(text)
 

@@ -98,9 +98,12 @@ def test_reference_examples_load_or_name_what_is_missing():
     assert ab.reactions[0].reactants == {"SpeciesA": 2}
     ind = ok["ABReactionIndividual.xml"]
     assert [sp.individual for sp in ind.species][:2] == [True, True]
-    assert "field parameter" in unsupported["Slit.xml"]
-    # a species name with digits (B00 ... B44) is not a number followed by a name
-    assert "RandomDrift.xml" not in unsupported or "script" in unsupported["RandomDrift.xml"]
+    # what still needs its Python script is named; without the scripts all load
+    assert all("script" in why for why in unsupported.values()), unsupported
+    for name in unsupported:
+        sbml.load(os.path.join(REF_EXAMPLES, name), ignore_scripts=True)
+    slit = sbml.load(os.path.join(REF_EXAMPLES, "Slit.xml"), ignore_scripts=True).model
+    assert slit.field_names and slit.flags & 1          # field parameters, nonlinear method
     # without its (Python 2) init script the Calcium model loads, with custom laws
     ca = sbml.load(os.path.join(REF_EXAMPLES, "Calcium.xml"), ignore_scripts=True).model
     assert ca.custom_laws is not None and sum(l is not None for l in ca.custom_laws) >= 3

@@ -132,3 +132,20 @@ def test_cli_runs_a_nonlinear_model_one_solver_per_run(gpgmp, tmp_path):
     assert not np.array_equal(finals[0], finals[1])          # two different runs
     # mass left the strip x < 5 it started in (the datasets hold the [y][x] buffer)
     assert finals[0].reshape(16, 16)[:, 5:].sum() > 0
+
+
+@pytest.mark.gpu
+def test_cli_writes_field_parameters(gpgmp, tmp_path):
+    """A model with a field parameter that its setField method accumulates: every dump
+    has a Fields group; the field starts at zero and grows where A is."""
+    path = _variant(tmp_path, "field_trace.xml", runs=2)
+    out = str(tmp_path / "f.h5")
+    assert cli.main([path, "--output", out, "--seed", "9"]) == 0
+    f = h5.read(out)
+    for r in ("0", "1"):
+        by_time = sorted(f[f"Runs/{r}"], key=lambda nm: float(f[f"Runs/{r}/{nm}"].attrs["time"][0]))
+        tr = [f[f"Runs/{r}/{nm}/Fields/trace"].value for nm in by_time]
+        assert tr[0].dtype == np.float32 and tr[0].shape == (12, 12)
+        assert np.all(tr[0] == 0)
+        assert np.all(np.diff(np.stack(tr).reshape(len(tr), -1), axis=0) >= 0)
+        assert tr[-1].sum() > 0
