@@ -91,25 +91,6 @@ cudaError_t run_fields(const IndKernels& k, const IndArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// sort by key, cell offsets (with the killed bin last), killed ids back to the pool
-int sort_and_count(IndList& l, IndArgs& a, cudaStream_t st) {
-    const int c = l.cur;
-    if (l.n > 0) {
-        CK(radix_sort_pairs_u32(l.keys[c], l.ids[c], l.keys[1 - c], l.ids[1 - c], l.n, l.key_bits, l.sort_scratch, st));
-        l.cur = 1 - c;
-    }
-    CK(cell_offsets_u32(l.keys[l.cur], l.n, l.ncells + 1, l.start[0], l.count, l.scan_scratch, st));
-    CK(cudaMemcpyAsync(&l.d_small[0], l.count + l.ncells, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(&l.d_small[1], (const char*)l.scan_scratch + scan_error_flag_offset(), sizeof(uint32_t),
-                       cudaMemcpyDeviceToDevice, st));
-    if (l.n > 0)   // the sort's own look-back error word
-        CK(cudaMemcpyAsync(&l.d_small[2], (const char*)l.sort_scratch + sort_layout(l.n, l.key_bits).off_counters + 16,
-                           sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    else
-        CK(cudaMemsetAsync(&l.d_small[2], 0, sizeof(uint32_t), st));
-    return GPGMP_OK;
-}
-
 void bind(IndList& l, IndArgs& a) {
     a.keys = l.keys[l.cur];
     a.ids = l.ids[l.cur];
@@ -124,16 +105,19 @@ void bind(IndList& l, IndArgs& a) {
     a.fRx = l.fields + 2 * l.ncells;
     a.fRy = l.fields + 3 * l.ncells;
     a.newborn = l.newborn;
+    a.killed = l.d_small;
 }
 
 }  // namespace
 
-int ind_alloc(IndList& l, int species, long long cap, long long ncells) {
+int ind_alloc(IndList& l, int species, long long cap, long long ncells, bool may_leave) {
     ind_free(l);
     l.species = species;
     l.cap = cap > 0 ? cap : 1;
     l.ncells = ncells;
-    l.key_bits = bits_for((uint32_t)ncells);
+    // the killed key (ncells) only occurs with an absorbing wall: without one the sort
+    // needs the bits of the last cell only
+    l.key_bits = bits_for((uint32_t)(may_leave ? ncells : ncells - 1));
     l.sort_bytes = sort_layout(l.cap, l.key_bits).bytes;
     l.scan_bytes = scan_scratch_bytes(ncells + 1);
     l.pop_bytes = 0;
@@ -155,7 +139,7 @@ int ind_alloc(IndList& l, int species, long long cap, long long ncells) {
     A((void**)&l.count, cb);
     A((void**)&l.goal, cb);
     A((void**)&l.fields, 4 * sizeof(float) * (size_t)ncells);
-    A((void**)&l.d_small, 3 * sizeof(uint32_t));
+    A((void**)&l.d_small, sizeof(uint32_t));
     A(&l.sort_scratch, l.sort_bytes);
     A(&l.scan_scratch, l.scan_bytes);
     A(&l.pop_scratch, l.pop_bytes);
@@ -181,7 +165,39 @@ void ind_free(IndList& l) {
     l.species = sp;
 }
 
+int ind_sort(IndList& l, cudaStream_t st) {
+    if (l.sorted) return GPGMP_OK;
+    const int c = l.cur;
+    if (l.n > 0) {
+        CK(radix_sort_pairs_u32(l.keys[c], l.ids[c], l.keys[1 - c], l.ids[1 - c], l.n, l.key_bits, l.sort_scratch, st));
+        l.cur = 1 - c;
+    }
+    CK(cell_offsets_u32(l.keys[l.cur], l.n, l.ncells + 1, l.start[0], l.count, l.scan_scratch, st));
+    uint32_t err[2] = {0, 0};
+    CK(cudaMemcpyAsync(&err[0], (const char*)l.scan_scratch + scan_error_flag_offset(), sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, st));
+    if (l.n > 0)
+        CK(cudaMemcpyAsync(&err[1], (const char*)l.sort_scratch + sort_layout(l.n, l.key_bits).off_counters + 16,
+                           sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    if (l.pending > 0) {
+        // the ones that left sort last: their ids go to the end of the pool
+        const long long alive = l.n - l.pending;
+        CK(cudaMemcpyAsync(l.pool[l.pcur] + l.npool, l.ids[l.cur] + alive, sizeof(uint32_t) * (size_t)l.pending,
+                           cudaMemcpyDeviceToDevice, st));
+        l.npool += l.pending;
+        l.n = alive;
+        l.pending = 0;
+        CK(cudaMemsetAsync(l.count + l.ncells, 0, sizeof(uint32_t), st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (err[0] || err[1]) return set_error(GPGMP_ERR_TIMEOUT, "a look-back wait of the sort or scan gave up");
+    l.sorted = true;
+    return GPGMP_OK;
+}
+
 int ind_fields(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {
+    int rc = ind_sort(l, st);
+    if (rc) return rc;
     bind(l, a);
     CK(run_fields(k, a, st));
     return GPGMP_OK;
@@ -222,36 +238,28 @@ int ind_build(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {
 int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, uint32_t* d_minkey,
               float* dt_out, cudaStream_t st) {
     bind(l, a);
+    CK(cudaMemsetAsync(l.count, 0, sizeof(uint32_t) * (size_t)(l.ncells + 1), st));
+    CK(cudaMemsetAsync(l.fields, 0, 4 * sizeof(float) * (size_t)l.ncells, st));
+    CK(cudaMemsetAsync(l.d_small, 0, sizeof(uint32_t), st));
     CK(run_sweep(k, a, st));
-    int rc = sort_and_count(l, a, st);
-    if (rc) return rc;
-    bind(l, a);
-    CK(run_fields(k, a, st));
+    l.sorted = false;
     k_ind_counts<<<grid_for(l.ncells), kIndThreads, 0, st>>>(a);
     CK(cudaGetLastError());
     const float* D = a.dir == 0 ? a.fDx : a.fDy;
     const float* r = a.dir == 0 ? a.fRx : a.fRy;
     CK(launch_timestep((int)l.ncells, D, r, dx, d_minkey, st, ts_kind, stay));
-    uint32_t h[4] = {0, 0, 0, 0};
-    CK(cudaMemcpyAsync(&h[0], l.d_small, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&h[3], d_minkey, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t h[2] = {0, 0};
+    CK(cudaMemcpyAsync(&h[0], l.d_small, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&h[1], d_minkey, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (h[1] || h[2]) return set_error(GPGMP_ERR_TIMEOUT, "a look-back wait of the sort or scan gave up");
-    const long long killed = h[0];
-    if (killed > 0) {
-        // individuals that left through an absorbing wall: their ids go to the end of the pool
-        const long long alive = l.n - killed;
-        CK(cudaMemcpyAsync(l.pool[l.pcur] + l.npool, l.ids[l.cur] + alive, sizeof(uint32_t) * (size_t)killed,
-                           cudaMemcpyDeviceToDevice, st));
-        l.npool += killed;
-        l.n = alive;
-        CK(cudaMemsetAsync(l.count + l.ncells, 0, sizeof(uint32_t), st));
-    }
-    *dt_out = key_to_float(h[3]);
+    l.pending += h[0];
+    *dt_out = key_to_float(h[1]);
     return GPGMP_OK;
 }
 
 int ind_maintain(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {
+    int rc0 = ind_sort(l, st);
+    if (rc0) return rc0;
     bind(l, a);
     k_ind_gather<<<grid_for(l.ncells), kIndThreads, 0, st>>>(a, l.goal);
     CK(cudaGetLastError());

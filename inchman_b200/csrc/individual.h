@@ -22,9 +22,9 @@ struct IndList {
     uint8_t* newborn = nullptr;       // [cap]
     uint32_t* start[2] = {nullptr, nullptr};   // [ncells + 1] first list position per key (+ the killed bin)
     uint32_t* count = nullptr;        // [ncells + 1]
-    int32_t* goal = nullptr;          // [ncells] counts to maintain
+    int32_t* goal = nullptr;          // [ncells + 1] counts to maintain
     float* fields = nullptr;          // [4][ncells]
-    uint32_t* d_small = nullptr;      // [3]: killed count, scan and sort error words (read after a sweep)
+    uint32_t* d_small = nullptr;      // individuals that left in the last sweep
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     void* scan_scratch = nullptr;
@@ -32,6 +32,8 @@ struct IndList {
     void* pop_scratch = nullptr;
     size_t pop_bytes = 0;
     int key_bits = 0;
+    bool sorted = true;               // the list is in key order (and start/count describe it)
+    long long pending = 0;            // left through an absorbing wall, still in the list until sorted
 };
 
 // The kernels of a model: prebuilt (no model code) or compiled with its drift /
@@ -41,15 +43,16 @@ struct IndKernels {
     bool newborn_active = false;
 };
 
-int ind_alloc(IndList& l, int species, long long cap, long long ncells);
+// may_leave: a wall is absorbing, so individuals can leave (their key is ncells)
+int ind_alloc(IndList& l, int species, long long cap, long long ncells, bool may_leave);
 void ind_free(IndList& l);
 
 // Builds the list from the counts of the species in the state (ids 0.. in cell
 // order, properties 0 for them and (1, 1, 0, 0) for the ids not yet used, as the
 // reference's IndividualSolver constructor fills them), then the fields.
 int ind_build(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st);
-// One sweep (a.dir), then sort, counts, fields and the new time step of that
-// direction (the smallest over every cell of every realisation) in *dt_out.
+// One sweep (a.dir) with the counts and fields folded in, then the new time step of
+// that direction (the smallest over every cell of every realisation) in *dt_out.
 int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, uint32_t* d_minkey,
               float* dt_out, cudaStream_t st);
 // After a reaction window: the list follows the counts (population bookkeeping);
@@ -57,6 +60,11 @@ int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind,
 int ind_maintain(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st);
 // Fields only (after the properties changed from the host).
 int ind_fields(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st);
+// Puts the list in key order (stable) and drops the individuals that left; the
+// sweeps leave it unsorted (they fold counts and fields in directly).
+int ind_sort(IndList& l, cudaStream_t st);
+// individuals in the list that are still in the domain
+inline long long ind_count(const IndList& l) { return l.n - l.pending; }
 
 // run-time compiled variants (jit.cpp)
 int jit_ind_kernels(const std::string& defines, const std::string& drift_code, const std::string& newborn_code,

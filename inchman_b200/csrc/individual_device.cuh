@@ -15,7 +15,10 @@
 //           leaves (key = the killed key, its id goes back to the pool).
 //   fields  (computeDiffusionConstants, IndividualSolver.cl:654-748): per cell, the
 //           largest diffusivity and drift magnitude the method gives its individuals
-//           (for the next time step) and the cell's new count.
+//           (for the next time step) and the cell's new count.  The sweep folds them in
+//           as it moves each individual (atomic maxima and counts), so the list needs no
+//           sort per sweep -- it is sorted when the bookkeeping or a reader needs the
+//           cell order; the draws are keyed by id, so the results do not depend on it.
 //   newborn (updateNewParticles, IndividualSolver.cl:1135-1293): the new-individuals
 //           method sets the properties of each individual created by a reaction
 //           window; RANDOM is a uniform draw.
@@ -57,6 +60,7 @@ struct IndArgs {
     float* fRx;                    // largest |DriftX|
     float* fRy;
     uint8_t* newborn;              // [cap] flag by id (newborn)
+    uint32_t* killed;              // individuals that left in this sweep (sweep)
 };
 
 // Where an individual is, for the methods (the same names the field kernels give them).
@@ -99,6 +103,11 @@ struct IndNewbornKeep {
     __device__ __forceinline__ void operator()(IndSpecies&, const IndArgs&, const IndPos&, Stream&) const {}
 };
 
+// largest non-negative float by its bits (they order as unsigned integers)
+__device__ __forceinline__ void ind_max_field(float* f, float v) {
+    if (v > 0.f) atomicMax(reinterpret_cast<unsigned int*>(f), __float_as_uint(v));
+}
+
 template <class DRIFT>
 __device__ __forceinline__ void ind_sweep_body(const IndArgs& a, const DRIFT& drift) {
     const long long area = (long long)a.W * a.H;
@@ -120,20 +129,38 @@ __device__ __forceinline__ void ind_sweep_body(const IndArgs& a, const DRIFT& dr
         st.init(a.seed, (uint32_t)r, a.step_seed, id, PH_INDIV | ((uint32_t)a.species << 8) | (uint32_t)a.dir);
         const float u = u01(st.next());
         const int mv = u < Pp ? 1 : (u < Pp + Pm ? -1 : 0);
-        if (mv == 0) continue;
-        const int c = a.dir == 0 ? pos.GridX : pos.GridY;
-        const int lim = a.dir == 0 ? a.W : a.H;
-        const int nc = c + mv;
-        uint32_t out;
-        if (nc < 0 || nc >= lim) {
-            const int wall = (a.dir == 0 ? 0 : 2) + (mv > 0 ? 1 : 0);
-            if (a.bmask[wall] == 0) continue;          // reflecting: the move is cancelled
-            out = a.killed_key;                        // absorbing: the individual leaves
-        } else {
-            const int ncell = a.dir == 0 ? pos.GridY * a.W + nc : nc * a.W + pos.GridX;
-            out = (uint32_t)((long long)r * area + ncell);
+        uint32_t out = key;
+        if (mv != 0) {
+            const int c = a.dir == 0 ? pos.GridX : pos.GridY;
+            const int lim = a.dir == 0 ? a.W : a.H;
+            const int nc = c + mv;
+            if (nc < 0 || nc >= lim) {
+                const int wall = (a.dir == 0 ? 0 : 2) + (mv > 0 ? 1 : 0);
+                if (a.bmask[wall] != 0) out = a.killed_key;   // absorbing: the individual leaves
+                // reflecting: the move is cancelled
+            } else {
+                const int ncell = a.dir == 0 ? pos.GridY * a.W + nc : nc * a.W + pos.GridX;
+                out = (uint32_t)((long long)r * area + ncell);
+            }
+            a.keys[i] = out;
         }
-        a.keys[i] = out;
+        if (out >= a.killed_key) {
+            atomicAdd(a.killed, 1u);
+            continue;
+        }
+        // the cell it is in now: its count, and its method's values for the cell's
+        // largest diffusivity and drift (computeDiffusionConstants; State is the cell's
+        // count before this sweep, as the reference's state buffer still holds it)
+        if (a.fDx) {
+            const int ncell = (int)(out - (long long)r * area);
+            IndSpecies sp2 = ind_load(a, id, r, ncell);
+            drift(sp2, a, ind_pos(a, ncell));
+            ind_max_field(a.fDx + out, sp2.DiffusivityX);
+            ind_max_field(a.fDy + out, sp2.DiffusivityY);
+            ind_max_field(a.fRx + out, fabsf(sp2.DriftX));
+            ind_max_field(a.fRy + out, fabsf(sp2.DriftY));
+            atomicAdd(const_cast<uint32_t*>(a.count) + out, 1u);
+        }
     }
 }
 

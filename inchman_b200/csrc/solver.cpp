@@ -280,7 +280,9 @@ int ind_refresh(gpgmp_solver* h, const int32_t* host_state) {
             if (cap >= ((long long)1 << 31)) cap = ((long long)1 << 31) - 1;
         }
         if (l.cap != cap || l.ncells != ncells || !l.keys[0]) {
-            int rc = ind_alloc(l, s, cap, ncells);
+            bool may_leave = false;
+            for (int b = 0; b < 4; ++b) may_leave = may_leave || h->m.boundary_mask[b] != 0;
+            int rc = ind_alloc(l, s, cap, ncells, may_leave);
             if (rc) return rc;
         }
         int rc = ind_build(l, ind_args(h, s, 0, 0.f, 0u), h->ind_k, h->stream);
@@ -812,13 +814,15 @@ int gpgmp_individual_count(gpgmp_solver* h, int32_t species, int64_t* n) {
     if (!h || !n) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (species < 0 || species >= h->g.S || h->ind.empty() || h->ind[species].species < 0)
         return set_error(GPGMP_ERR_INVALID, "species %d is not an individual species", species);
-    *n = h->ind[species].n;
+    *n = ind_count(h->ind[species]);
     return GPGMP_OK;
 }
 
 int gpgmp_get_individuals(gpgmp_solver* h, int32_t species, uint32_t* keys, uint32_t* ids, float* props,
                           int64_t capacity, int64_t* n) {
     int rc = gpgmp_individual_count(h, species, n);
+    if (rc) return rc;
+    rc = ind_sort(h->ind[species], h->stream);   // the cell order (the sweeps leave it unsorted)
     if (rc) return rc;
     const IndList& l = h->ind[species];
     const long long m = l.n < capacity ? l.n : (capacity > 0 ? capacity : 0);

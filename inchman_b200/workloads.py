@@ -5,6 +5,7 @@ seeded.  Units:
   cell-steps/s      lattice cells x realisations x event-loop steps per second
   particle-steps/s  particles x steps per second
   individuals/s     individuals in the list x bookkeeping calls per second
+  individual-sweeps/s  individuals x directional sweeps per second
 """
 from __future__ import annotations
 
@@ -280,9 +281,80 @@ def population(args, rank, world):
                                "algorithmic_bytes_per_step": alg}})
 
 
+def individuals(args, rank, world):
+    """Individual species in the drift-diffusion solver: 256 x 256 cells, 4 individuals
+    per cell (262,144, the reference's c_maxNumIndividuals), each with its own
+    diffusivity (0.3..0.7) and drift (-0.2..0.2); one step = one x and one y sweep of
+    every individual (one kernel moves it and folds its cell's count and fields in,
+    then the counts go to the state and the time step is read back; the list is
+    sorted only when read).  Unit: individual-sweeps/s.
+
+    Roofline: per individual and sweep the bytes that must move at least once -- read
+    key, id and four properties, write the key (28 B) -- plus 24 B per cell (count and
+    four fields written and read, the state written)."""
+    import torch
+    from . import _lib
+    from .model import DiffusionModel
+    from .solver import Solver
+    W = 256
+    m = DiffusionModel(width=W, height=W, physical_length=float(W), solver=_lib.STOCHASTIC_INHOMOGENEOUS)
+    m.add_species("A", 0.0, individual=True)
+    m.drift_method = _lib.DRIFT_HOMOGENEOUS
+    m.drift_params = [0.5, 0.5, 0.0, 0.0] + [0.0] * 4
+    m.individual_capacity = 1 << 19
+    st = np.full((1, 1, W, W), 4, np.int32)
+    n = int(st.sum())
+    rng = np.random.default_rng(1234)
+    props = np.stack([rng.uniform(0.3, 0.7, n), rng.uniform(0.3, 0.7, n), rng.uniform(-0.2, 0.2, n),
+                      rng.uniform(-0.2, 0.2, n)]).astype(np.float32)
+    with Solver(m, realisations=1, seed=1234) as s:
+        s.set_state(st)
+        s.set_individual_properties(0, props)
+        seed = 1
+        t = 0.0
+
+        def one_step(seed, t):
+            dx, dy = s.timesteps()
+            t = t + float(max(dx[0], dy[0]))
+            return s.diffuse(0, t, seed), t
+
+        for _ in range(args.warmup):
+            seed, t = one_step(seed, t)
+        torch.cuda.synchronize()
+        a, b = _events()
+        a.record()
+        for _ in range(args.steps):
+            seed, t = one_step(seed, t)
+        b.record()
+        torch.cuda.synchronize()
+        tsec = a.elapsed_time(b) / 1e3
+        n_end = s.individual_count(0)
+    sweeps = 2 * args.steps
+    value = n * sweeps / tsec
+    alg = 28 * n + 24 * W * W                           # per sweep
+    ach = alg / (tsec / sweeps) / 1e9
+    peak, peak_kind = _peaks()
+    return _base(args, world, value, "individual-sweeps/s", "individuals_256x256_262144",
+                 {"grid": [W, W], "individuals": n, "steps_timed": args.steps, "sweeps_per_step": 2},
+                 tsec / args.steps * 1e3,
+                 {"dtype": "u32+f32", "individuals_left": n_end,
+                  # per sweep: the fused move, the counts, the time step
+                  "gpu_launches": 3 * sweeps,
+                  "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                               "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_sweep": alg}})
+
+
+def _peaks():
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import load_peaks
+    return load_peaks()
+
+
 def run(args, rank, world):
     table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles,
-             "ensemble": ensemble, "population": population}
+             "ensemble": ensemble, "population": population, "individuals": individuals}
     if args.workload not in table:
         raise SystemExit(f"unknown workload {args.workload}; one of gray_scott, {', '.join(table)}")
     return table[args.workload](args, rank, world)

@@ -102,8 +102,10 @@ float orc_rep_timestep(const orc_model* m, int species, int sweep_y, const float
 void orc_rep_diffusivity_drift(const orc_model* m, int species, float* dx, float* dy, float* rx, float* ry);
 void orc_set_custom_hazard(float (*fn)(int r, const int32_t* x));
 int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int dir, float dt,
-                          uint32_t step_seed, uint32_t* keys, uint32_t* ids, int64_t n, const float* props,
-                          int64_t cap, float* fields, uint32_t* killed_ids, int64_t* n_killed);
+                          uint32_t step_seed, uint32_t* keys, const uint32_t* ids, int64_t n, const float* props,
+                          int64_t cap, float* fields);
+int64_t orc_rep_ind_sort(uint32_t* keys, uint32_t* ids, int64_t n, int64_t ncells, uint32_t* killed_ids,
+                         int64_t* n_killed);
 float orc_rep_timestep_cells(const float* D, const float* r, int64_t n, float dx);
 int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
                   int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots,

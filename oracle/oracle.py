@@ -66,7 +66,8 @@ def orc():
             "orc_rep_inhomog_sweep": (None, [vp, vp, C.c_int, u32, C.c_int, C.c_int, u32, f32, vp, vp]),
             "orc_rep_timestep": (f32, [vp, C.c_int, C.c_int, vp, vp]),
             "orc_rep_ind_sweep": (C.c_int64, [vp, vp, C.c_int, C.c_uint32, C.c_int, C.c_int, f32, C.c_uint32, vp, vp,
-                                              C.c_int64, vp, C.c_int64, vp, vp, vp]),
+                                              C.c_int64, vp, C.c_int64, vp]),
+            "orc_rep_ind_sort": (C.c_int64, [vp, vp, C.c_int64, C.c_int64, vp, vp]),
             "orc_rep_timestep_cells": (f32, [vp, vp, C.c_int64, f32]),
             "orc_rep_diffusivity_drift": (None, [vp, C.c_int, vp, vp, vp, vp]),
             "orc_rep_solve": (C.c_int, [vp, vp, C.c_int, u32, vp, vp, C.c_int, P(C.c_int), P(i64), vp]),

@@ -438,25 +438,31 @@ int orc_rep_solve(const orc_model* m, int32_t* state, int R, uint32_t seed,
 
 /* ---- individual species ------------------------------------------------------------
  * One sweep of an individual species with the properties as stored (no model code),
- * restating individual_device.cuh (ind_sweep_body, ind_fields_body, ind_counts_body)
- * and individual.cu (ind_sweep) after the reference's individual_diffuseX/Y,
- * computeDiffusionConstants and computeCellIndices (IndividualSolver.cl:654-1015,
- * IndividualSolver.cpp:1083-1153): every individual draws once (stream (seed, r),
+ * restating individual_device.cuh (ind_sweep_body, ind_counts_body) after the
+ * reference's individual_diffuseX/Y and computeDiffusionConstants
+ * (IndividualSolver.cl:654-1015): every individual draws once (stream (seed, r),
  * counter (step_seed, id, PH_INDIV | species << 8 | dir)) and moves one cell with the
- * inhomogeneous sweep's probabilities of its own D and r, reflecting walls cancel the
- * move, absorbing walls remove it; then the stable sort by key, the counts into the
- * species' planes and the fields [4][R*area] (largest D x, D y, |r x|, |r y| per cell).
- * keys/ids: the list (sorted by key = r*area + cell), updated in place; removed ids are
- * written to killed_ids (list order).  Returns the new list length. */
+ * inhomogeneous sweep's probabilities of its own D and r; reflecting walls cancel the
+ * move, absorbing walls remove it (key = R * area).  Then the counts of the species'
+ * planes and the fields [4][R*area] (largest D x, D y, |r x|, |r y| of the individuals
+ * in each cell).  keys are updated in place and not sorted (orc_rep_ind_sort sorts);
+ * returns the number that left in this sweep. */
 int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t seed, int species, int dir, float dt,
-                          uint32_t step_seed, uint32_t* keys, uint32_t* ids, int64_t n, const float* props,
-                          int64_t cap, float* fields, uint32_t* killed_ids, int64_t* n_killed) {
+                          uint32_t step_seed, uint32_t* keys, const uint32_t* ids, int64_t n, const float* props,
+                          int64_t cap, float* fields) {
     const int W = m->width, H = m->height, S = m->num_species;
     const int64_t area = (int64_t)W * H, ncells = area * R;
     const float dx = m->physical_length / (float)(dir == 0 ? W : H);
     const uint32_t killed = (uint32_t)ncells;
+    int64_t left = 0;
+    for (int64_t k = 0; k < 4 * ncells; ++k) fields[k] = 0.f;
+    for (int64_t k = 0; k < ncells; ++k) {
+        const int r = (int)(k / area);
+        state[((int64_t)r * S + species) * area + (k - (int64_t)r * area)] = 0;
+    }
     for (int64_t i = 0; i < n; ++i) {
         const uint32_t key = keys[i], id = ids[i];
+        if (key >= killed) continue;
         const int r = (int)(key / area);
         const int cell = (int)(key - (int64_t)r * area);
         const int gx = cell % W, gy = cell / W;
@@ -468,18 +474,31 @@ int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t se
         orc_stream_init(&s, seed, (uint32_t)r, step_seed, id, ORC_PH_INDIV | ((uint32_t)species << 8) | (uint32_t)dir);
         const float u = orc_u01(orc_stream_next(&s));
         const int mv = u < Pp ? 1 : (u < Pp + Pm ? -1 : 0);
-        if (mv == 0) continue;
-        const int c = dir == 0 ? gx : gy, lim = dir == 0 ? W : H, nc = c + mv;
-        if (nc < 0 || nc >= lim) {
-            const int wall = (dir == 0 ? 0 : 2) + (mv > 0 ? 1 : 0);
-            if (m->boundary_mask[wall] == 0) continue;
-            keys[i] = killed;
-        } else {
-            const int ncell = dir == 0 ? gy * W + nc : nc * W + gx;
-            keys[i] = (uint32_t)((int64_t)r * area + ncell);
+        uint32_t out = key;
+        if (mv != 0) {
+            const int c = dir == 0 ? gx : gy, lim = dir == 0 ? W : H, nc = c + mv;
+            if (nc < 0 || nc >= lim) {
+                const int wall = (dir == 0 ? 0 : 2) + (mv > 0 ? 1 : 0);
+                if (m->boundary_mask[wall] != 0) out = killed;
+            } else {
+                out = (uint32_t)((int64_t)r * area + (dir == 0 ? gy * W + nc : nc * W + gx));
+            }
+            keys[i] = out;
         }
+        if (out >= killed) { ++left; continue; }
+        state[((int64_t)r * S + species) * area + (out - (int64_t)r * area)] += 1;
+        fields[out] = fmaxf(fields[out], props[id]);
+        fields[ncells + out] = fmaxf(fields[ncells + out], props[cap + id]);
+        fields[2 * ncells + out] = fmaxf(fields[2 * ncells + out], fabsf(props[2 * cap + id]));
+        fields[3 * ncells + out] = fmaxf(fields[3 * ncells + out], fabsf(props[3 * cap + id]));
     }
-    /* stable sort by key: counting sort over ncells + 1 bins */
+    return left;
+}
+
+/* the list in key order (a stable sort), the individuals that left (key ncells) taken
+ * out: their ids are written to killed_ids; returns the remaining length */
+int64_t orc_rep_ind_sort(uint32_t* keys, uint32_t* ids, int64_t n, int64_t ncells, uint32_t* killed_ids,
+                         int64_t* n_killed) {
     int64_t* cnt = (int64_t*)calloc((size_t)ncells + 2, sizeof(int64_t));
     uint32_t* k2 = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     uint32_t* i2 = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
@@ -492,25 +511,10 @@ int64_t orc_rep_ind_sweep(const orc_model* m, int32_t* state, int R, uint32_t se
     }
     int64_t alive = 0, nk = 0;
     for (int64_t i = 0; i < n; ++i) {
-        if (k2[i] == killed) killed_ids[nk++] = i2[i];
+        if (k2[i] >= (uint32_t)ncells) killed_ids[nk++] = i2[i];
         else { keys[alive] = k2[i]; ids[alive] = i2[i]; ++alive; }
     }
     *n_killed = nk;
-    /* fields (State before the counts change is not used without model code) and counts */
-    for (int64_t k = 0; k < ncells; ++k) fields[k] = fields[ncells + k] = fields[2 * ncells + k] = fields[3 * ncells + k] = 0.f;
-    for (int64_t k = 0; k < ncells; ++k) {
-        const int r = (int)(k / area);
-        state[((int64_t)r * S + species) * area + (k - (int64_t)r * area)] = 0;
-    }
-    for (int64_t i = 0; i < alive; ++i) {
-        const uint32_t k = keys[i], id = ids[i];
-        const int r = (int)(k / area);
-        state[((int64_t)r * S + species) * area + (k - (int64_t)r * area)] += 1;
-        fields[k] = fmaxf(fields[k], props[id]);
-        fields[ncells + k] = fmaxf(fields[ncells + k], props[cap + id]);
-        fields[2 * ncells + k] = fmaxf(fields[2 * ncells + k], fabsf(props[2 * cap + id]));
-        fields[3 * ncells + k] = fmaxf(fields[3 * ncells + k], fabsf(props[3 * cap + id]));
-    }
     free(cnt); free(k2); free(i2);
     return alive;
 }

@@ -99,15 +99,19 @@ def test_sweeps_match_the_oracle(gpgmp):
     nk = C.c_int64(0)
     o = oracle.orc()
     new_dt = []
+    left = 0
     for dr, dt in ((0, dtx0[0]), (1, dty0[0])):
-        n = o.orc_rep_ind_sweep(C.byref(d), oracle.ptr(o_state), R, seed, 0, dr, float(dt), step0 + dr,
-                                oracle.ptr(k), oracle.ptr(i), n, oracle.ptr(props), props.shape[1], oracle.ptr(fields),
-                                oracle.ptr(killed), C.byref(nk))
+        left += o.orc_rep_ind_sweep(C.byref(d), oracle.ptr(o_state), R, seed, 0, dr, float(dt), step0 + dr,
+                                    oracle.ptr(k), oracle.ptr(i), n, oracle.ptr(props), props.shape[1],
+                                    oracle.ptr(fields))
         dx = m.physical_length / (m.width if dr == 0 else m.height)
         off = (0 if dr == 0 else 1) * R * area
         roff = (2 if dr == 0 else 3) * R * area
         new_dt.append(o.orc_rep_timestep_cells(oracle.ptr(fields[off:]), oracle.ptr(fields[roff:]), R * area,
                                                float(np.float32(dx))))
+    # the list is sorted when read (once, after both sweeps)
+    n = o.orc_rep_ind_sort(oracle.ptr(k), oracle.ptr(i), n, R * area, oracle.ptr(killed), C.byref(nk))
+    assert nk.value == left > 0
     assert np.array_equal(g_state, o_state)
     assert np.array_equal(g_keys, k[:n]) and np.array_equal(g_ids, i[:n])
     assert len(g_keys) < len(keys)                      # some left through the absorbing wall (x+)
