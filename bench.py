@@ -116,13 +116,21 @@ def barrier(world):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The largest x over the ranks (the job's time is its slowest rank's)."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank: float, seconds: float, world: int) -> float:
+    """Whole-job throughput of independent replicas: every rank's units over the
+    slowest rank's time."""
+    return units_per_rank * world / max_over_ranks(seconds, world)
 
 
 def flush_l2(buf):
@@ -165,7 +173,7 @@ def bench_gray_scott(args, rank, world):
         barrier(world)
     per = [a.elapsed_time(b) / 1e3 for a, b in times]
     t_total = max_over_ranks(sum(per), world)
-    value = cell_steps * args.steps * world / t_total
+    value = cell_steps * args.steps * world / t_total      # replica_value with the reduced time
     t_launch = sum(per) / len(per)
     # ---- batched: the nine solves of the central finite-difference check (base and
     # +-h in F, k, Du, Dv), one 16-CTA cluster each in one launch, against the same
