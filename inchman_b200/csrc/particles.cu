@@ -10,16 +10,20 @@
 // a step is
 //   move:    x += vx dt + sqrt(2 D dt) z (Box-Muller normals from the particle's
 //            Philox stream), reflecting walls, key = floor(y) G + floor(x);
-//   bin:     stable radix sort of (key, index), count per cell, exclusive scan;
+//   bin:     stable radix sort of (key, index) (the move counts the digits), count
+//            per cell;
 //   react:   in each cell the k-th A (in sorted order) pairs with the k-th B and the
 //            pair is removed with probability p (one 32-bit draw per pair against
 //            floor(p 2^32));
-//   compact: survivors in sorted order (exclusive scan of the alive flags).
+//   compact: survivors in sorted order.
+// React and compact are one kernel over the cells that also scans the counts into
+// the cell starts.
 // Compiled with -fmad=false: positions must round as the CPU replay does.
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "lookback.cuh"
 #include "host_common.h"
 #include "sort_kernels.h"
 #include "../../include/gpgmp_c.h"
@@ -36,8 +40,14 @@ __device__ __forceinline__ float reflect_into(float x, float L) {
     return x;
 }
 
+// The move also counts the radix digits of the new keys for every sort pass (the
+// histogram the sort would otherwise read the keys again for).
 __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n, int G, float sig, float ax, float ay,
-                       uint32_t seed, uint32_t step, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                       uint32_t seed, uint32_t step, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                       uint32_t* __restrict__ hist, int passes) {
+    __shared__ uint32_t s_h[4][256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __syncthreads();
     const float L = (float)G;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         Stream st;
@@ -52,52 +62,223 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
         y = reflect_into(y, L);
         px[i] = x;
         py[i] = y;
-        keys[i] = (uint32_t)(int)y * (uint32_t)G + (uint32_t)(int)x;
+        const uint32_t k = (uint32_t)(int)y * (uint32_t)G + (uint32_t)(int)x;
+        keys[i] = k;
         vals[i] = (uint32_t)i;
+        for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xffu], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+        const uint32_t c = (&s_h[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
     }
 }
 
-__global__ void k_fill_u32(uint32_t* p, int64_t n, uint32_t v) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = v;
+// React and compact in one pass over the cells, with two decoupled look-back scans
+// (lookback.cuh).  A tile of 1024 cells (four per thread) takes its cells' starts
+// from the scan of the counts; its particles are then one contiguous range of the
+// sorted list, whose species bytes the block stages in shared memory.  Each thread
+// pairs the A's and B's of its cells there (the k-th A in sorted order with the k-th
+// B; a pair goes with probability thresh / 2^32, one 32-bit draw per pair from the
+// cell's stream), the tile takes its survivors' output offset from the scan of the
+// survivor counts, and each warp writes the survivors of its share of the range
+// (position and species) with ballot-ranked, coalesced stores: the order of
+// compacting the sorted list by alive flags.  The last tile writes the total.  A tile
+// with more particles than the staging holds walks each cell in global memory with
+// alive flags instead.
+constexpr int kRcThreads = 256;
+constexpr int kRcCells = 4;
+constexpr int kRcTile = kRcThreads * kRcCells;
+constexpr int kRcWarps = kRcThreads / 32;
+constexpr uint8_t kRcDead = 0xffu;
+
+// exclusive sum over the block (kRcThreads threads); *total = the block's sum
+__device__ __forceinline__ uint32_t block_excl_sum(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kRcWarps ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < kRcWarps) s_warp[lane] = w;
+    }
+    __syncthreads();
+    *total = s_warp[kRcWarps - 1];
+    return (warp == 0 ? 0u : s_warp[warp - 1]) + incl - v;
 }
 
-__global__ void k_react(const uint32_t* __restrict__ start, const uint32_t* __restrict__ count, int64_t ncells,
-                        const uint32_t* __restrict__ svals, const uint8_t* __restrict__ sp, uint32_t seed,
-                        uint32_t step, uint32_t thresh, uint32_t* __restrict__ alive) {
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells;
-         c += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t cnt = count[c];
-        if (cnt < 2) continue;
-        const uint32_t s0 = start[c], e = s0 + cnt;
-        Stream st;
-        st.init(seed, 1u, step, (uint32_t)c, PH_PAIR);
-        uint32_t ia = s0, ib = s0;
-        for (;;) {
-            while (ia < e && sp[svals[ia]] != 0) ia++;
-            while (ib < e && sp[svals[ib]] != 1) ib++;
-            if (ia >= e || ib >= e) break;
-            const uint32_t u = st.next();
-            if (u < thresh) {
+// Pairs one cell's A's and B's in order; dead pairs are marked in sp (kRcDead) or,
+// with alive != nullptr, cleared in alive.  Returns the number of pairs removed.
+template <class SP>
+__device__ __forceinline__ uint32_t pair_cell(uint32_t b, uint32_t f, const SP& species, uint32_t seed, uint32_t step,
+                                              uint32_t cell, uint32_t thresh, uint8_t* mark, uint32_t* alive) {
+    Stream st;
+    st.init(seed, 1u, step, cell, PH_PAIR);
+    uint32_t ia = b, ib = b, removed = 0;
+    for (;;) {
+        while (ia < f && species(ia) != 0) ia++;
+        while (ib < f && species(ib) != 1) ib++;
+        if (ia >= f || ib >= f) break;
+        if (st.next() < thresh) {
+            if (mark) {
+                mark[ia] = kRcDead;
+                mark[ib] = kRcDead;
+            } else {
                 alive[ia] = 0;
                 alive[ib] = 0;
             }
-            ia++;
-            ib++;
+            removed++;
         }
+        ia++;
+        ib++;
     }
+    return removed;
 }
 
-__global__ void k_gather(const uint32_t* __restrict__ alive, const uint32_t* __restrict__ pos,
-                         const uint32_t* __restrict__ svals, int64_t n, const float* __restrict__ x,
-                         const float* __restrict__ y, const uint8_t* __restrict__ sp, float* __restrict__ x2,
-                         float* __restrict__ y2, uint8_t* __restrict__ sp2) {
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-        if (!alive[j]) continue;
-        const uint32_t d = pos[j], s = svals[j];
-        x2[d] = x[s];
-        y2[d] = y[s];
-        sp2[d] = sp[s];
+// scratch (uint64 words): [0] tile counter (u32), error word (u32 at byte 8), total
+// (u32 at byte 16), then the status words of the two scans, ntiles each.
+// Dynamic shared memory: cap bytes (species of the staged particles).
+__global__ void __launch_bounds__(kRcThreads) k_react_compact(
+    const uint32_t* __restrict__ count, uint32_t* __restrict__ start, int64_t ncells,
+    const uint32_t* __restrict__ svals, const float* __restrict__ x, const float* __restrict__ y,
+    const uint8_t* __restrict__ sp, uint32_t seed, uint32_t step, uint32_t thresh, uint32_t* __restrict__ alive,
+    float* __restrict__ x2, float* __restrict__ y2, uint8_t* __restrict__ sp2, uint64_t* __restrict__ scratch,
+    uint32_t ntiles, uint32_t cap) {
+    extern __shared__ uint8_t s_sp[];          // [cap] species, kRcDead = removed
+    __shared__ uint32_t s_tile, s_prefix;
+    __shared__ uint32_t s_warp[kRcWarps];
+    __shared__ uint32_t s_wbase[kRcWarps];
+    unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
+    int* err = reinterpret_cast<int*>(scratch) + 2;
+    uint32_t* total = reinterpret_cast<uint32_t*>(scratch) + 4;
+    uint64_t* status_start = scratch + 4;
+    uint64_t* status_out = status_start + ntiles;
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t c0 = (int64_t)tile * kRcTile + (int64_t)threadIdx.x * kRcCells;
+    uint32_t cnt[kRcCells];
+    if (c0 + kRcCells <= ncells) {
+        const uint4 w = *reinterpret_cast<const uint4*>(count + c0);
+        cnt[0] = w.x; cnt[1] = w.y; cnt[2] = w.z; cnt[3] = w.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kRcCells; ++j) cnt[j] = c0 + j < ncells ? count[c0 + j] : 0u;
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kRcCells; ++j) sum += cnt[j];
+    uint32_t agg;
+    const uint32_t ex = block_excl_sum(sum, s_warp, &agg);
+    if (warp == 0) {
+        const uint32_t p = warp_lookback_u32(status_start, tile, agg, err);
+        if (lane == 0) s_prefix = p;
+    }
+    __syncthreads();
+    const uint32_t S = s_prefix;               // the tile's first particle in the sorted list
+    uint32_t o[kRcCells + 1];                  // the cells' offsets within the tile
+    o[0] = ex;
+#pragma unroll
+    for (int j = 0; j < kRcCells; ++j) o[j + 1] = o[j] + cnt[j];
+    if (c0 + kRcCells <= ncells) {
+        *reinterpret_cast<uint4*>(start + c0) = make_uint4(S + o[0], S + o[1], S + o[2], S + o[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kRcCells; ++j)
+            if (c0 + j < ncells) start[c0 + j] = S + o[j];
+    }
+    const bool staged = agg <= cap;            // the same in every thread of the block
+    uint32_t removed = 0;
+    if (staged) {
+        for (uint32_t p0 = 0; p0 < agg; p0 += 4 * kRcThreads) {
+            uint32_t src[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t p = p0 + u * kRcThreads + threadIdx.x;
+                src[u] = p < agg ? svals[S + p] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t p = p0 + u * kRcThreads + threadIdx.x;
+                if (p < agg) s_sp[p] = sp[src[u]];
+            }
+        }
+        __syncthreads();
+        const auto staged_sp = [&](uint32_t q) { return s_sp[q]; };
+#pragma unroll
+        for (int j = 0; j < kRcCells; ++j)
+            if (cnt[j] >= 2)
+                removed += pair_cell(o[j], o[j + 1], staged_sp, seed, step, (uint32_t)(c0 + j), thresh, s_sp, nullptr);
+    } else {
+        const auto global_sp = [&](uint32_t q) { return sp[svals[q]]; };
+        for (uint32_t q = S + o[0]; q < S + o[kRcCells]; ++q) alive[q] = 1u;
+#pragma unroll
+        for (int j = 0; j < kRcCells; ++j) {
+            if (cnt[j] >= 2) {
+                removed += pair_cell(S + o[j], S + o[j + 1], global_sp, seed, step, (uint32_t)(c0 + j), thresh,
+                                     nullptr, alive);
+            }
+        }
+    }
+    const uint32_t surv = sum - 2 * removed;
+    uint32_t agg2;
+    const uint32_t ex2 = block_excl_sum(surv, s_warp, &agg2);
+    if (warp == 0) {
+        const uint32_t p = warp_lookback_u32(status_out, tile, agg2, err);
+        if (lane == 0) {
+            s_prefix = p;
+            if (tile == ntiles - 1) *total = p + agg2;
+        }
+    }
+    __syncthreads();
+    if (staged) {
+        // warp w writes rows of 32 particles of its share [w0, w1) of the range
+        const uint32_t share = ((agg + kRcWarps * 32 - 1) / (kRcWarps * 32)) * 32;
+        const uint32_t w0 = min(agg, (uint32_t)warp * share), w1 = min(agg, w0 + share);
+        uint32_t mine = 0;
+        for (uint32_t r = w0; r < w1; r += 32) {
+            const uint32_t p = r + lane;
+            const bool live = p < w1 && s_sp[p] != kRcDead;
+            mine += __popc(__ballot_sync(0xffffffffu, live));
+        }
+        if (lane == 0) s_wbase[warp] = mine;
+        __syncthreads();
+        uint32_t d = s_prefix;
+        for (int w = 0; w < warp; ++w) d += s_wbase[w];
+        for (uint32_t r = w0; r < w1; r += 32) {
+            const uint32_t p = r + lane;
+            const bool live = p < w1 && s_sp[p] != kRcDead;
+            const unsigned m = __ballot_sync(0xffffffffu, live);
+            if (live) {
+                const uint32_t dd = d + __popc(m & ((1u << lane) - 1u));
+                const uint32_t src = svals[S + p];
+                x2[dd] = x[src];
+                y2[dd] = y[src];
+                sp2[dd] = s_sp[p];
+            }
+            d += __popc(m);
+        }
+    } else {
+        uint32_t d = s_prefix + ex2;
+        for (uint32_t q = S + o[0]; q < S + o[kRcCells]; ++q) {
+            if (removed && !alive[q]) continue;
+            const uint32_t src = svals[q];
+            x2[d] = x[src];
+            y2[d] = y[src];
+            sp2[d] = sp[src];
+            d++;
+        }
     }
 }
 
@@ -121,9 +302,11 @@ struct gpgmp_particles {
     float *x = nullptr, *y = nullptr, *x2 = nullptr, *y2 = nullptr;
     uint8_t *sp = nullptr, *sp2 = nullptr;
     uint32_t *keys = nullptr, *vals = nullptr, *skeys = nullptr, *svals = nullptr;
-    uint32_t *start = nullptr, *count = nullptr, *alive = nullptr, *pos = nullptr;
-    void *sort_scratch = nullptr, *scan_scratch = nullptr;
-    uint32_t* host_tail = nullptr;   // pinned: last scan value and last flag
+    uint32_t *start = nullptr, *count = nullptr, *alive = nullptr;
+    void* sort_scratch = nullptr;
+    uint64_t* rc_scratch = nullptr;  // react + compact: tile counter, error word, total, scan status words
+    uint32_t rc_tiles = 0;
+    uint32_t* host_tail = nullptr;   // pinned: the number of particles after a step
 };
 
 #define CK(expr)                                                                                              \
@@ -138,7 +321,7 @@ int gpgmp_particles_destroy(gpgmp_particles* h) {
     if (!h) return GPGMP_OK;
     cudaStreamSynchronize(h->stream);
     void* ptrs[] = {h->x, h->y, h->x2, h->y2, h->sp, h->sp2, h->keys, h->vals, h->skeys, h->svals, h->start,
-                    h->count, h->alive, h->pos, h->sort_scratch, h->scan_scratch};
+                    h->count, h->alive, h->sort_scratch, h->rc_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->host_tail) cudaFreeHost(h->host_tail);
@@ -169,11 +352,11 @@ int gpgmp_particles_create(int64_t capacity, int32_t grid, float D, float vx, fl
     A((void**)&h->x2, sizeof(float) * capacity); A((void**)&h->y2, sizeof(float) * capacity);
     A((void**)&h->sp, capacity); A((void**)&h->sp2, capacity);
     A((void**)&h->keys, n4); A((void**)&h->vals, n4); A((void**)&h->skeys, n4); A((void**)&h->svals, n4);
-    A((void**)&h->alive, n4); A((void**)&h->pos, n4);
+    A((void**)&h->alive, n4);
     A((void**)&h->start, sizeof(uint32_t) * (size_t)ncells); A((void**)&h->count, sizeof(uint32_t) * (size_t)ncells);
     A(&h->sort_scratch, sort_layout(capacity, bits).bytes);
-    const int64_t scan_n = capacity > ncells ? capacity : ncells;
-    A(&h->scan_scratch, scan_scratch_bytes(scan_n));
+    h->rc_tiles = (uint32_t)((ncells + kRcTile - 1) / kRcTile);
+    A((void**)&h->rc_scratch, sizeof(uint64_t) * (4 + 2 * (size_t)h->rc_tiles));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host_tail, 2 * sizeof(uint32_t));
     if (e != cudaSuccess) {
         int c = set_error(e == cudaErrorMemoryAllocation ? GPGMP_ERR_NOMEM : GPGMP_ERR_CUDA, "allocation: %s",
@@ -222,24 +405,30 @@ static int particles_step_one(gpgmp_particles* h) {
     const float ax = h->vx * h->dt, ay = h->vy * h->dt;
     const uint32_t step = (uint32_t)h->step;
     if (n > 0) {
-        k_move<<<grid_of(n, 256), 256, 0, st>>>(h->x, h->y, n, h->grid, sig, ax, ay, h->seed, step, h->keys, h->vals);
+        CK(radix_sort_begin(n, h->key_bits, h->sort_scratch, st));
+        const int passes = sort_layout(n, h->key_bits).passes;
+        k_move<<<grid_of(n, 256 * 8), 256, 0, st>>>(h->x, h->y, n, h->grid, sig, ax, ay, h->seed, step, h->keys,
+                                                     h->vals, radix_sort_hist(n, h->key_bits, h->sort_scratch),
+                                                     passes);
         CK(cudaGetLastError());
-        CK(radix_sort_pairs_u32(h->keys, h->vals, h->skeys, h->svals, n, h->key_bits, h->sort_scratch, st));
+        CK(radix_sort_finish(h->keys, h->vals, h->skeys, h->svals, n, h->key_bits, h->sort_scratch, st));
     }
-    CK(cell_offsets_u32(h->skeys, n, ncells, h->start, h->count, h->scan_scratch, st));
-    if (n > 0) {
-        k_fill_u32<<<grid_of(n, 256), 256, 0, st>>>(h->alive, n, 1u);
-        k_react<<<grid_of(ncells, 128), 128, 0, st>>>(h->start, h->count, ncells, h->svals, h->sp, h->seed, step,
-                                                       h->thresh, h->alive);
-        CK(cudaGetLastError());
-        CK(scan_exclusive_u32(h->alive, h->pos, n, h->scan_scratch, st));
-        k_gather<<<grid_of(n, 256), 256, 0, st>>>(h->alive, h->pos, h->svals, n, h->x, h->y, h->sp, h->x2, h->y2,
-                                                   h->sp2);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(&h->host_tail[0], h->pos + n - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&h->host_tail[1], h->alive + n - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        h->n = (int64_t)h->host_tail[0] + h->host_tail[1];
+    CK(cell_counts_u32(h->skeys, n, ncells, h->count, st));
+    CK(cudaMemsetAsync(h->rc_scratch, 0, sizeof(uint64_t) * (4 + 2 * (size_t)h->rc_tiles), st));
+    // staging for twice the mean number of particles per tile (+ 1024), up to 47 KB
+    // (with the static shared memory, within the 48 KB a launch gets without opting in)
+    uint64_t want = (uint64_t)(2.0 * (double)n * kRcTile / (double)ncells) + 1024;
+    if (want > 47 * 1024) want = 47 * 1024;
+    const uint32_t cap = (uint32_t)want;
+    k_react_compact<<<h->rc_tiles, kRcThreads, cap, st>>>(
+        h->count, h->start, ncells, h->svals, h->x, h->y, h->sp, h->seed, step, h->thresh, h->alive, h->x2, h->y2,
+        h->sp2, h->rc_scratch, h->rc_tiles, cap);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&h->host_tail[0], reinterpret_cast<uint32_t*>(h->rc_scratch) + 4, sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h->n = (int64_t)h->host_tail[0];
+    {
         float* t;
         t = h->x; h->x = h->x2; h->x2 = t;
         t = h->y; h->y = h->y2; h->y2 = t;
@@ -280,7 +469,7 @@ int gpgmp_particles_status(gpgmp_particles* h, int32_t* status) {
     const SortLayout L = sort_layout(h->cap, h->key_bits);
     int a = 0, b = 0;
     CK(cudaMemcpy(&a, (const char*)h->sort_scratch + L.off_counters + 16, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&b, (const char*)h->scan_scratch + scan_error_flag_offset(), sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&b, (const char*)h->rc_scratch + 8, sizeof(int), cudaMemcpyDeviceToHost));
     *status = (a || b) ? GPGMP_ERR_TIMEOUT : GPGMP_OK;
     return GPGMP_OK;
 }

@@ -312,11 +312,23 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     }
 }
 
+// Counts per cell.  Equal neighbours within a warp are added as one run (the keys come
+// sorted, so a warp holds a few runs): the last lane of each run adds its length.
 __global__ void k_histogram_cells(const uint32_t* __restrict__ keys, int64_t n, uint32_t ncells,
                                   uint32_t* __restrict__ count) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        if (k < ncells) atomicAdd(&count[k], 1u);
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+        const int64_t i = base + lane;
+        const uint32_t k = i < n ? keys[i] : 0xffffffffu;   // past the end: no cell
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, k, 1);
+        const uint32_t next = __shfl_down_sync(0xffffffffu, k, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || k != prev);
+        const bool last = lane == 31 || k != next;
+        if (last && k < ncells) {
+            const int first = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+            atomicAdd(&count[k], (uint32_t)(lane - first + 1));
+        }
     }
 }
 
@@ -373,8 +385,20 @@ SortLayout sort_layout(int64_t n, int key_bits) {
     return L;
 }
 
-cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
-                                 int key_bits, void* scratch, cudaStream_t st) {
+cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const SortLayout L = sort_layout(n, key_bits);
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortStagingBytes);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(scratch, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
+}
+
+uint32_t* radix_sort_hist(int64_t n, int key_bits, void* scratch) {
+    return (uint32_t*)((char*)scratch + sort_layout(n, key_bits).off_hist);
+}
+
+cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
+                              int key_bits, void* scratch, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const SortLayout L = sort_layout(n, key_bits);
     char* base = (char*)scratch;
@@ -383,25 +407,18 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     uint32_t* look = (uint32_t*)(base + L.off_look);
     uint32_t* ak = (uint32_t*)(base + L.off_alt_keys);
     uint32_t* av = (uint32_t*)(base + L.off_alt_vals);
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortStagingBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(base, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
-    if (e != cudaSuccess) return e;
-    k_radix_histogram<<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
     k_radix_bin_offsets<<<L.passes, 256, 0, st>>>(hist);
     // ping-pong so that the last pass lands in (kout, vout)
     const uint32_t* sk = kin;
     const uint32_t* sv = vin;
     for (int p = 0; p < L.passes; ++p) {
-        const bool last = p == L.passes - 1;
         const bool to_out = ((L.passes - 1 - p) % 2) == 0;
         uint32_t* dk = to_out ? kout : ak;
         uint32_t* dv = to_out ? vout : av;
-        (void)last;
         k_onesweep<<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(sk, sv, dk, dv, n, 8 * p, hist + 256 * p,
                                                                look + (size_t)256 * L.tiles * p, counters + p,
                                                                (int*)(counters + 4));
-        e = cudaGetLastError();
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         sk = dk;
         sv = dv;
@@ -409,12 +426,28 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     return cudaSuccess;
 }
 
-cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
-                             void* scan_scratch, cudaStream_t st) {
+cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
+                                 int key_bits, void* scratch, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e = radix_sort_begin(n, key_bits, scratch, st);
+    if (e != cudaSuccess) return e;
+    k_radix_histogram<<<grid_cap(n, 256), 256, 0, st>>>(kin, n, sort_layout(n, key_bits).passes,
+                                                         radix_sort_hist(n, key_bits, scratch));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return radix_sort_finish(kin, vin, kout, vout, n, key_bits, scratch, st);
+}
+
+cudaError_t cell_counts_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* count, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * (size_t)ncells, st);
     if (e != cudaSuccess) return e;
     if (n > 0) k_histogram_cells<<<grid_cap(n, 256), 256, 0, st>>>(sorted_keys, n, (uint32_t)ncells, count);
-    e = cudaGetLastError();
+    return cudaGetLastError();
+}
+
+cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
+                             void* scan_scratch, cudaStream_t st) {
+    cudaError_t e = cell_counts_u32(sorted_keys, n, ncells, count, st);
     if (e != cudaSuccess) return e;
     return scan_exclusive_u32(count, start, ncells, scan_scratch, st);
 }

@@ -21,8 +21,17 @@ struct SortLayout {
 SortLayout sort_layout(int64_t n, int key_bits);
 cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
                                  int key_bits, void* scratch, cudaStream_t st);
+// The same in two halves around a caller's kernel that adds the digit counts of every
+// pass ([passes][256], radix_sort_hist) while it writes the keys: begin clears the
+// scratch, finish sorts.
+cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_t st);
+uint32_t* radix_sort_hist(int64_t n, int key_bits, void* scratch);
+cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
+                              int key_bits, void* scratch, cudaStream_t st);
 
-// count[c] = number of keys equal to c, start = exclusive scan of count
+// count[c] = number of keys equal to c (keys at or past ncells are not counted)
+cudaError_t cell_counts_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* count, cudaStream_t st);
+// count as above, start = exclusive scan of count
 cudaError_t cell_offsets_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* start, uint32_t* count,
                              void* scan_scratch, cudaStream_t st);
 // the reference's [left, right] cell indices from start and count

@@ -98,7 +98,9 @@ int64_t orc_particles_run(int64_t n, float* px, float* py, uint8_t* sp, int G, f
     const float sig = sqrtf(2.0f * D * dt);
     const float ax = vx * dt, ay = vy * dt;
     const int64_t ncells = (int64_t)G * G;
-    const uint32_t thresh = (uint32_t)floor((double)p_react * 4294967296.0);
+    /* floor(p 2^32), held to 2^32 - 1 for p = 1 (the largest 32-bit threshold) */
+    const double tp = floor((double)p_react * 4294967296.0);
+    const uint32_t thresh = tp < 4294967295.0 ? (uint32_t)tp : 4294967295u;
     uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     uint32_t* vals = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     uint32_t* start = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)ncells);

@@ -99,3 +99,54 @@ def test_particle_steps_bit_exact(gpgmp, n, grid, steps):
     # removals come in A/B pairs
     assert (np.sum(gsp == 0) - np.sum(gsp == 1)) == (np.sum(sp == 0) - np.sum(sp == 1))
     assert m < n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p_react", [0.05, 1.0])
+def test_particle_steps_clustered_bit_exact(gpgmp, p_react):
+    """Particles packed into 8 x 8 cells of a 128 x 128 grid: hundreds per cell, and
+    more in one tile of cells than its shared-memory staging holds (the kernel then
+    pairs and compacts those cells in global memory)."""
+    from inchman_b200 import individual as ind
+    n, grid, steps = 30_000, 128, 3
+    rng = np.random.default_rng(17)
+    x = rng.uniform(60.0, 68.0, n).astype(np.float32)
+    y = rng.uniform(60.0, 68.0, n).astype(np.float32)
+    sp = rng.integers(0, 2, n).astype(np.uint8)
+    p = ind.Particles(n, grid, D=0.05, vx=0.0, vy=0.0, dt=1.0, p_react=p_react, seed=99)
+    p.set(x, y, sp, step=0)
+    p.step(steps)
+    gx, gy, gsp = p.get()
+    assert p.status() == 0
+    ox, oy, osp = x.copy(), y.copy(), sp.copy()
+    m = oracle.orc().orc_particles_run(n, oracle.ptr(ox), oracle.ptr(oy), oracle.ptr(osp), grid, 0.05, 0.0, 0.0, 1.0,
+                                       p_react, 99, 0, steps)
+    assert len(gx) == m and m < n
+    assert np.array_equal(gx, ox[:m]) and np.array_equal(gy, oy[:m]) and np.array_equal(gsp, osp[:m])
+
+
+@pytest.mark.parametrize("clustered", [False, True])
+def test_particle_bins_follow_the_step(gpgmp, clustered):
+    """Without reactions a step keeps every particle, in cell order: the bins of the
+    step (start, count, sorted keys) are those of the positions it returns."""
+    from inchman_b200 import individual as ind
+    n, grid = 50_000, 128
+    if clustered:
+        rng = np.random.default_rng(3)
+        x = rng.uniform(30.0, 34.0, n).astype(np.float32)
+        y = rng.uniform(90.0, 92.0, n).astype(np.float32)
+        sp = rng.integers(0, 2, n).astype(np.uint8)
+    else:
+        x, y, sp = ind.uniform_particles(n, grid, seed=8)
+    p = ind.Particles(n, grid, D=0.3, vx=0.2, vy=-0.1, dt=1.0, p_react=0.0, seed=4)
+    p.set(x, y, sp, step=0)
+    p.step(1)
+    gx, gy, gsp = p.get()
+    start, count, keys, idx = p.bins()
+    cells = gy.astype(np.int64) * grid + gx.astype(np.int64)
+    assert len(gx) == n and np.all(np.diff(cells) >= 0)
+    want = np.bincount(cells, minlength=grid * grid)
+    assert np.array_equal(count, want)
+    assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
+    assert np.array_equal(keys, cells.astype(np.uint32))
+    assert np.array_equal(np.sort(idx), np.arange(n, dtype=np.uint32))
