@@ -33,9 +33,15 @@ __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
+constexpr int kLookDepth = 4;   // status words per lane per round: 128 tiles
+
 // Called by all 32 lanes of one warp.  Publishes tile's aggregate, looks back over
-// the preceding tiles 32 at a time, publishes the inclusive prefix and returns the
-// exclusive prefix (in every lane).  err is set when a wait exceeds kSpinLimit.
+// the preceding tiles 128 at a time (lane l, slot u reads the tile 32 u + l + 1
+// before the window's start, so the nearest tiles come first), publishes the
+// inclusive prefix and returns the exclusive prefix (in every lane).  Only the tiles
+// up to the nearest one with an inclusive prefix need to have published; the loads
+// of a round are independent, so a tile far from any inclusive prefix sums 128
+// aggregates per memory round trip.  err is set when a wait exceeds kSpinLimit.
 __device__ __forceinline__ uint32_t warp_lookback_u32(uint64_t* status, uint32_t tile, uint32_t aggregate, int* err) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
@@ -46,26 +52,44 @@ __device__ __forceinline__ uint32_t warp_lookback_u32(uint64_t* status, uint32_t
     int64_t look = (int64_t)tile - 1;
     uint32_t exclusive = 0, spins = 0;
     while (true) {
-        const int64_t idx = look - lane;
-        const uint64_t w = idx >= 0 ? ld_volatile_u64(&status[idx]) : kScanFlagP;
-        const uint32_t flag = (uint32_t)(w >> 32);
-        // wait until every lane of the window has at least an aggregate
-        if (__any_sync(0xffffffffu, flag == 0)) {
+        uint64_t w[kLookDepth];
+#pragma unroll
+        for (int u = 0; u < kLookDepth; ++u) {
+            const int64_t idx = look - lane - 32 * u;
+            w[u] = idx >= 0 ? ld_volatile_u64(&status[idx]) : kScanFlagP;   // before tile 0: prefix 0
+        }
+        // the nearest inclusive prefix of the round: slot pu, lane pl
+        int pu = kLookDepth, pl = 31;
+#pragma unroll
+        for (int u = kLookDepth - 1; u >= 0; --u) {
+            const unsigned m = __ballot_sync(0xffffffffu, (uint32_t)(w[u] >> 32) == 2u);
+            if (m) {
+                pu = u;
+                pl = __ffs(m) - 1;
+            }
+        }
+        // the tiles that count: every slot before pu, slot pu up to lane pl
+        bool missing = false;
+        uint32_t val = 0;
+#pragma unroll
+        for (int u = 0; u < kLookDepth; ++u) {
+            if (u < pu || (u == pu && lane <= pl)) {
+                missing |= (uint32_t)(w[u] >> 32) == 0u;
+                val += (uint32_t)w[u];
+            }
+        }
+        if (__any_sync(0xffffffffu, missing)) {
             if (++spins > kSpinLimit) {
                 if (lane == 0) atomicExch(err, 1);
                 break;
             }
             continue;
         }
-        const unsigned pmask = __ballot_sync(0xffffffffu, flag == 2);
-        // lanes up to and including the first inclusive prefix contribute
-        const int first_p = pmask ? __ffs(pmask) - 1 : 32;
-        uint32_t val = lane <= first_p ? (uint32_t)w : 0u;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
         exclusive += val;
-        if (pmask) break;
-        look -= 32;
+        if (pu < kLookDepth) break;
+        look -= 32 * kLookDepth;
     }
     if (lane == 0) st_release_u64(&status[tile], kScanFlagP | (uint32_t)(exclusive + aggregate));
     return exclusive;

@@ -49,23 +49,43 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
     for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
     __syncthreads();
     const float L = (float)G;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        Stream st;
-        st.init(seed, 0u, step, (uint32_t)i, PH_PART);
-        float z0, z1;
-        normal2(st, &z0, &z1);
-        float x = px[i] + ax;
-        x = x + sig * z0;
-        float y = py[i] + ay;
-        y = y + sig * z1;
-        x = reflect_into(x, L);
-        y = reflect_into(y, L);
-        px[i] = x;
-        py[i] = y;
-        const uint32_t k = (uint32_t)(int)y * (uint32_t)G + (uint32_t)(int)x;
-        keys[i] = k;
-        vals[i] = (uint32_t)i;
-        for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xffu], 1u);
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // whole warps step together (the digit counts below are warp-collective)
+    for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+        const int64_t i = base + lane;
+        const bool valid = i < n;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        uint32_t k = 0;
+        if (valid) {
+            Stream st;
+            st.init(seed, 0u, step, (uint32_t)i, PH_PART);
+            float z0, z1;
+            normal2(st, &z0, &z1);
+            float x = px[i] + ax;
+            x = x + sig * z0;
+            float y = py[i] + ay;
+            y = y + sig * z1;
+            x = reflect_into(x, L);
+            y = reflect_into(y, L);
+            px[i] = x;
+            py[i] = y;
+            k = (uint32_t)(int)y * (uint32_t)G + (uint32_t)(int)x;
+            keys[i] = k;
+            vals[i] = (uint32_t)i;
+        }
+        // The particles come in the last step's cell order, so a warp's upper digits
+        // are mostly all the same: one add for the warp then, one per lane otherwise.
+        const int lead = __ffs(vmask) - 1;
+        for (int p = 0; p < passes; ++p) {
+            const uint32_t d = (k >> (8 * p)) & 0xffu;
+            const uint32_t d0 = __shfl_sync(0xffffffffu, d, lead);
+            if (__all_sync(0xffffffffu, !valid || d == d0)) {
+                if (lane == lead) atomicAdd(&s_h[p][d0], (uint32_t)__popc(vmask));
+            } else if (valid) {
+                atomicAdd(&s_h[p][d], 1u);
+            }
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {

@@ -122,7 +122,7 @@ static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "one thread per dig
 constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
 constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
-constexpr int kLookWindow = 8;   // predecessor tiles read per look-back step
+constexpr int kLookWindow = 4;   // predecessor tiles read per look-back step
 
 // one pass over the keys counts every digit position: hist[pass][256]
 __global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n, int passes,
