@@ -44,9 +44,11 @@ __device__ __forceinline__ float reflect_into(float x, float L) {
 // histogram the sort would otherwise read the keys again for).
 __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n, int G, float sig, float ax, float ay,
                        uint32_t seed, uint32_t step, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                       uint32_t* __restrict__ hist, int passes) {
-    __shared__ uint32_t s_h[4][256];
-    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+                       uint32_t* __restrict__ hist, int passes, int rb) {
+    __shared__ uint32_t s_h[3 * 1024];   // [passes][1 << rb]: 4 x 256 or up to 3 x 1024
+    const int dig = 1 << rb;
+    const uint32_t dmask = (uint32_t)dig - 1u;
+    for (int i = threadIdx.x; i < passes * dig; i += blockDim.x) s_h[i] = 0;
     __syncthreads();
     const float L = (float)G;
     const int lane = threadIdx.x & 31;
@@ -78,18 +80,18 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
         // are mostly all the same: one add for the warp then, one per lane otherwise.
         const int lead = __ffs(vmask) - 1;
         for (int p = 0; p < passes; ++p) {
-            const uint32_t d = (k >> (8 * p)) & 0xffu;
+            const uint32_t d = (k >> (rb * p)) & dmask;
             const uint32_t d0 = __shfl_sync(0xffffffffu, d, lead);
             if (__all_sync(0xffffffffu, !valid || d == d0)) {
-                if (lane == lead) atomicAdd(&s_h[p][d0], (uint32_t)__popc(vmask));
+                if (lane == lead) atomicAdd(&s_h[p * dig + d0], (uint32_t)__popc(vmask));
             } else if (valid) {
-                atomicAdd(&s_h[p][d], 1u);
+                atomicAdd(&s_h[p * dig + d], 1u);
             }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
-        const uint32_t c = (&s_h[0][0])[i];
+    for (int i = threadIdx.x; i < passes * dig; i += blockDim.x) {
+        const uint32_t c = s_h[i];
         if (c) atomicAdd(&hist[i], c);
     }
 }
@@ -426,10 +428,10 @@ static int particles_step_one(gpgmp_particles* h) {
     const uint32_t step = (uint32_t)h->step;
     if (n > 0) {
         CK(radix_sort_begin(n, h->key_bits, h->sort_scratch, st));
-        const int passes = sort_layout(n, h->key_bits).passes;
+        const SortLayout L = sort_layout(n, h->key_bits);
         k_move<<<grid_of(n, 256 * 8), 256, 0, st>>>(h->x, h->y, n, h->grid, sig, ax, ay, h->seed, step, h->keys,
                                                      h->vals, radix_sort_hist(n, h->key_bits, h->sort_scratch),
-                                                     passes);
+                                                     L.passes, L.digit_bits);
         CK(cudaGetLastError());
         CK(radix_sort_finish(h->keys, h->vals, h->skeys, h->svals, n, h->key_bits, h->sort_scratch, st));
     }

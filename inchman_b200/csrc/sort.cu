@@ -10,9 +10,10 @@
 // Here, from the published methods (not from the reference's SDK-derived code):
 //  - exclusive scan: single pass with decoupled look-back (Merrill & Garland 2016);
 //  - radix sort: onesweep (Adinets & Merrill 2022): one histogram kernel for every
-//    digit position, then one kernel per 8-bit digit that ranks its tile (warp
-//    match_any), publishes per-digit tile counts, looks back for the prefix and
-//    scatters through shared memory; stable;
+//    digit position, then one kernel per digit (8 bits, or 10 where that saves a
+//    pass: 17-20 and 25-30 key bits) that ranks its tile (peer masks from ballots),
+//    publishes per-digit tile counts, looks back for the prefix and scatters through
+//    shared memory; stable;
 //  - cell offsets: key histogram + exclusive scan (start), count; the reference's
 //    left/right indices follow from them.
 // Every look-back spin has an iteration limit; exceeding it sets the error word
@@ -117,37 +118,52 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
 constexpr int kSortThreads = 512;
 constexpr int kSortItems = 15;
 constexpr int kSortTile = kSortThreads * kSortItems;   // 7680: fewer tiles, a shorter look-back chain
-constexpr int kDigitWarps = 256 / 32;                  // threads 0-255 own one digit each in the digit phases
-static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "one thread per digit");
+static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "a thread per digit (8-bit digits)");
 constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
 constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
 constexpr int kLookWindow = 4;   // predecessor tiles read per look-back step
+constexpr int kHistWords = 3 * 1024;   // digit counts of every pass: 4 x 256 or up to 3 x 1024
 
-// one pass over the keys counts every digit position: hist[pass][256]
+// Digits of RB bits: DIG values, owned kDPT at a time by the first kDigitThreads threads
+// in the digit phases (8 bits: threads 0-255, one each; 10 bits: all 512, two each).
+template <int RB>
+struct Radix {
+    static constexpr int DIG = 1 << RB;
+    static constexpr uint32_t MASK = (uint32_t)DIG - 1u;
+    static constexpr int kDigitThreads = DIG < kSortThreads ? DIG : kSortThreads;
+    static constexpr int kDPT = DIG / kDigitThreads;
+    static constexpr int kDigitWarps = kDigitThreads / 32;
+};
+
+// one pass over the keys counts every digit position: hist[pass][DIG]
+template <int RB>
 __global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n, int passes,
                                                          uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s_h[4][256];
-    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    using R = Radix<RB>;
+    __shared__ uint32_t s_h[kHistWords];
+    for (int i = threadIdx.x; i < passes * R::DIG; i += blockDim.x) s_h[i] = 0;
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t k = keys[i];
-        for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xffu], 1u);
+        for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p * R::DIG + ((k >> (RB * p)) & R::MASK)], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
-        const uint32_t c = (&s_h[0][0])[i];
+    for (int i = threadIdx.x; i < passes * R::DIG; i += blockDim.x) {
+        const uint32_t c = s_h[i];
         if (c) atomicAdd(&hist[i], c);
     }
 }
 
-// exclusive scan of each pass's 256 bins (one block per pass)
+// exclusive scan of each pass's DIG bins (one block of DIG threads per pass)
+template <int RB>
 __global__ void k_radix_bin_offsets(uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s[256];
-    uint32_t* h = hist + blockIdx.x * 256;
+    using R = Radix<RB>;
+    __shared__ uint32_t s[R::DIG];
+    uint32_t* h = hist + blockIdx.x * R::DIG;
     s[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
-    for (int o = 1; o < 256; o <<= 1) {
+    for (int o = 1; o < R::DIG; o <<= 1) {
         uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
         __syncthreads();
         s[threadIdx.x] += t;
@@ -159,24 +175,32 @@ __global__ void k_radix_bin_offsets(uint32_t* __restrict__ hist) {
 // One onesweep pass.  Warp w of a tile owns keys [w*32*IT, (w+1)*32*IT) of the tile
 // in a warp-striped layout (item j of lane l is key j*32 + l), so processing items in
 // order and lanes in order is index order: the ranks are stable.
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin,
                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            int64_t n, int shift, const uint32_t* __restrict__ bins,
                                                            uint32_t* __restrict__ look, unsigned int* tile_counter,
                                                            int* err) {
-    __shared__ uint32_t s_warp_hist[kWarps][256];
-    __shared__ uint32_t s_count[256];        // the tile's count of each digit
-    __shared__ uint32_t s_tile_off[256];     // exclusive offset of each digit inside the tile
-    __shared__ uint32_t s_global[256];       // global start of each digit's run of this tile
+    using R = Radix<RB>;
+    constexpr int DIG = R::DIG;
+    constexpr int DPT = R::kDPT;
+    // per warp and digit: the warp's count, then its offset among the tile's warps
+    // (at most 7680, so 16 bits)
+    __shared__ uint16_t s_warp_hist[kWarps][DIG];
+    __shared__ uint32_t s_count[DIG];        // the tile's count of each digit
+    __shared__ uint32_t s_tile_off[DIG];     // exclusive offset of each digit inside the tile
+    __shared__ uint32_t s_global[DIG];       // global start of each digit's run of this tile
+    __shared__ uint32_t s_w[R::kDigitWarps];
     extern __shared__ uint32_t s_staging[];  // keys then values in tile-sorted order (dynamic: 60 KB)
     uint32_t* s_keys = s_staging;
     uint32_t* s_vals = s_staging + kSortTile;
     __shared__ uint32_t s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    for (int i = threadIdx.x; i < kWarps * 256; i += kSortThreads) (&s_warp_hist[0][0])[i] = 0;
-    if (threadIdx.x < 256) s_count[threadIdx.x] = 0;
+    for (int i = threadIdx.x; i < kWarps * DIG / 2; i += kSortThreads)
+        reinterpret_cast<uint32_t*>(&s_warp_hist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < DIG; i += kSortThreads) s_count[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const int64_t tbase = (int64_t)tile * kSortTile;
@@ -192,23 +216,28 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     // before the ranking so that the look-back of later tiles can start early
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j)
-        if (wbase + j * 32 + lane < n) atomicAdd(&s_count[(key[j] >> shift) & 0xffu], 1u);
+        if (wbase + j * 32 + lane < n) atomicAdd(&s_count[(key[j] >> shift) & R::MASK], 1u);
     __syncthreads();
-    const int d = threadIdx.x;   // the digit of threads 0-255
-    const bool digit_thread = d < 256;
-    const uint32_t tile_count = digit_thread ? s_count[d] : 0u;
-    uint32_t* lk = look + (size_t)tile * 256;
-    if (digit_thread) st_release_u32(&lk[d], (tile == 0 ? kFlagP : kFlagA) | tile_count);
-    // warp-level ranking (stable): the lanes holding the same digit, from eight ballots
+    // digit thread t owns digits t*DPT .. t*DPT + DPT - 1
+    const bool digit_thread = threadIdx.x < R::kDigitThreads;
+    const int d0 = threadIdx.x * DPT;
+    uint32_t tile_count[DPT];
+    uint32_t* lk = look + (size_t)tile * DIG;
+#pragma unroll
+    for (int q = 0; q < DPT; ++q) {
+        tile_count[q] = digit_thread ? s_count[d0 + q] : 0u;
+        if (digit_thread) st_release_u32(&lk[d0 + q], (tile == 0 ? kFlagP : kFlagA) | tile_count[q]);
+    }
+    // warp-level ranking (stable): the lanes holding the same digit, from RB ballots
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t idx = wbase + j * 32 + lane;
         const bool ok = idx < n;
-        const uint32_t dj = (key[j] >> shift) & 0xffu;
+        const uint32_t dj = (key[j] >> shift) & R::MASK;
         unsigned peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
+        for (int b = 0; b < RB; ++b) {
             const unsigned bal = __ballot_sync(0xffffffffu, (dj >> b) & 1u);
             peers &= ((dj >> b) & 1u) ? bal : ~bal;
         }
@@ -218,7 +247,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
         uint32_t prior = 0;
         if (ok && lane == leader) {
             prior = s_warp_hist[warp][dj];
-            s_warp_hist[warp][dj] = prior + __popc(peers);
+            s_warp_hist[warp][dj] = (uint16_t)(prior + __popc(peers));
         }
         prior = __shfl_sync(0xffffffffu, prior, leader);
         rank[j] = prior + __popc(peers & lt);
@@ -227,30 +256,45 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     __syncthreads();
     // per digit: counts over warps -> warp offsets (in place)
     if (digit_thread) {
-        uint32_t run = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t c = s_warp_hist[w][d];
-            s_warp_hist[w][d] = run;
-            run += c;
+        for (int q = 0; q < DPT; ++q) {
+            uint32_t run = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                const uint32_t c = s_warp_hist[w][d0 + q];
+                s_warp_hist[w][d0 + q] = (uint16_t)run;
+                run += c;
+            }
         }
     }
-    // look back for the prefix of this digit
-    uint32_t excl = 0;
+    // look back for the prefix of each owned digit: kLookWindow tiles at a time (the
+    // loads of all owned digits in flight together), summing the counts up to and
+    // including the nearest inclusive prefix
+    uint32_t excl[DPT];
+#pragma unroll
+    for (int q = 0; q < DPT; ++q) excl[q] = 0;
     if (digit_thread && tile > 0) {
-        // look back kLookWindow tiles at a time (their loads in flight together): sum
-        // the counts up to and including the nearest inclusive prefix
+        bool done[DPT];
+#pragma unroll
+        for (int q = 0; q < DPT; ++q) done[q] = false;
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
-        bool done = false;
-        while (!done) {
-            uint32_t w[kLookWindow];
+        while (true) {
+            bool all_done = true;
 #pragma unroll
-            for (int j = 0; j < kLookWindow; ++j)
-                w[j] = t - j >= 0 ? ld_acquire_u32(&look[(size_t)(t - j) * 256 + d]) : kFlagP;
+            for (int q = 0; q < DPT; ++q) all_done = all_done && done[q];
+            if (all_done) break;
+            uint32_t w[DPT][kLookWindow];
+#pragma unroll
+            for (int q = 0; q < DPT; ++q)
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j)
+                    w[q][j] = (!done[q] && t - j >= 0) ? ld_acquire_u32(&look[(size_t)(t - j) * DIG + d0 + q]) : kFlagP;
             bool ready = true;
 #pragma unroll
-            for (int j = 0; j < kLookWindow; ++j) ready = ready && (w[j] & ~kValMask) != 0;
+            for (int q = 0; q < DPT; ++q)
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j) ready = ready && (w[q][j] & ~kValMask) != 0;
             if (!ready) {
                 if (++spins > kSpinLimit) {
                     atomicExch(err, 1);
@@ -259,20 +303,26 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
                 continue;
             }
 #pragma unroll
-            for (int j = 0; j < kLookWindow; ++j) {
-                if (!done) {
-                    excl += w[j] & kValMask;
-                    done = (w[j] & ~kValMask) == kFlagP;
+            for (int q = 0; q < DPT; ++q) {
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j) {
+                    if (!done[q]) {
+                        excl[q] += w[q][j] & kValMask;
+                        done[q] = (w[q][j] & ~kValMask) == kFlagP;
+                    }
                 }
             }
             t -= kLookWindow;
         }
-        st_release_u32(&lk[d], kFlagP | ((excl + tile_count) & kValMask));
+#pragma unroll
+        for (int q = 0; q < DPT; ++q) st_release_u32(&lk[d0 + q], kFlagP | ((excl[q] + tile_count[q]) & kValMask));
     }
-    // tile-local digit offsets (exclusive scan of tile_count over digits)
+    // tile-local digit offsets (exclusive scan of the tile counts over the digits)
     {
-        __shared__ uint32_t s_w[kDigitWarps];
-        uint32_t incl = tile_count;
+        uint32_t mine = 0;
+#pragma unroll
+        for (int q = 0; q < DPT; ++q) mine += tile_count[q];
+        uint32_t incl = mine;
         if (digit_thread) {
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -283,10 +333,14 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
         }
         __syncthreads();
         if (digit_thread) {
-            uint32_t wo = 0;
-            for (int w = 0; w < warp; ++w) wo += s_w[w];
-            s_tile_off[d] = wo + incl - tile_count;
-            s_global[d] = bins[d] + excl;
+            uint32_t off = incl - mine;
+            for (int w = 0; w < warp; ++w) off += s_w[w];
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                s_tile_off[d0 + q] = off;
+                s_global[d0 + q] = bins[d0 + q] + excl[q];
+                off += tile_count[q];
+            }
         }
     }
     __syncthreads();
@@ -295,7 +349,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t idx = wbase + j * 32 + lane;
         if (idx < n) {
-            const uint32_t dd = (key[j] >> shift) & 0xffu;
+            const uint32_t dd = (key[j] >> shift) & R::MASK;
             const uint32_t lp = s_tile_off[dd] + s_warp_hist[warp][dd] + rank[j];
             s_keys[lp] = key[j];
             s_vals[lp] = vin[idx];
@@ -305,7 +359,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     const int valid = (int)(n - tbase < kSortTile ? n - tbase : kSortTile);
     for (int i = threadIdx.x; i < valid; i += kSortThreads) {
         const uint32_t k = s_keys[i];
-        const uint32_t dd = (k >> shift) & 0xffu;
+        const uint32_t dd = (k >> shift) & R::MASK;
         const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
         kout[g] = k;
         vout[g] = s_vals[i];
@@ -371,14 +425,18 @@ int scan_error_flag_offset() { return 8; }   // byte offset of the error word in
 
 SortLayout sort_layout(int64_t n, int key_bits) {
     SortLayout L{};
-    L.passes = (key_bits + 7) / 8;
-    if (L.passes < 1) L.passes = 1;
-    if (L.passes > 4) L.passes = 4;
+    if (key_bits < 1) key_bits = 1;
+    if (key_bits > 32) key_bits = 32;
+    const int p8 = (key_bits + 7) / 8, p10 = (key_bits + 9) / 10;
+    // 10-bit digits where they save a pass (17-20 and 25-30 key bits)
+    L.digit_bits = (key_bits > 16 && key_bits <= 30 && p10 < p8) ? 10 : 8;
+    L.passes = L.digit_bits == 10 ? p10 : p8;
+    const size_t dig = (size_t)1 << L.digit_bits;
     L.tiles = (n + kSortTile - 1) / kSortTile;
     size_t off = 0;
-    L.off_hist = off;    off += align256(sizeof(uint32_t) * 256 * 4);
+    L.off_hist = off;    off += align256(sizeof(uint32_t) * kHistWords);
     L.off_counters = off; off += align256(sizeof(uint32_t) * 8);     // tile counters [4], error word [4]
-    L.off_look = off;    off += align256(sizeof(uint32_t) * 256 * (size_t)(L.tiles > 0 ? L.tiles : 1) * L.passes);
+    L.off_look = off;    off += align256(sizeof(uint32_t) * dig * (size_t)(L.tiles > 0 ? L.tiles : 1) * L.passes);
     L.off_alt_keys = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.off_alt_vals = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.bytes = off;
@@ -388,9 +446,14 @@ SortLayout sort_layout(int64_t n, int key_bits) {
 cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const SortLayout L = sort_layout(n, key_bits);
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortStagingBytes);
+    cudaError_t e = L.digit_bits == 10
+                        ? cudaFuncSetAttribute(k_onesweep<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSortStagingBytes)
+                        : cudaFuncSetAttribute(k_onesweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSortStagingBytes);
     if (e != cudaSuccess) return e;
-    return cudaMemsetAsync(scratch, 0, L.off_look + sizeof(uint32_t) * 256 * (size_t)L.tiles * L.passes, st);
+    return cudaMemsetAsync(scratch, 0,
+                           L.off_look + sizeof(uint32_t) * ((size_t)1 << L.digit_bits) * (size_t)L.tiles * L.passes, st);
 }
 
 uint32_t* radix_sort_hist(int64_t n, int key_bits, void* scratch) {
@@ -401,13 +464,15 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
                               int key_bits, void* scratch, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const SortLayout L = sort_layout(n, key_bits);
+    const int rb = L.digit_bits, dig = 1 << rb;
     char* base = (char*)scratch;
     uint32_t* hist = (uint32_t*)(base + L.off_hist);
     uint32_t* counters = (uint32_t*)(base + L.off_counters);
     uint32_t* look = (uint32_t*)(base + L.off_look);
     uint32_t* ak = (uint32_t*)(base + L.off_alt_keys);
     uint32_t* av = (uint32_t*)(base + L.off_alt_vals);
-    k_radix_bin_offsets<<<L.passes, 256, 0, st>>>(hist);
+    if (rb == 10) k_radix_bin_offsets<10><<<L.passes, 1024, 0, st>>>(hist);
+    else k_radix_bin_offsets<8><<<L.passes, 256, 0, st>>>(hist);
     // ping-pong so that the last pass lands in (kout, vout)
     const uint32_t* sk = kin;
     const uint32_t* sv = vin;
@@ -415,9 +480,13 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
         const bool to_out = ((L.passes - 1 - p) % 2) == 0;
         uint32_t* dk = to_out ? kout : ak;
         uint32_t* dv = to_out ? vout : av;
-        k_onesweep<<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(sk, sv, dk, dv, n, 8 * p, hist + 256 * p,
-                                                               look + (size_t)256 * L.tiles * p, counters + p,
-                                                               (int*)(counters + 4));
+        uint32_t* lp = look + (size_t)dig * L.tiles * p;
+        if (rb == 10)
+            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4));
+        else
+            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         sk = dk;
@@ -431,8 +500,10 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     if (n <= 0) return cudaSuccess;
     cudaError_t e = radix_sort_begin(n, key_bits, scratch, st);
     if (e != cudaSuccess) return e;
-    k_radix_histogram<<<grid_cap(n, 256), 256, 0, st>>>(kin, n, sort_layout(n, key_bits).passes,
-                                                         radix_sort_hist(n, key_bits, scratch));
+    const SortLayout L = sort_layout(n, key_bits);
+    uint32_t* hist = radix_sort_hist(n, key_bits, scratch);
+    if (L.digit_bits == 10) k_radix_histogram<10><<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
+    else k_radix_histogram<8><<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return radix_sort_finish(kin, vin, kout, vout, n, key_bits, scratch, st);

@@ -13,6 +13,7 @@ int scan_error_flag_offset();
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, cudaStream_t st);
 
 struct SortLayout {
+    int digit_bits;   // 8, or 10 where that saves a pass; hist is [passes][1 << digit_bits]
     int passes;
     int64_t tiles;
     size_t off_hist, off_counters, off_look, off_alt_keys, off_alt_vals, bytes;
@@ -22,7 +23,7 @@ SortLayout sort_layout(int64_t n, int key_bits);
 cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
                                  int key_bits, void* scratch, cudaStream_t st);
 // The same in two halves around a caller's kernel that adds the digit counts of every
-// pass ([passes][256], radix_sort_hist) while it writes the keys: begin clears the
+// pass ([passes][1 << digit_bits], radix_sort_hist) while it writes the keys: begin clears the
 // scratch, finish sorts.
 cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_t st);
 uint32_t* radix_sort_hist(int64_t n, int key_bits, void* scratch);
