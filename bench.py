@@ -42,14 +42,57 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clock and clock-event (throttle) reasons of this process's GPU, read through
+    NVML every 10 ms from a thread while the timed region runs (read-only queries; the
+    GPU is found by its PCI bus id, so a remapped CUDA_VISIBLE_DEVICES still names the
+    right board).  Falls back to nvidia-smi at 200 ms where NVML is unavailable."""
 
-    def __init__(self, index: int = 0):
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, index: int = 0, period: float = 0.01):
         self.index = index
+        self.period = period
+        self.samples = []          # (sm_mhz, max_mhz, reason bits)
         self.proc = None
         self.lines = []
+        self._stop = threading.Event()
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(torch.cuda.current_device())
+        bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _poll(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while True:
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx),
+                                     int(get_reasons(h))))
+            except Exception:
+                pass
+            if self._stop.wait(self.period):
+                break
 
     def __enter__(self):
+        try:
+            nv, h = self._handle()
+            self._nvml = nv
+            self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.t.start()
+            t0 = time.perf_counter()
+            while not self.samples and time.perf_counter() - t0 < 1.0:   # first sample before the work
+                time.sleep(0.001)
+            return self
+        except Exception:
+            self._nvml = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -68,6 +111,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self._nvml is not None:
+            self._stop.set()
+            self.t.join(timeout=5)
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -77,7 +127,13 @@ class ClockSampler:
 
     def summary(self):
         mhz, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for sm, m, bits in self.samples:
+            mhz.append(sm)
+            mx = m
+            for nm, bit in self.REASONS:
+                if bits & bit:
+                    reasons.add(nm)
+        names = [nm for nm, _ in self.REASONS]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -91,7 +147,7 @@ class ClockSampler:
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(mhz)}
+                "samples": len(mhz), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def dist_setup(args):

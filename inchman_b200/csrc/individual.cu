@@ -136,10 +136,18 @@ int ind_alloc(IndList& l, int species, long long cap, long long ncells, bool may
     }
     A((void**)&l.props, 4 * sizeof(float) * (size_t)l.cap);
     A((void**)&l.newborn, (size_t)l.cap);
-    A((void**)&l.count, cb);
     A((void**)&l.goal, cb);
-    A((void**)&l.fields, 4 * sizeof(float) * (size_t)ncells);
-    A((void**)&l.d_small, sizeof(uint32_t));
+    // count, fields and the two result words in one block, so that a sweep clears them
+    // with one memset
+    const size_t cb_al = (cb + 255) & ~(size_t)255;
+    const size_t fb_al = (4 * sizeof(float) * (size_t)ncells + 255) & ~(size_t)255;
+    A(&l.sweep_block, cb_al + fb_al + 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) {
+        l.count = (uint32_t*)l.sweep_block;
+        l.fields = (float*)((char*)l.sweep_block + cb_al);
+        l.d_small = (uint32_t*)((char*)l.sweep_block + cb_al + fb_al);
+        e = cudaMallocHost((void**)&l.h_small, 4 * sizeof(uint32_t));
+    }
     A(&l.sort_scratch, l.sort_bytes);
     A(&l.scan_scratch, l.scan_bytes);
     A(&l.pop_scratch, l.pop_bytes);
@@ -155,11 +163,12 @@ int ind_alloc(IndList& l, int species, long long cap, long long ncells, bool may
 }
 
 void ind_free(IndList& l) {
-    void* ptrs[] = {l.keys[0], l.keys[1], l.ids[0],  l.ids[1],  l.pool[0],   l.pool[1],        l.start[0],
-                    l.start[1], l.props, l.newborn, l.count,   l.goal,      l.fields,         l.d_small,
+    void* ptrs[] = {l.keys[0], l.keys[1], l.ids[0],  l.ids[1],       l.pool[0],      l.pool[1],
+                    l.start[0], l.start[1], l.props, l.newborn, l.goal,         l.sweep_block,
                     l.sort_scratch, l.scan_scratch, l.pop_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (l.h_small) cudaFreeHost(l.h_small);
     const int sp = l.species;
     l = IndList();
     l.species = sp;
@@ -235,26 +244,25 @@ int ind_build(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {
     return ind_fields(l, a, k, st);
 }
 
-int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, uint32_t* d_minkey,
-              float* dt_out, cudaStream_t st) {
+int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, int slot,
+              cudaStream_t st) {
     bind(l, a);
-    CK(cudaMemsetAsync(l.count, 0, sizeof(uint32_t) * (size_t)(l.ncells + 1), st));
-    CK(cudaMemsetAsync(l.fields, 0, 4 * sizeof(float) * (size_t)l.ncells, st));
-    CK(cudaMemsetAsync(l.d_small, 0, sizeof(uint32_t), st));
+    // count, fields and the departures word (the time step word is set by launch_timestep)
+    CK(cudaMemsetAsync(l.sweep_block, 0, (size_t)((char*)(l.d_small + 1) - (char*)l.sweep_block), st));
     CK(run_sweep(k, a, st));
     l.sorted = false;
     k_ind_counts<<<grid_for(l.ncells), kIndThreads, 0, st>>>(a);
     CK(cudaGetLastError());
     const float* D = a.dir == 0 ? a.fDx : a.fDy;
     const float* r = a.dir == 0 ? a.fRx : a.fRy;
-    CK(launch_timestep((int)l.ncells, D, r, dx, d_minkey, st, ts_kind, stay));
-    uint32_t h[2] = {0, 0};
-    CK(cudaMemcpyAsync(&h[0], l.d_small, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&h[1], d_minkey, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    l.pending += h[0];
-    *dt_out = key_to_float(h[1]);
+    CK(launch_timestep((int)l.ncells, D, r, dx, l.d_small + 1, st, ts_kind, stay));
+    CK(cudaMemcpyAsync(l.h_small + 2 * slot, l.d_small, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     return GPGMP_OK;
+}
+
+float ind_sweep_result(IndList& l, int slot) {
+    l.pending += l.h_small[2 * slot];
+    return key_to_float(l.h_small[2 * slot + 1]);
 }
 
 int ind_maintain(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {

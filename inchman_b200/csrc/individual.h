@@ -24,7 +24,9 @@ struct IndList {
     uint32_t* count = nullptr;        // [ncells + 1]
     int32_t* goal = nullptr;          // [ncells + 1] counts to maintain
     float* fields = nullptr;          // [4][ncells]
-    uint32_t* d_small = nullptr;      // individuals that left in the last sweep
+    uint32_t* d_small = nullptr;      // [2]: individuals that left in the last sweep, its time step key
+    void* sweep_block = nullptr;      // one allocation: count, fields, d_small (cleared by one memset per sweep)
+    uint32_t* h_small = nullptr;      // pinned [2 slots][2]: d_small of the sweeps of one diffuse call
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     void* scan_scratch = nullptr;
@@ -52,9 +54,12 @@ void ind_free(IndList& l);
 // reference's IndividualSolver constructor fills them), then the fields.
 int ind_build(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st);
 // One sweep (a.dir) with the counts and fields folded in, then the new time step of
-// that direction (the smallest over every cell of every realisation) in *dt_out.
-int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, uint32_t* d_minkey,
-              float* dt_out, cudaStream_t st);
+// that direction (the smallest over every cell of every realisation).  Enqueued only:
+// the number that left and the time step land in h_small[slot]; once the stream has
+// been synchronised, ind_sweep_result books the departures and returns the time step.
+int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, int slot,
+              cudaStream_t st);
+float ind_sweep_result(IndList& l, int slot);
 // After a reaction window: the list follows the counts (population bookkeeping);
 // the individuals created get the new-individuals method's properties.
 int ind_maintain(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st);

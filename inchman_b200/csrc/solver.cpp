@@ -724,21 +724,30 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
     if (!h->ind.empty() && h->ind[i].species >= 0) {
         // InhomogeneousSolver::diffuse for an individual species (:264-269, :303-335):
         // move the individuals, then new fields and a new time step of that direction
+        // Both sweeps go out before the host waits: the y sweep takes the time step
+        // known before this call, so the x sweep's results are read with its own.
         h->sim_time = t;
+        bool swept[2] = {false, false};
         for (int dir = 0; dir < 2; ++dir) {
-            float& nxt = dir == 0 ? h->nextX[i] : h->nextY[i];
-            if (!(nxt <= t)) continue;
-            float& dd = dir == 0 ? h->ddX[i] : h->ddY[i];
-            float& small = dir == 0 ? h->smallX[i] : h->smallY[i];
+            if (!((dir == 0 ? h->nextX[i] : h->nextY[i]) <= t)) continue;
+            const float dd = dir == 0 ? h->ddX[i] : h->ddY[i];
             const float dxd = h->m.physical_length / (float)(dir == 0 ? h->m.width : h->m.height);
-            float ndt = 0.f;
             int rc = ind_sweep(h->ind[i], ind_args(h, i, dir, dd, (uint32_t)*seed), h->ind_k, dxd, h->ts_kind, h->stay,
-                               h->d_minkey, &ndt, h->stream);
+                               dir, h->stream);
             if (rc) return rc;
             (*seed)++;
-            small = ndt;
-            nxt += small;
-            dd = small;
+            swept[dir] = true;
+        }
+        if (swept[0] || swept[1]) {
+            cudaError_t e = cudaStreamSynchronize(h->stream);
+            if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "individual sweeps: %s", cudaGetErrorString(e));
+        }
+        for (int dir = 0; dir < 2; ++dir) {
+            if (!swept[dir]) continue;
+            float& small = dir == 0 ? h->smallX[i] : h->smallY[i];
+            small = ind_sweep_result(h->ind[i], dir);
+            (dir == 0 ? h->nextX[i] : h->nextY[i]) += small;
+            (dir == 0 ? h->ddX[i] : h->ddY[i]) = small;
         }
         h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
         return GPGMP_OK;
