@@ -347,6 +347,23 @@ def bench_gray_scott(args, rank, world):
     return line
 
 
+def cpu_baseline_particles(steps=3):
+    """The oracle's replay of the particle step (OpenMP C) on the host cores: a bounded
+    sample of three steps of the same 2^22 seeded particles as the GPU workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from inchman_b200.individual import uniform_particles
+    G = 1024
+    x, y, sp = uniform_particles(1 << 22, G, seed=1234)
+    n = len(x)
+    t0 = time.perf_counter()
+    m = oracle.orc().orc_particles_run(n, oracle.ptr(x), oracle.ptr(y), oracle.ptr(sp), G, 0.5, 0.1, 0.0, 1.0, 0.05,
+                                       1234, 0, steps)
+    dt = time.perf_counter() - t0
+    return {"value": (n + m) / 2 * steps / dt, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} steps of the same {n} particles (oracle, OpenMP)"}
+
+
 def cpu_baseline_gray_scott(cfg, steps=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -419,6 +436,8 @@ def main(argv=None):
     else:
         from inchman_b200 import workloads
         line = workloads.run(args, rank, world)
+        if args.workload == "particles" and rank == 0 and world == 1:
+            line["cpu_baseline"] = cpu_baseline_particles()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
