@@ -22,6 +22,10 @@ constexpr int kIndThreads = 256;
 __global__ void __launch_bounds__(kIndThreads) k_ind_sweep(IndArgs a) { ind_sweep_body(a, IndDriftStored()); }
 __global__ void __launch_bounds__(kIndThreads) k_ind_fields(IndArgs a) { ind_fields_body(a, IndDriftStored()); }
 __global__ void __launch_bounds__(kIndThreads) k_ind_counts(IndArgs a) { ind_counts_body(a); }
+__global__ void __launch_bounds__(kIndThreads) k_ind_counts_timestep(IndArgs a, float dx, int kind, float stay,
+                                                                     uint32_t* inv_min_key) {
+    ind_counts_timestep_body(a, dx, kind, stay, inv_min_key);
+}
 
 // goal[r * area + cell] = the species' count in the state
 __global__ void k_ind_gather(IndArgs a, int32_t* __restrict__ goal) {
@@ -247,22 +251,19 @@ int ind_build(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {
 int ind_sweep(IndList& l, IndArgs a, const IndKernels& k, float dx, int ts_kind, float stay, int slot,
               cudaStream_t st) {
     bind(l, a);
-    // count, fields and the departures word (the time step word is set by launch_timestep)
-    CK(cudaMemsetAsync(l.sweep_block, 0, (size_t)((char*)(l.d_small + 1) - (char*)l.sweep_block), st));
+    // count, fields, the departures word and the inverted time step key
+    CK(cudaMemsetAsync(l.sweep_block, 0, (size_t)((char*)(l.d_small + 2) - (char*)l.sweep_block), st));
     CK(run_sweep(k, a, st));
     l.sorted = false;
-    k_ind_counts<<<grid_for(l.ncells), kIndThreads, 0, st>>>(a);
+    k_ind_counts_timestep<<<grid_for(l.ncells), kIndThreads, 0, st>>>(a, dx, ts_kind, stay, l.d_small + 1);
     CK(cudaGetLastError());
-    const float* D = a.dir == 0 ? a.fDx : a.fDy;
-    const float* r = a.dir == 0 ? a.fRx : a.fRy;
-    CK(launch_timestep((int)l.ncells, D, r, dx, l.d_small + 1, st, ts_kind, stay));
     CK(cudaMemcpyAsync(l.h_small + 2 * slot, l.d_small, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     return GPGMP_OK;
 }
 
 float ind_sweep_result(IndList& l, int slot) {
     l.pending += l.h_small[2 * slot];
-    return key_to_float(l.h_small[2 * slot + 1]);
+    return key_to_float(~l.h_small[2 * slot + 1]);
 }
 
 int ind_maintain(IndList& l, IndArgs a, const IndKernels& k, cudaStream_t st) {

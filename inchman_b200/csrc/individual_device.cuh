@@ -190,6 +190,38 @@ __device__ __forceinline__ void ind_fields_body(const IndArgs& a, const DRIFT& d
     }
 }
 
+// the cells' new counts, then the smallest time step of the sweep's direction over
+// every cell from the fields the sweep folded in (k_timestep's rule): the key of the
+// smallest step goes into *inv_min_key inverted, as an atomic maximum, so that the
+// word starts from zero with the others the sweep clears
+__device__ __forceinline__ void ind_counts_timestep_body(const IndArgs& a, float dx, int kind, float stay,
+                                                         uint32_t* inv_min_key) {
+    const long long area = (long long)a.W * a.H;
+    const long long total = (long long)a.R * area;
+    const float* D = a.dir == 0 ? a.fDx : a.fDy;
+    const float* r = a.dir == 0 ? a.fRx : a.fRy;
+    uint32_t best = 0u;   // inverted key: larger is a smaller step
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int rr = (int)(k / area);
+        const long long cell = k - (long long)rr * area;
+        a.planes[a.species][((long long)rr * a.S + a.species) * area + cell] = (int)a.count[k];
+        const float ts = kind == kTsFpe             ? fpe_timestep(D[k], r[k], dx, stay)
+                         : kind == kTsDeterministic ? det_timestep(D[k], r[k], dx)
+                                                    : cell_timestep(D[k], r[k], dx);
+        if (ts == ts) {   // NaN is skipped, as fminf does
+            const uint32_t b = __float_as_uint(ts);
+            const uint32_t key = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+            best = ~key > best ? ~key : best;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other > best ? other : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best) atomicMax(inv_min_key, best);
+}
+
 // the cells' new counts, once every thread of the fields pass has read the old ones
 __device__ __forceinline__ void ind_counts_body(const IndArgs& a) {
     const long long area = (long long)a.W * a.H;
