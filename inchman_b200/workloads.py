@@ -300,8 +300,8 @@ def individuals(args, rank, world):
     per cell (262,144, the reference's c_maxNumIndividuals), each with its own
     diffusivity (0.3..0.7) and drift (-0.2..0.2); one step = one x and one y sweep of
     every individual (one kernel moves it and folds its cell's count and fields in,
-    then the counts go to the state and the time step is read back; the list is
-    sorted only when read).  Unit: individual-sweeps/s.
+    a second writes the counts to the state and takes the time step, which is read
+    back; the list is sorted only when read).  Unit: individual-sweeps/s.
 
     Roofline: per individual and sweep the bytes that must move at least once -- read
     key, id and four properties, write the key (28 B) -- plus 24 B per cell (count and
@@ -352,8 +352,8 @@ def individuals(args, rank, world):
                  {"grid": [W, W], "individuals": n, "steps_timed": args.steps, "sweeps_per_step": 2},
                  tsec / args.steps * 1e3,
                  {"dtype": "u32+f32", "individuals_left": n_end,
-                  # per sweep: the fused move, the counts, the time step
-                  "gpu_launches": 3 * sweeps,
+                  # per sweep: the fused move, the counts with the time step
+                  "gpu_launches": 2 * sweeps,
                   "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_sweep": alg}})
 
