@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
 #pragma unroll
     for (int q = 0; q < DPT; ++q) {
         tile_count[q] = digit_thread ? s_count[d0 + q] : 0u;
-        if (digit_thread) st_release_u32(&lk[d0 + q], (tile == 0 ? kFlagP : kFlagA) | tile_count[q]);
+        if (digit_thread) st_relaxed_u32(&lk[d0 + q], (tile == 0 ? kFlagP : kFlagA) | tile_count[q]);
     }
     // warp-level ranking (stable): the lanes holding the same digit, from RB ballots
     const unsigned lt = (1u << lane) - 1u;
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
             for (int q = 0; q < DPT; ++q)
 #pragma unroll
                 for (int j = 0; j < kLookWindow; ++j)
-                    w[q][j] = (!done[q] && t - j >= 0) ? ld_acquire_u32(&look[(size_t)(t - j) * DIG + d0 + q]) : kFlagP;
+                    w[q][j] = (!done[q] && t - j >= 0) ? ld_relaxed_u32(&look[(size_t)(t - j) * DIG + d0 + q]) : kFlagP;
             bool ready = true;
 #pragma unroll
             for (int q = 0; q < DPT; ++q)
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
             t -= kLookWindow;
         }
 #pragma unroll
-        for (int q = 0; q < DPT; ++q) st_release_u32(&lk[d0 + q], kFlagP | ((excl[q] + tile_count[q]) & kValMask));
+        for (int q = 0; q < DPT; ++q) st_relaxed_u32(&lk[d0 + q], kFlagP | ((excl[q] + tile_count[q]) & kValMask));
     }
     // tile-local digit offsets (exclusive scan of the tile counts over the digits)
     {
