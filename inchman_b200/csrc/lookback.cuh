@@ -24,6 +24,9 @@ __device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t* p) {
 __device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
@@ -51,14 +54,16 @@ constexpr int kLookDepth = 4;   // status words per lane per round: 128 tiles
 // inclusive prefix and returns the exclusive prefix (in every lane).  Only the tiles
 // up to the nearest one with an inclusive prefix need to have published; the loads
 // of a round are independent, so a tile far from any inclusive prefix sums 128
-// aggregates per memory round trip.  err is set when a wait exceeds kSpinLimit.
+// aggregates per memory round trip.  A status word carries its whole payload (flag
+// and value), so it is published and read with relaxed accesses (no fences).  err is
+// set when a wait exceeds kSpinLimit.
 __device__ __forceinline__ uint32_t warp_lookback_u32(uint64_t* status, uint32_t tile, uint32_t aggregate, int* err) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        if (lane == 0) st_release_u64(&status[0], kScanFlagP | aggregate);
+        if (lane == 0) st_relaxed_u64(&status[0], kScanFlagP | aggregate);
         return 0u;
     }
-    if (lane == 0) st_release_u64(&status[tile], kScanFlagA | aggregate);
+    if (lane == 0) st_relaxed_u64(&status[tile], kScanFlagA | aggregate);
     int64_t look = (int64_t)tile - 1;
     uint32_t exclusive = 0, spins = 0;
     while (true) {
@@ -101,7 +106,7 @@ __device__ __forceinline__ uint32_t warp_lookback_u32(uint64_t* status, uint32_t
         if (pu < kLookDepth) break;
         look -= 32 * kLookDepth;
     }
-    if (lane == 0) st_release_u64(&status[tile], kScanFlagP | (uint32_t)(exclusive + aggregate));
+    if (lane == 0) st_relaxed_u64(&status[tile], kScanFlagP | (uint32_t)(exclusive + aggregate));
     return exclusive;
 }
 
