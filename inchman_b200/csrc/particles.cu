@@ -10,8 +10,8 @@
 // a step is
 //   move:    x += vx dt + sqrt(2 D dt) z (Box-Muller normals from the particle's
 //            Philox stream), reflecting walls, key = floor(y) G + floor(x);
-//   bin:     stable radix sort of (key, index) (the move counts the digits), count
-//            per cell;
+//   bin:     stable radix sort of (key, index) (the move counts the digits, the
+//            sort's last pass the particles per cell);
 //   react:   in each cell the k-th A (in sorted order) pairs with the k-th B and the
 //            pair is removed with probability p (one 32-bit draw per pair against
 //            floor(p 2^32));
@@ -426,6 +426,7 @@ static int particles_step_one(gpgmp_particles* h) {
     const float sig = sqrtf(2.0f * h->D * h->dt);
     const float ax = h->vx * h->dt, ay = h->vy * h->dt;
     const uint32_t step = (uint32_t)h->step;
+    CK(cudaMemsetAsync(h->count, 0, sizeof(uint32_t) * (size_t)ncells, st));
     if (n > 0) {
         CK(radix_sort_begin(n, h->key_bits, h->sort_scratch, st));
         const SortLayout L = sort_layout(n, h->key_bits);
@@ -433,9 +434,10 @@ static int particles_step_one(gpgmp_particles* h) {
                                                      h->vals, radix_sort_hist(n, h->key_bits, h->sort_scratch),
                                                      L.passes, L.digit_bits);
         CK(cudaGetLastError());
-        CK(radix_sort_finish(h->keys, h->vals, h->skeys, h->svals, n, h->key_bits, h->sort_scratch, st));
+        // the last pass also counts the particles per cell
+        CK(radix_sort_finish(h->keys, h->vals, h->skeys, h->svals, n, h->key_bits, h->sort_scratch, st, h->count,
+                             ncells));
     }
-    CK(cell_counts_u32(h->skeys, n, ncells, h->count, st));
     CK(cudaMemsetAsync(h->rc_scratch, 0, sizeof(uint64_t) * (4 + 2 * (size_t)h->rc_tiles), st));
     // staging for twice the mean number of particles per tile (+ 1024), up to 47 KB
     // (with the static shared memory, within the 48 KB a launch gets without opting in)

@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            int64_t n, int shift, const uint32_t* __restrict__ bins,
                                                            uint32_t* __restrict__ look, unsigned int* tile_counter,
-                                                           int* err) {
+                                                           int* err, uint32_t* __restrict__ cell_count,
+                                                           uint32_t ncells) {
     using R = Radix<RB>;
     constexpr int DIG = R::DIG;
     constexpr int DPT = R::kDPT;
@@ -357,12 +358,36 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     }
     __syncthreads();
     const int valid = (int)(n - tbase < kSortTile ? n - tbase : kSortTile);
-    for (int i = threadIdx.x; i < valid; i += kSortThreads) {
-        const uint32_t k = s_keys[i];
-        const uint32_t dd = (k >> shift) & R::MASK;
-        const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
-        kout[g] = k;
-        vout[g] = s_vals[i];
+    if (!cell_count) {
+        for (int i = threadIdx.x; i < valid; i += kSortThreads) {
+            const uint32_t k = s_keys[i];
+            const uint32_t dd = (k >> shift) & R::MASK;
+            const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
+            kout[g] = k;
+            vout[g] = s_vals[i];
+        }
+        return;
+    }
+    // last pass with cell counts: the staged keys are the tile's keys in full order, so
+    // a warp's 32 consecutive keys form a few runs of equal cells; the last lane of each
+    // run adds the run's length (whole warps step together for the shuffles)
+    for (int b = threadIdx.x - lane; b < valid; b += kSortThreads) {
+        const int i = b + lane;
+        const bool ok = i < valid;
+        const uint32_t k = ok ? s_keys[i] : 0xffffffffu;
+        if (ok) {
+            const uint32_t dd = (k >> shift) & R::MASK;
+            const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
+            kout[g] = k;
+            vout[g] = s_vals[i];
+        }
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, k, 1);
+        const uint32_t next = __shfl_down_sync(0xffffffffu, k, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || k != prev);
+        if (ok && k < ncells && (lane == 31 || k != next)) {
+            const int first = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+            atomicAdd(&cell_count[k], (uint32_t)(lane - first + 1));
+        }
     }
 }
 
@@ -461,7 +486,7 @@ uint32_t* radix_sort_hist(int64_t n, int key_bits, void* scratch) {
 }
 
 cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
-                              int key_bits, void* scratch, cudaStream_t st) {
+                              int key_bits, void* scratch, cudaStream_t st, uint32_t* cell_count, int64_t ncells) {
     if (n <= 0) return cudaSuccess;
     const SortLayout L = sort_layout(n, key_bits);
     const int rb = L.digit_bits, dig = 1 << rb;
@@ -481,12 +506,15 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
         uint32_t* dk = to_out ? kout : ak;
         uint32_t* dv = to_out ? vout : av;
         uint32_t* lp = look + (size_t)dig * L.tiles * p;
+        uint32_t* cc = p == L.passes - 1 ? cell_count : nullptr;
         if (rb == 10)
             k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
-                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4));
+                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
+                (uint32_t)ncells);
         else
             k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
-                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4));
+                sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
+                (uint32_t)ncells);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         sk = dk;

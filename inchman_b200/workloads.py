@@ -185,14 +185,14 @@ def particles(args, rank, world):
     x1, _, _ = p.get()
     ps = (n0 + len(x1)) / 2 * args.steps
     # kernels per step for the 20-bit cell keys: move, bin offsets, two 10-bit onesweep
-    # passes, cell counts, react + compact
-    launches = 6 * args.steps
+    # passes (the last counts the cells), react + compact
+    launches = 5 * args.steps
     # Roofline of the whole step (the kernels run inside one library call): the bytes
     # that must move at least once per particle -- move 24 (read x, y; write x, y, key,
-    # index), two sort passes 2 x 16, cell counts 4, react + compact 4 index + 1
-    # species + 8 position read, 9 written -- plus 12 B per cell (count written and
-    # read, start written)
-    alg = 82.0 * ps / args.steps + 12.0 * G * G
+    # index), two sort passes 2 x 16 (the cell counts come with the last), react +
+    # compact 4 index + 1 species + 8 position read, 9 written -- plus 12 B per cell
+    # (count written and read, start written)
+    alg = 78.0 * ps / args.steps + 12.0 * G * G
     ach = alg / (t / args.steps) / 1e9
     peak, peak_kind = _peaks()
     extra = {"particles_left": len(x1), "dtype": "f32+u32", "gpu_launches": launches,
