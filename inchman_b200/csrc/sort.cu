@@ -12,8 +12,9 @@
 //  - radix sort: onesweep (Adinets & Merrill 2022): one histogram kernel for every
 //    digit position, then one kernel per digit (8 bits, or 10 where that saves a
 //    pass: 17-20 and 25-30 key bits) that ranks its tile (peer masks from ballots),
-//    publishes per-digit tile counts, looks back for the prefix and scatters through
-//    shared memory; stable;
+//    publishes per-digit tile counts, looks back for the prefix, scans the pass's
+//    digit counts into the digits' global starts itself and scatters through shared
+//    memory; stable;
 //  - cell offsets: key histogram + exclusive scan (start), count; the reference's
 //    left/right indices follow from them.
 // Every look-back spin has an iteration limit; exceeding it sets the error word
@@ -155,23 +156,6 @@ __global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restr
     }
 }
 
-// exclusive scan of each pass's DIG bins (one block of DIG threads per pass)
-template <int RB>
-__global__ void k_radix_bin_offsets(uint32_t* __restrict__ hist) {
-    using R = Radix<RB>;
-    __shared__ uint32_t s[R::DIG];
-    uint32_t* h = hist + blockIdx.x * R::DIG;
-    s[threadIdx.x] = h[threadIdx.x];
-    __syncthreads();
-    for (int o = 1; o < R::DIG; o <<= 1) {
-        uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
-        __syncthreads();
-        s[threadIdx.x] += t;
-        __syncthreads();
-    }
-    h[threadIdx.x] = s[threadIdx.x] - h[threadIdx.x];
-}
-
 // One onesweep pass.  Warp w of a tile owns keys [w*32*IT, (w+1)*32*IT) of the tile
 // in a warp-striped layout (item j of lane l is key j*32 + l), so processing items in
 // order and lanes in order is index order: the ranks are stable.
@@ -193,6 +177,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     __shared__ uint32_t s_tile_off[DIG];     // exclusive offset of each digit inside the tile
     __shared__ uint32_t s_global[DIG];       // global start of each digit's run of this tile
     __shared__ uint32_t s_w[R::kDigitWarps];
+    __shared__ uint32_t s_hw[R::kDigitWarps];
     extern __shared__ uint32_t s_staging[];  // keys then values in tile-sorted order (dynamic: 60 KB)
     uint32_t* s_keys = s_staging;
     uint32_t* s_vals = s_staging + kSortTile;
@@ -318,29 +303,46 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
 #pragma unroll
         for (int q = 0; q < DPT; ++q) st_relaxed_u32(&lk[d0 + q], kFlagP | ((excl[q] + tile_count[q]) & kValMask));
     }
-    // tile-local digit offsets (exclusive scan of the tile counts over the digits)
+    // tile-local digit offsets (exclusive scan of the tile counts over the digits) and
+    // the digits' global starts (exclusive scan of the pass's digit counts in bins; every
+    // tile scans them itself, so no separate launch turns counts into offsets)
     {
-        uint32_t mine = 0;
+        uint32_t mine = 0, hmine = 0, hc[DPT];
 #pragma unroll
-        for (int q = 0; q < DPT; ++q) mine += tile_count[q];
-        uint32_t incl = mine;
+        for (int q = 0; q < DPT; ++q) {
+            hc[q] = digit_thread ? bins[d0 + q] : 0u;
+            mine += tile_count[q];
+            hmine += hc[q];
+        }
+        uint32_t incl = mine, hincl = hmine;
         if (digit_thread) {
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                const uint32_t ht = __shfl_up_sync(0xffffffffu, hincl, o);
+                if (lane >= o) {
+                    incl += t;
+                    hincl += ht;
+                }
             }
-            if (lane == 31) s_w[warp] = incl;
+            if (lane == 31) {
+                s_w[warp] = incl;
+                s_hw[warp] = hincl;
+            }
         }
         __syncthreads();
         if (digit_thread) {
-            uint32_t off = incl - mine;
-            for (int w = 0; w < warp; ++w) off += s_w[w];
+            uint32_t off = incl - mine, hoff = hincl - hmine;
+            for (int w = 0; w < warp; ++w) {
+                off += s_w[w];
+                hoff += s_hw[w];
+            }
 #pragma unroll
             for (int q = 0; q < DPT; ++q) {
                 s_tile_off[d0 + q] = off;
-                s_global[d0 + q] = bins[d0 + q] + excl[q];
+                s_global[d0 + q] = hoff + excl[q];
                 off += tile_count[q];
+                hoff += hc[q];
             }
         }
     }
@@ -496,8 +498,6 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
     uint32_t* look = (uint32_t*)(base + L.off_look);
     uint32_t* ak = (uint32_t*)(base + L.off_alt_keys);
     uint32_t* av = (uint32_t*)(base + L.off_alt_vals);
-    if (rb == 10) k_radix_bin_offsets<10><<<L.passes, 1024, 0, st>>>(hist);
-    else k_radix_bin_offsets<8><<<L.passes, 256, 0, st>>>(hist);
     // ping-pong so that the last pass lands in (kout, vout)
     const uint32_t* sk = kin;
     const uint32_t* sv = vin;

@@ -184,9 +184,9 @@ def particles(args, rank, world):
     t = a.elapsed_time(b) / 1e3
     x1, _, _ = p.get()
     ps = (n0 + len(x1)) / 2 * args.steps
-    # kernels per step for the 20-bit cell keys: move, bin offsets, two 10-bit onesweep
-    # passes (the last counts the cells), react + compact
-    launches = 5 * args.steps
+    # kernels per step for the 20-bit cell keys: move, two 10-bit onesweep passes (the
+    # last counts the cells), react + compact
+    launches = 4 * args.steps
     # Roofline of the whole step (the kernels run inside one library call): the bytes
     # that must move at least once per particle -- move 24 (read x, y; write x, y, key,
     # index), two sort passes 2 x 16 (the cell counts come with the last), react +
