@@ -103,7 +103,7 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
 // pairs the A's and B's of its cells there (the k-th A in sorted order with the k-th
 // B; a pair goes with probability thresh / 2^32, one 32-bit draw per pair from the
 // cell's stream), the tile takes its survivors' output offset from the scan of the
-// survivor counts, and each warp writes the survivors of its share of the range
+// survivor counts, and each warp writes the survivors of its own threads' cells
 // (position and species) with ballot-ranked, coalesced stores: the order of
 // compacting the sorted list by alive flags.  The last tile writes the total.  A tile
 // with more particles than the staging holds walks each cell in global memory with
@@ -170,7 +170,9 @@ __device__ __forceinline__ uint32_t pair_cell(uint32_t b, uint32_t f, const SP& 
 // scratch (uint64 words): [0] tile counter (u32), error word (u32 at byte 8), total
 // (u32 at byte 16), then the status words of the two scans, ntiles each.
 // Dynamic shared memory: cap bytes (species of the staged particles).
-__global__ void __launch_bounds__(kRcThreads) k_react_compact(
+// (at most 32 registers: eight tiles per SM, so the 1024 tiles of a 1024 x 1024 grid
+// are resident in one wave)
+__global__ void __launch_bounds__(kRcThreads, 8) k_react_compact(
     const uint32_t* __restrict__ count, uint32_t* __restrict__ start, int64_t ncells,
     const uint32_t* __restrict__ svals, const float* __restrict__ x, const float* __restrict__ y,
     const uint8_t* __restrict__ sp, uint32_t seed, uint32_t step, uint32_t thresh, uint32_t* __restrict__ alive,
@@ -179,7 +181,6 @@ __global__ void __launch_bounds__(kRcThreads) k_react_compact(
     extern __shared__ uint8_t s_sp[];          // [cap] species, kRcDead = removed
     __shared__ uint32_t s_tile, s_prefix;
     __shared__ uint32_t s_warp[kRcWarps];
-    __shared__ uint32_t s_wbase[kRcWarps];
     unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
     int* err = reinterpret_cast<int*>(scratch) + 2;
     uint32_t* total = reinterpret_cast<uint32_t*>(scratch) + 4;
@@ -221,6 +222,9 @@ __global__ void __launch_bounds__(kRcThreads) k_react_compact(
             if (c0 + j < ncells) start[c0 + j] = S + o[j];
     }
     const bool staged = agg <= cap;            // the same in every thread of the block
+    // the part of the staged range that holds this warp's threads' cells
+    const uint32_t w0 = __shfl_sync(0xffffffffu, o[0], 0);
+    const uint32_t w1 = __shfl_sync(0xffffffffu, o[kRcCells], 31);
     uint32_t removed = 0;
     if (staged) {
         for (uint32_t p0 = 0; p0 < agg; p0 += 4 * kRcThreads) {
@@ -265,19 +269,10 @@ __global__ void __launch_bounds__(kRcThreads) k_react_compact(
     }
     __syncthreads();
     if (staged) {
-        // warp w writes rows of 32 particles of its share [w0, w1) of the range
-        const uint32_t share = ((agg + kRcWarps * 32 - 1) / (kRcWarps * 32)) * 32;
-        const uint32_t w0 = min(agg, (uint32_t)warp * share), w1 = min(agg, w0 + share);
-        uint32_t mine = 0;
-        for (uint32_t r = w0; r < w1; r += 32) {
-            const uint32_t p = r + lane;
-            const bool live = p < w1 && s_sp[p] != kRcDead;
-            mine += __popc(__ballot_sync(0xffffffffu, live));
-        }
-        if (lane == 0) s_wbase[warp] = mine;
-        __syncthreads();
-        uint32_t d = s_prefix;
-        for (int w = 0; w < warp; ++w) d += s_wbase[w];
+        // warp w writes the particles of its own threads' cells -- one contiguous part
+        // [w0, w1) of the staged range -- in rows of 32; its survivors start where its
+        // first lane's exclusive survivor count says
+        uint32_t d = s_prefix + __shfl_sync(0xffffffffu, ex2, 0);
         for (uint32_t r = w0; r < w1; r += 32) {
             const uint32_t p = r + lane;
             const bool live = p < w1 && s_sp[p] != kRcDead;
