@@ -100,7 +100,8 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
 // (lookback.cuh).  A tile of 1024 cells (four per thread) takes its cells' starts
 // from the scan of the counts; its particles are then one contiguous range of the
 // sorted list, whose species bytes the block stages in shared memory.  Each thread
-// pairs the A's and B's of its cells there (the k-th A in sorted order with the k-th
+// pairs the A's and B's of its cells there (from species bit masks in a cell of up to
+// 32, by walking the staged bytes in a larger one) (the k-th A in sorted order with the k-th
 // B; a pair goes with probability thresh / 2^32, one 32-bit draw per pair from the
 // cell's stream), the tile takes its survivors' output offset from the scan of the
 // survivor counts, and each warp writes the survivors of its own threads' cells
@@ -241,11 +242,47 @@ __global__ void __launch_bounds__(kRcThreads, 8) k_react_compact(
             }
         }
         __syncthreads();
-        const auto staged_sp = [&](uint32_t q) { return s_sp[q]; };
 #pragma unroll
-        for (int j = 0; j < kRcCells; ++j)
-            if (cnt[j] >= 2)
-                removed += pair_cell(o[j], o[j + 1], staged_sp, seed, step, (uint32_t)(c0 + j), thresh, s_sp, nullptr);
+        for (int j = 0; j < kRcCells; ++j) {
+            if (cnt[j] >= 2) {
+                Stream st;
+                st.init(seed, 1u, step, (uint32_t)(c0 + j), PH_PAIR);
+                if (cnt[j] <= 32) {
+                    // species masks of the cell; the k-th set bits of the two masks pair
+                    uint32_t am = 0, bm = 0;
+                    for (uint32_t q = 0; q < cnt[j]; ++q) {
+                        const uint8_t t = s_sp[o[j] + q];
+                        am |= (uint32_t)(t == 0) << q;
+                        bm |= (uint32_t)(t == 1) << q;
+                    }
+                    while (am && bm) {
+                        const int ia = __ffs(am) - 1, ib = __ffs(bm) - 1;
+                        am &= am - 1u;
+                        bm &= bm - 1u;
+                        if (st.next() < thresh) {
+                            s_sp[o[j] + ia] = kRcDead;
+                            s_sp[o[j] + ib] = kRcDead;
+                            removed++;
+                        }
+                    }
+                } else {
+                    uint32_t ia = o[j], ib = o[j];
+                    const uint32_t f = o[j + 1];
+                    for (;;) {
+                        while (ia < f && s_sp[ia] != 0) ia++;
+                        while (ib < f && s_sp[ib] != 1) ib++;
+                        if (ia >= f || ib >= f) break;
+                        if (st.next() < thresh) {
+                            s_sp[ia] = kRcDead;
+                            s_sp[ib] = kRcDead;
+                            removed++;
+                        }
+                        ia++;
+                        ib++;
+                    }
+                }
+            }
+        }
     } else {
         const auto global_sp = [&](uint32_t q) { return sp[svals[q]]; };
         for (uint32_t q = S + o[0]; q < S + o[kRcCells]; ++q) alive[q] = 1u;
