@@ -100,10 +100,10 @@ __global__ void k_move(float* __restrict__ px, float* __restrict__ py, int64_t n
 // (lookback.cuh).  A tile of 1024 cells (four per thread) takes its cells' starts
 // from the scan of the counts; its particles are then one contiguous range of the
 // sorted list, whose species bytes the block stages in shared memory.  Each thread
-// pairs the A's and B's of its cells there (from species bit masks in a cell of up to
-// 32, by walking the staged bytes in a larger one) (the k-th A in sorted order with the k-th
-// B; a pair goes with probability thresh / 2^32, one 32-bit draw per pair from the
-// cell's stream), the tile takes its survivors' output offset from the scan of the
+// pairs the A's and B's of its cells there: the k-th A in sorted order with the k-th
+// B, a pair going with probability thresh / 2^32 (one 32-bit draw per pair from the
+// cell's stream), from species bit masks in a cell of up to 32 particles and by
+// walking the staged bytes in a larger one.  Then the tile takes its survivors' output offset from the scan of the
 // survivor counts, and each warp writes the survivors of its own threads' cells
 // (position and species) with ballot-ranked, coalesced stores: the order of
 // compacting the sorted list by alive flags.  The last tile writes the total.  A tile
