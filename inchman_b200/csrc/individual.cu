@@ -181,11 +181,14 @@ void ind_free(IndList& l) {
 int ind_sort(IndList& l, cudaStream_t st) {
     if (l.sorted) return GPGMP_OK;
     const int c = l.cur;
+    // the sort's last pass counts the individuals per key (cells and the killed bin)
+    CK(cudaMemsetAsync(l.count, 0, sizeof(uint32_t) * (size_t)(l.ncells + 1), st));
     if (l.n > 0) {
-        CK(radix_sort_pairs_u32(l.keys[c], l.ids[c], l.keys[1 - c], l.ids[1 - c], l.n, l.key_bits, l.sort_scratch, st));
+        CK(radix_sort_pairs_u32(l.keys[c], l.ids[c], l.keys[1 - c], l.ids[1 - c], l.n, l.key_bits, l.sort_scratch, st,
+                                l.count, l.ncells + 1));
         l.cur = 1 - c;
     }
-    CK(cell_offsets_u32(l.keys[l.cur], l.n, l.ncells + 1, l.start[0], l.count, l.scan_scratch, st));
+    CK(scan_exclusive_u32(l.count, l.start[0], l.ncells + 1, l.scan_scratch, st));
     uint32_t err[2] = {0, 0};
     CK(cudaMemcpyAsync(&err[0], (const char*)l.scan_scratch + scan_error_flag_offset(), sizeof(uint32_t),
                        cudaMemcpyDeviceToHost, st));

@@ -524,7 +524,7 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
 }
 
 cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
-                                 int key_bits, void* scratch, cudaStream_t st) {
+                                 int key_bits, void* scratch, cudaStream_t st, uint32_t* cell_count, int64_t ncells) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = radix_sort_begin(n, key_bits, scratch, st);
     if (e != cudaSuccess) return e;
@@ -534,7 +534,7 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     else k_radix_histogram<8><<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    return radix_sort_finish(kin, vin, kout, vout, n, key_bits, scratch, st);
+    return radix_sort_finish(kin, vin, kout, vout, n, key_bits, scratch, st, cell_count, ncells);
 }
 
 cudaError_t cell_counts_u32(const uint32_t* sorted_keys, int64_t n, int64_t ncells, uint32_t* count, cudaStream_t st) {

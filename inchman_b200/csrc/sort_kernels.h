@@ -20,8 +20,11 @@ struct SortLayout {
 };
 // scratch layout of one radix sort; the error word is the uint32 at off_counters + 16
 SortLayout sort_layout(int64_t n, int key_bits);
+// With cell_count (zeroed by the caller), the last pass also adds the number of keys
+// equal to each c < ncells into cell_count[c].
 cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t n,
-                                 int key_bits, void* scratch, cudaStream_t st);
+                                 int key_bits, void* scratch, cudaStream_t st, uint32_t* cell_count = nullptr,
+                                 int64_t ncells = 0);
 // The same in two halves around a caller's kernel that adds the digit counts of every
 // pass ([passes][1 << digit_bits], radix_sort_hist) while it writes the keys: begin clears the
 // scratch, finish sorts.  With cell_count (zeroed by the caller), the last pass also
