@@ -726,21 +726,26 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
         // move the individuals, then new fields and a new time step of that direction
         // Both sweeps go out before the host waits: the y sweep takes the time step
         // known before this call, so the x sweep's results are read with its own.
+        // A sweep that fails to go out stops the loop, but a sweep already out is still
+        // booked (its departures and time step), so the list stays consistent.
         h->sim_time = t;
         bool swept[2] = {false, false};
+        int rc_launch = GPGMP_OK;
         for (int dir = 0; dir < 2; ++dir) {
             if (!((dir == 0 ? h->nextX[i] : h->nextY[i]) <= t)) continue;
             const float dd = dir == 0 ? h->ddX[i] : h->ddY[i];
             const float dxd = h->m.physical_length / (float)(dir == 0 ? h->m.width : h->m.height);
-            int rc = ind_sweep(h->ind[i], ind_args(h, i, dir, dd, (uint32_t)*seed), h->ind_k, dxd, h->ts_kind, h->stay,
-                               dir, h->stream);
-            if (rc) return rc;
+            rc_launch = ind_sweep(h->ind[i], ind_args(h, i, dir, dd, (uint32_t)*seed), h->ind_k, dxd, h->ts_kind,
+                                  h->stay, dir, h->stream);
+            if (rc_launch) break;
             (*seed)++;
             swept[dir] = true;
         }
         if (swept[0] || swept[1]) {
             cudaError_t e = cudaStreamSynchronize(h->stream);
-            if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "individual sweeps: %s", cudaGetErrorString(e));
+            if (e != cudaSuccess)
+                return rc_launch ? rc_launch
+                                 : set_error(GPGMP_ERR_CUDA, "individual sweeps: %s", cudaGetErrorString(e));
         }
         for (int dir = 0; dir < 2; ++dir) {
             if (!swept[dir]) continue;
@@ -750,7 +755,7 @@ int gpgmp_diffuse(gpgmp_solver* h, int32_t i, float t, int32_t* seed) {
             (dir == 0 ? h->ddX[i] : h->ddY[i]) = small;
         }
         h->next[i] = h->nextX[i] < h->nextY[i] ? h->nextX[i] : h->nextY[i];
-        return GPGMP_OK;
+        return rc_launch;
     }
     if (h->nextX[i] <= t) {
         const int c = h->cur[i];
