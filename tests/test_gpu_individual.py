@@ -37,7 +37,7 @@ def test_exclusive_scan_bit_exact(gpgmp, n):
 
 @pytest.mark.parametrize("n,bits", [(1, 32), (3839, 8), (3841, 20), (65536, 32), (1_000_003, 21), (1 << 22, 20),
                                     (7681, 10), (200_000, 16), (200_001, 17), (777_777, 26), (123_457, 30),
-                                    (1 << 20, 24)])
+                                    (1 << 20, 24), (7680, 20), (2 * 7680 + 1, 20), (7680, 8)])
 def test_sort_pairs_stable_bit_exact(gpgmp, n, bits):
     from inchman_b200 import individual as ind
     rng = np.random.default_rng(bits + n)
@@ -152,3 +152,35 @@ def test_particle_bins_follow_the_step(gpgmp, clustered):
     assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
     assert np.array_equal(keys, cells.astype(np.uint32))
     assert np.array_equal(np.sort(idx), np.arange(n, dtype=np.uint32))
+
+
+@pytest.mark.parametrize("case", ["empty", "single", "all_a", "no_reaction", "full_reaction"])
+def test_particle_step_edge_cases(gpgmp, case):
+    """Edge cases of the particle step against the oracle: no particles, one particle,
+    one species only (no pairs), p = 0 (everyone stays) and p = 1."""
+    from inchman_b200 import individual as ind
+    grid, steps = 64, 3
+    n = {"empty": 0, "single": 1}.get(case, 5000)
+    rng = np.random.default_rng(23)
+    x = rng.uniform(0.0, grid, n).astype(np.float32)
+    y = rng.uniform(0.0, grid, n).astype(np.float32)
+    sp = (np.zeros(n) if case == "all_a" else rng.integers(0, 2, n)).astype(np.uint8)
+    p_react = {"no_reaction": 0.0, "full_reaction": 1.0}.get(case, 0.3)
+    p = ind.Particles(max(n, 1), grid, D=0.4, vx=0.05, vy=0.02, dt=1.0, p_react=p_react, seed=7)
+    p.set(x, y, sp, step=0)
+    p.step(steps)
+    gx, gy, gsp = p.get()
+    assert p.status() == 0
+    ox, oy, osp = x.copy(), y.copy(), sp.copy()
+    m = oracle.orc().orc_particles_run(n, oracle.ptr(ox), oracle.ptr(oy), oracle.ptr(osp), grid, 0.4, 0.05, 0.02,
+                                       1.0, p_react, 7, 0, steps) if n else 0
+    assert len(gx) == m
+    assert np.array_equal(gx, ox[:m]) and np.array_equal(gy, oy[:m]) and np.array_equal(gsp, osp[:m])
+    if case in ("all_a", "no_reaction"):
+        assert m == n
+    # the last step's bins hold the particles it started with
+    start, count, _, _ = p.bins()
+    assert int(count.sum()) >= len(gx)
+    if case in ("all_a", "no_reaction", "empty", "single"):
+        assert int(count.sum()) == len(gx)
+    assert np.array_equal(start, (np.cumsum(count) - count).astype(np.uint32))
