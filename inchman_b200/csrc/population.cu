@@ -63,6 +63,14 @@ struct PopHeader {
 };
 static_assert(sizeof(PopHeader) == 64, "header size");
 
+// one thread's pinned landing place for the 64-byte header readback
+struct PinnedHeader {
+    PopHeader* p = nullptr;
+    ~PinnedHeader() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
 // what the move kernel needs about one cell, in one 16-byte load
 struct __align__(16) CellPlan {
     uint32_t surv_base;   // new position of the cell's first survivor: new start + births
@@ -456,9 +464,18 @@ int population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n_act
                                                          seed, step, new_start, birth_off, plan, keys_out, ids_out,
                                                          cap_out, pool_out, cap_pool, head);
     CK(cudaGetLastError());
-    PopHeader h;
-    CK(cudaMemcpyAsync(&h, head, sizeof h, cudaMemcpyDeviceToHost, st));
+    // the header comes back into this thread's pinned copy (a plain async copy, no
+    // staging through a pageable buffer); a call returns only after its copy landed
+    thread_local PinnedHeader t_pinned;
+    if (!t_pinned.p && cudaMallocHost((void**)&t_pinned.p, sizeof(PopHeader)) != cudaSuccess) {
+        cudaGetLastError();
+        t_pinned.p = nullptr;
+    }
+    PopHeader h_stack;
+    PopHeader* hp = t_pinned.p ? t_pinned.p : &h_stack;
+    CK(cudaMemcpyAsync(hp, head, sizeof(PopHeader), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    const PopHeader h = *hp;
     if (h.lookback_err) return set_error(GPGMP_ERR_TIMEOUT, "a scan's look-back wait gave up");
     const int64_t n_new = (int64_t)h.goal_total, B = h.totals[1], K = h.totals[2];
     if (h.check == kPopShortPool)

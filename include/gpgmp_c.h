@@ -329,7 +329,8 @@ int gpgmp_scratch_status(const void* scratch, int32_t kind, int64_t n, int32_t k
  * Outputs: keys_out / ids_out (n_active_out entries, at most capacity_out), pool_out
  * (n_pool_out ids, at most pool_capacity), start_out (optional, ncells entries: the
  * new cell starts; the new counts are goal).  Device pointers; returns after the
- * work is done (the totals are read back).  GPGMP_ERR_INVALID when the pool has
+ * work is done (the totals are read back, into a 64-byte pinned host buffer that the
+ * calling thread's first call allocates).  GPGMP_ERR_INVALID when the pool has
  * fewer free ids than births or an output is too small. */
 int gpgmp_population_scratch_bytes(int64_t n_active, int64_t ncells, size_t* bytes);
 int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t n_active,
