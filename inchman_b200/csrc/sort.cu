@@ -458,12 +458,13 @@ SortLayout sort_layout(int64_t n, int key_bits) {
     // 10-bit digits where they save a pass (17-20 and 25-30 key bits)
     L.digit_bits = (key_bits > 16 && key_bits <= 30 && p10 < p8) ? 10 : 8;
     L.passes = L.digit_bits == 10 ? p10 : p8;
-    const size_t dig = (size_t)1 << L.digit_bits;
     L.tiles = (n + kSortTile - 1) / kSortTile;
     size_t off = 0;
     L.off_hist = off;    off += align256(sizeof(uint32_t) * kHistWords);
     L.off_counters = off; off += align256(sizeof(uint32_t) * 8);     // tile counters [4], error word [4]
-    L.off_look = off;    off += align256(sizeof(uint32_t) * dig * (size_t)(L.tiles > 0 ? L.tiles : 1) * L.passes);
+    // look-back words for the widest layout (3 passes x 1024 digits >= 4 x 256), so that
+    // the scratch size does not depend on key_bits
+    L.off_look = off;    off += align256(sizeof(uint32_t) * kHistWords * (size_t)(L.tiles > 0 ? L.tiles : 1));
     L.off_alt_keys = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.off_alt_vals = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.bytes = off;

@@ -302,6 +302,7 @@ int gpgmp_scan_scratch_bytes(int64_t n, size_t* bytes);
 /* out[i] = in[0] + ... + in[i-1] (mod 2^32); out[0] = 0 */
 int gpgmp_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, size_t scratch_bytes,
                              void* stream);
+/* the sort's scratch size depends on n only: one buffer serves every key_bits */
 int gpgmp_sort_scratch_bytes(int64_t n, int32_t key_bits, size_t* bytes);
 /* stable sort of (key, value) by the low key_bits bits of key; n < 2^30; in and out
  * must not overlap */

@@ -30,6 +30,20 @@ def test_library_exports_every_declared_symbol(gpgmp):
     assert not missing, missing
 
 
+def test_sort_scratch_size_does_not_depend_on_key_bits(gpgmp):
+    """One scratch buffer serves a sort of any key width (8- and 10-bit digit layouts
+    alike), so a caller may size it once for n."""
+    from inchman_b200 import _lib
+    L = _lib.lib()
+    for n in (1, 7680, 7681, 1 << 22):
+        sizes = set()
+        for bits in range(1, 33):
+            b = C.c_size_t(0)
+            assert L.gpgmp_sort_scratch_bytes(C.c_int64(n), C.c_int32(bits), C.byref(b)) == 0
+            sizes.add(b.value)
+        assert len(sizes) == 1, (n, sizes)
+
+
 def test_error_path_without_gpu(gpgmp):
     """Argument errors come back as codes with a message, never as a crash or exit."""
     from inchman_b200 import _lib
