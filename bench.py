@@ -9,7 +9,7 @@ region); adjoint_forward_ratio = time of the gradient (adjoint with checkpointin
 recomputation included) over the time of one forward solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload gray_scott|ssa_plain|lotka_volterra|ensemble|particles|population|individuals]
+                    [--workload gray_scott|ssa_plain|lotka_volterra|ensemble|particles|population|individuals|scan_sort]
 
 Multi-GPU: every rank runs its own replica (the path does not shard: replicas
 only); value = total cell-steps of all ranks / max over ranks of the time.

@@ -37,9 +37,18 @@ constexpr int kScanTile = kScanThreads * kScanItems;   // 4096
 // ---- exclusive scan ------------------------------------------------------------
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
 // (flag << 32) | value, flag 0 = not ready, 1 = tile aggregate, 2 = inclusive prefix.
+// A thread scans 16 consecutive values.  A full tile whose pointers are 16-byte
+// aligned (vec) moves through shared memory: warp-contiguous 16-byte loads and stores
+// (every HBM request coalesced), one uint4 of padding per eight so that the threads'
+// 64-byte rows read and write without bank conflicts.  The last, partial tile and
+// unaligned pointers take plain loads and stores.
+constexpr int kScanQuads = kScanTile / 4;                 // uint4 per tile
+__device__ __forceinline__ int scan_pad(int i4) { return i4 + (i4 >> 3); }
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t* __restrict__ in,
                                                                  uint32_t* __restrict__ out, int64_t n,
-                                                                 uint64_t* __restrict__ scratch) {
+                                                                 uint64_t* __restrict__ scratch, int vec) {
+    __shared__ uint4 s_io[kScanQuads + kScanQuads / 8];
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[kScanThreads / 32];
     __shared__ uint32_t s_prefix;
@@ -49,13 +58,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    const int64_t tbase = (int64_t)tile * kScanTile;
+    const bool full = vec && tbase + kScanTile <= n;    // the same in every thread of the block
+    const int64_t base = tbase + (int64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    if (base + kScanItems <= n) {
-        const uint4* p = reinterpret_cast<const uint4*>(in + base);
+    if (full) {
+        const uint4* src = reinterpret_cast<const uint4*>(in + tbase);
 #pragma unroll
         for (int q = 0; q < kScanItems / 4; ++q) {
-            uint4 w = p[q];
+            const int i4 = q * kScanThreads + threadIdx.x;
+            s_io[scan_pad(i4)] = src[i4];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const uint4 w = s_io[scan_pad(threadIdx.x * (kScanItems / 4) + q)];
             v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
         }
     } else {
@@ -95,8 +112,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
     }
     __syncthreads();
     uint32_t run = s_prefix + thread_excl;
-    if (base + kScanItems <= n) {
-        uint4* p = reinterpret_cast<uint4*>(out + base);
+    if (full) {
+        // every thread read its inputs from s_io before the barriers above
 #pragma unroll
         for (int q = 0; q < kScanItems / 4; ++q) {
             uint4 w;
@@ -104,7 +121,14 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
             w.y = run; run += v[4 * q + 1];
             w.z = run; run += v[4 * q + 2];
             w.w = run; run += v[4 * q + 3];
-            p[q] = w;
+            s_io[scan_pad(threadIdx.x * (kScanItems / 4) + q)] = w;
+        }
+        __syncthreads();
+        uint4* dst = reinterpret_cast<uint4*>(out + tbase);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const int i4 = q * kScanThreads + threadIdx.x;
+            dst[i4] = s_io[scan_pad(i4)];
         }
     } else {
 #pragma unroll
@@ -444,7 +468,8 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, voi
     const int64_t tiles = (n + kScanTile - 1) / kScanTile;
     cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st);
     if (e != cudaSuccess) return e;
-    k_scan_exclusive<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, (uint64_t*)scratch);
+    const int vec = (((uintptr_t)in | (uintptr_t)out) & 15u) == 0 ? 1 : 0;
+    k_scan_exclusive<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, (uint64_t*)scratch, vec);
     return cudaGetLastError();
 }
 

@@ -366,9 +366,67 @@ def _peaks():
     return load_peaks()
 
 
+def scan_sort(args, rank, world):
+    """The individual-particle primitives on their own, through the C ABI: exclusive
+    scan of 2^27 uint32 values (512 MB in, 512 MB out: larger than L2, so no flush is
+    needed between calls) and stable sorts of 2^24 (key, value) pairs with 20-bit keys
+    (two 10-bit passes) and 32-bit keys (four 8-bit passes).  Unit of the line's value:
+    scanned values/s; the sorts are reported beside it in keys/s.
+
+    Roofline (scan): 8 B per value (read, write); (sort) 16 B per key and pass (read
+    key and value, write key and value)."""
+    import torch
+    from . import individual as ind
+    dev = "cuda"
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234)
+    n = 1 << 27
+    x = torch.randint(0, 16, (n,), dtype=torch.int32, device=dev, generator=gen)
+    out = torch.empty_like(x)
+    scr = ind.scan_scratch(n)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = _events()
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3 / args.steps
+
+    t_scan = timed(lambda: ind._call("gpgmp_exclusive_scan_u32", ind._ptr(x), ind._ptr(out), n, ind._ptr(scr),
+                                     scr.numel(), ind._stream()))
+    peak, peak_kind = _peaks()
+    ns = 1 << 24
+    sorts = {}
+    for bits, passes in ((20, 2), (32, 4)):
+        k = torch.randint(0, 1 << bits, (ns,), dtype=torch.int64, device=dev, generator=gen).to(torch.int32)
+        v = torch.arange(ns, dtype=torch.int32, device=dev)
+        ko, vo = torch.empty_like(k), torch.empty_like(v)
+        sscr = ind.sort_scratch(ns, bits)
+        t = timed(lambda: ind._call("gpgmp_sort_pairs_u32", ind._ptr(k), ind._ptr(v), ind._ptr(ko), ind._ptr(vo), ns,
+                                    bits, ind._ptr(sscr), sscr.numel(), ind._stream()))
+        ach = 16.0 * passes * ns / t / 1e9
+        sorts[f"keys_{bits}bit"] = {"pairs": ns, "passes": passes, "ms_per_sort": t * 1e3, "keys_per_s": ns / t,
+                                    "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                                                 "frac": ach / peak, "peak_kind": peak_kind}}
+        del k, v, ko, vo, sscr
+    ach = 8.0 * n / t_scan / 1e9
+    return _base(args, world, n / t_scan, "values/s", "scan_2^27_u32_sort_2^24_pairs",
+                 {"scan_values": n, "sort_pairs": ns, "l2": "inputs larger than L2 (scan)"}, t_scan * 1e3,
+                 {"dtype": "u32", "sorts": sorts,
+                  # per timed scan: one scan kernel; per sort: histogram + one kernel per pass
+                  "gpu_launches": args.steps * (1 + (1 + 2) + (1 + 4)),
+                  "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                               "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_scan": 8 * n}})
+
+
 def run(args, rank, world):
     table = {"ssa_plain": ssa_plain, "lotka_volterra": lotka_volterra, "particles": particles,
-             "ensemble": ensemble, "population": population, "individuals": individuals}
+             "ensemble": ensemble, "population": population, "individuals": individuals, "scan_sort": scan_sort}
     if args.workload not in table:
         raise SystemExit(f"unknown workload {args.workload}; one of gray_scott, {', '.join(table)}")
     return table[args.workload](args, rank, world)

@@ -18,7 +18,7 @@ def _np(t):
     return t.cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("n", [0, 1, 5, 4095, 4096, 4097, 100_003, 1 << 22])
+@pytest.mark.parametrize("n", [0, 1, 5, 4095, 4096, 4097, 8192, 100_003, 1 << 22, 1 << 26])
 def test_exclusive_scan_bit_exact(gpgmp, n):
     from inchman_b200 import individual as ind
     rng = np.random.default_rng(n)
@@ -33,6 +33,22 @@ def test_exclusive_scan_bit_exact(gpgmp, n):
     got = _np(ind.exclusive_scan_u32(_t(x), scratch))
     assert np.array_equal(got, want)
     assert ind.scratch_status(scratch, 0) == 0
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3])
+def test_exclusive_scan_of_an_unaligned_view(gpgmp, offset):
+    """Input that starts 4, 8 or 12 bytes past a 16-byte boundary (a slice of a larger
+    buffer) is scanned element by element, with the same result."""
+    from inchman_b200 import individual as ind
+    n = 3 * 4096 + 17
+    rng = np.random.default_rng(offset)
+    x = rng.integers(0, 2**32, size=n + offset, dtype=np.uint64).astype(np.uint32)
+    want = np.zeros(n, np.uint32)
+    oracle.orc().orc_exclusive_scan_u32(oracle.ptr(np.ascontiguousarray(x[offset:])), oracle.ptr(want), n)
+    view = _t(x)[offset:]
+    assert view.data_ptr() % 16 != 0
+    got = _np(ind.exclusive_scan_u32(view, ind.scan_scratch(n)))
+    assert np.array_equal(got, want)
 
 
 @pytest.mark.parametrize("n,bits", [(1, 32), (3839, 8), (3841, 20), (65536, 32), (1_000_003, 21), (1 << 22, 20),
