@@ -31,8 +31,8 @@ namespace gpgmp {
 namespace {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kScanTile = kScanThreads * kScanItems;   // 4096
+constexpr int kScanItems = 32;
+constexpr int kScanTile = kScanThreads * kScanItems;   // 8192
 
 // ---- exclusive scan ------------------------------------------------------------
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
@@ -587,9 +587,9 @@ cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t
 
 // ---- exclusive scan without allocation -----------------------------------------
 // For callers that must not call cudaMalloc: the scan's scratch (tile counter,
-// error word, one status word per 4096-value tile) lives in a fixed file-scope
+// error word, one status word per 8192-value tile) lives in a fixed file-scope
 // device array instead of a caller buffer.  Every device that loads this library
-// holds the array (128 KiB) until the process exits; it serves scans of up to
+// holds the array (64 KiB) until the process exits; it serves scans of up to
 // kNoAllocMaxN values.
 namespace gpgmp {
 namespace {
