@@ -30,14 +30,15 @@
 namespace gpgmp {
 namespace {
 
-constexpr int kScanThreads = 256;
+constexpr int kScanThreads = 512;
 constexpr int kScanItems = 32;
-constexpr int kScanTile = kScanThreads * kScanItems;   // 8192
+constexpr int kScanTile = kScanThreads * kScanItems;   // 16384
 
 // ---- exclusive scan ------------------------------------------------------------
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
 // (flag << 32) | value, flag 0 = not ready, 1 = tile aggregate, 2 = inclusive prefix.
-// A thread scans 16 consecutive values.  A full tile whose pointers are 16-byte
+// A tile is 512 threads x 32 consecutive values (16384: fewer tiles, a shorter
+// look-back chain).  A full tile whose pointers are 16-byte
 // aligned (vec) moves through shared memory: warp-contiguous 16-byte loads and stores
 // (every HBM request coalesced), one uint4 of padding per eight so that the threads'
 // 64-byte rows read and write without bank conflicts.  The last, partial tile and
@@ -48,7 +49,7 @@ __device__ __forceinline__ int scan_pad(int i4) { return i4 + (i4 >> 3); }
 __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t* __restrict__ in,
                                                                  uint32_t* __restrict__ out, int64_t n,
                                                                  uint64_t* __restrict__ scratch, int vec) {
-    __shared__ uint4 s_io[kScanQuads + kScanQuads / 8];
+    extern __shared__ uint4 s_io[];   // kScanQuads + kScanQuads / 8 (dynamic: 72 KB)
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[kScanThreads / 32];
     __shared__ uint32_t s_prefix;
@@ -469,7 +470,10 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, voi
     cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st);
     if (e != cudaSuccess) return e;
     const int vec = (((uintptr_t)in | (uintptr_t)out) & 15u) == 0 ? 1 : 0;
-    k_scan_exclusive<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, (uint64_t*)scratch, vec);
+    const int smem = (int)(sizeof(uint4) * (kScanQuads + kScanQuads / 8));
+    e = cudaFuncSetAttribute(k_scan_exclusive, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    k_scan_exclusive<<<(unsigned)tiles, kScanThreads, smem, st>>>(in, out, n, (uint64_t*)scratch, vec);
     return cudaGetLastError();
 }
 
@@ -587,9 +591,9 @@ cudaError_t left_right_u32(const uint32_t* start, const uint32_t* count, int64_t
 
 // ---- exclusive scan without allocation -----------------------------------------
 // For callers that must not call cudaMalloc: the scan's scratch (tile counter,
-// error word, one status word per 8192-value tile) lives in a fixed file-scope
+// error word, one status word per 16384-value tile) lives in a fixed file-scope
 // device array instead of a caller buffer.  Every device that loads this library
-// holds the array (64 KiB) until the process exits; it serves scans of up to
+// holds the array (32 KiB) until the process exits; it serves scans of up to
 // kNoAllocMaxN values.
 namespace gpgmp {
 namespace {

@@ -344,7 +344,7 @@ int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t
  * whose device memory is owned and accounted by another allocator (a framework's
  * memory pool), or that cannot take cudaMalloc's implicit synchronisation or its
  * failure in the middle of a time loop.  No counterpart in the reference.  The
- * scratch is a fixed 64 KiB device array inside the library, so n is at most
+ * scratch is a fixed 32 KiB device array inside the library, so n is at most
  * 2^26 (67,108,864) values; larger n is rejected with GPGMP_ERR_INVALID.  The first
  * call on each device looks the array up (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  Every call on a device
