@@ -38,11 +38,11 @@ constexpr int kScanTile = kScanThreads * kScanItems;   // 16384
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
 // (flag << 32) | value, flag 0 = not ready, 1 = tile aggregate, 2 = inclusive prefix.
 // A tile is 512 threads x 32 consecutive values (16384: fewer tiles, a shorter
-// look-back chain).  A full tile whose pointers are 16-byte
-// aligned (vec) moves through shared memory: warp-contiguous 16-byte loads and stores
-// (every HBM request coalesced), one uint4 of padding per eight so that the threads'
-// 64-byte rows read and write without bank conflicts.  The last, partial tile and
-// unaligned pointers take plain loads and stores.
+// look-back chain).  A full tile whose pointers are 16-byte aligned (vec) moves
+// through shared memory: warp-contiguous 16-byte loads and stores (every HBM request
+// coalesced), one uint4 of padding per eight so that the threads' 128-byte rows read
+// and write without bank conflicts.  The last, partial tile and unaligned pointers
+// take plain loads and stores.
 constexpr int kScanQuads = kScanTile / 4;                 // uint4 per tile
 __device__ __forceinline__ int scan_pad(int i4) { return i4 + (i4 >> 3); }
 
