@@ -637,8 +637,26 @@ extern "C" int gpgmp_exclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* ou
     void* scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;
-    // zeroes the counter and the status words this scan uses, then scans
+    // zeroes the counter, the error word and the status words this scan uses, then scans
     cudaError_t e = scan_exclusive_u32(in, out, n, scratch, (cudaStream_t)stream);
     if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "scan: %s", cudaGetErrorString(e));
+    return GPGMP_OK;
+}
+
+// Waits for `stream` and reads the error word of the built-in scratch: GPGMP_ERR_TIMEOUT
+// in *status when the last scan's look-back gave up (its output is then wrong).  The
+// next no-allocation scan clears the word, so this is read before it.
+extern "C" int gpgmp_exclusive_scan_u32_noalloc_status(void* stream, int32_t* status) {
+    using namespace gpgmp;
+    if (!status) return set_error(GPGMP_ERR_INVALID, "bad argument");
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "cudaStreamSynchronize: %s", cudaGetErrorString(e));
+    uint32_t word = 0;
+    e = cudaMemcpy(&word, (const char*)scratch + scan_error_flag_offset(), sizeof(word), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return set_error(GPGMP_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
+    *status = word ? GPGMP_ERR_TIMEOUT : GPGMP_OK;
     return GPGMP_OK;
 }

@@ -7,7 +7,7 @@
 namespace gpgmp {
 
 // scratch of one exclusive scan of n values: a tile counter, an error word and one
-// status word per 4096-value tile; the error word sits at byte scan_error_flag_offset()
+// status word per kScanTile (16384) values; the error word sits at byte scan_error_flag_offset()
 size_t scan_scratch_bytes(int64_t n);
 int scan_error_flag_offset();
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, void* scratch, cudaStream_t st);

@@ -18,7 +18,8 @@ def _np(t):
     return t.cpu().numpy().view(np.uint32)
 
 
-@pytest.mark.parametrize("n", [0, 1, 5, 4095, 4096, 4097, 8192, 100_003, 1 << 22, 1 << 26])
+@pytest.mark.parametrize("n", [0, 1, 5, 4095, 4096, 4097, 8192, 16383, 16384, 16385, 2 * 16384 + 1, 100_003,
+                               1 << 22, 1 << 26])
 def test_exclusive_scan_bit_exact(gpgmp, n):
     from inchman_b200 import individual as ind
     rng = np.random.default_rng(n)
@@ -38,9 +39,10 @@ def test_exclusive_scan_bit_exact(gpgmp, n):
 @pytest.mark.parametrize("offset", [1, 2, 3])
 def test_exclusive_scan_of_an_unaligned_view(gpgmp, offset):
     """Input that starts 4, 8 or 12 bytes past a 16-byte boundary (a slice of a larger
-    buffer) is scanned element by element, with the same result."""
+    buffer) is scanned element by element, with the same result; several 16384-value
+    tiles take that path, so the look-back between them is crossed too."""
     from inchman_b200 import individual as ind
-    n = 3 * 4096 + 17
+    n = 3 * 16384 + 17
     rng = np.random.default_rng(offset)
     x = rng.integers(0, 2**32, size=n + offset, dtype=np.uint64).astype(np.uint32)
     want = np.zeros(n, np.uint32)
