@@ -83,6 +83,7 @@ class ModelDesc(C.Structure):
         ("num_fields", C.c_int32),
         ("field_values", C.POINTER(C.c_float)),
         ("set_field_code", C.c_char_p),
+        ("reaction_mask", C.POINTER(C.c_uint8)),
     ]
 
 

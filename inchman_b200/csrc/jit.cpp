@@ -186,7 +186,8 @@ int jit_ssa_kernel(const std::string& defines, const std::vector<std::string>& l
       << "struct JitPlanes { int* p[" << kMaxSpecies << "]; };\n"
       << "extern \"C\" __global__ void __launch_bounds__(" << kJitSsaThreads << ")\n"
       << "gpgmp_jit_ssa(JitPlanes planes, int S, int area, int R, const gpgmp_reaction* __restrict__ reactions,\n"
-      << "              int nreac, unsigned seed, unsigned step_seed, float window, int* __restrict__ status) {\n"
+      << "              int nreac, unsigned seed, unsigned step_seed, float window, int* __restrict__ status,\n"
+      << "              const unsigned* __restrict__ rmask, int rmask_words) {\n"
       << "  using namespace gpgmp;\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
       << "  gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);\n"
@@ -202,7 +203,15 @@ int jit_ssa_kernel(const std::string& defines, const std::vector<std::string>& l
       << "  for (int s = 0; s < S; ++s) x[s * " << kJitSsaThreads << "] = planes.p[s][((int64_t)r * S + s) * area + c];\n"
       << "  Stream st;\n"
       << "  st.init(seed, (uint32_t)r, step_seed, (uint32_t)c, PH_SSA);\n"
-      << "  const int e = ssa_cell_h(rt, nreac, x, " << kJitSsaThreads << ", st, window, ModelHazard{});\n"
+      << "  int e;\n"
+      << "  if (rmask) {\n"
+      << "    CellReactions on;\n"
+      << "    on.load(rmask, rmask_words, area, c);\n"
+      << "    e = ssa_cell_h(rt, nreac, x, " << kJitSsaThreads
+      << ", st, window, GatedHazard<ModelHazard>{ModelHazard{}, on});\n"
+      << "  } else {\n"
+      << "    e = ssa_cell_h(rt, nreac, x, " << kJitSsaThreads << ", st, window, ModelHazard{});\n"
+      << "  }\n"
       << "  for (int s = 0; s < S; ++s) planes.p[s][((int64_t)r * S + s) * area + c] = x[s * " << kJitSsaThreads
       << "];\n"
       << "  if (e) atomicOr(&status[r], e);\n"
@@ -223,7 +232,10 @@ cudaError_t launch_ssa_jit(JitFunction fn, const GridDesc& g, Planes planes, con
     const int64_t total = (int64_t)R * area;
     const unsigned blocks = (unsigned)((total + kJitSsaThreads - 1) / kJitSsaThreads);
     const unsigned smem = (unsigned)(sizeof(gpgmp_reaction) * nreac + sizeof(int) * S * kJitSsaThreads);
-    void* args[] = {&planes, &S, &area, &R, (void*)&d_reactions, &nreac, &seed, &step_seed, &window, &d_status};
+    const uint32_t* rmask = g.rmask;
+    int rmask_words = g.rmask_words;
+    void* args[] = {&planes, &S,        &area,      &R,          (void*)&d_reactions, &nreac, &seed, &step_seed,
+                    &window, &d_status, (void*)&rmask, &rmask_words};
     std::lock_guard<std::mutex> lk(g_mu);
     return launch((CUfunction)fn, blocks, kJitSsaThreads, smem, st, args);
 }

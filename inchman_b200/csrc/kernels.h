@@ -21,6 +21,10 @@ struct FPlanes {
 struct GridDesc {
     int W, H, S, R;          // grid, species, realisations
     int bmask[4];
+    // localised reactions: [rmask_words][W * H] bits, bit r % 32 of word r / 32 of a
+    // cell set where reaction r may fire; NULL when every reaction fires everywhere
+    const uint32_t* rmask;
+    int rmask_words;
 };
 
 cudaError_t launch_init_poisson(const GridDesc& g, Planes planes, uint32_t seed, const float* d_lambda,

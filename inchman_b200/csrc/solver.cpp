@@ -47,6 +47,7 @@ struct gpgmp_solver {
     float* d_fbuf[2] = {nullptr, nullptr};
     int fcur = 0;
     gpgmp_reaction* d_reactions = nullptr;
+    uint32_t* d_rmask = nullptr;      // localised reactions: [words][area] bits (GridDesc::rmask), or NULL
     int32_t* d_status = nullptr;
     float* d_diff = nullptr;
     float *d_Dx = nullptr, *d_Dy = nullptr, *d_rx = nullptr, *d_ry = nullptr;
@@ -149,7 +150,7 @@ int normalize(gpgmp_solver* h) {
 void free_all(gpgmp_solver* h) {
     void* ptrs[] = {h->d_buf[0], h->d_buf[1], h->d_fbuf[0], h->d_fbuf[1], h->d_reactions, h->d_status, h->d_diff,
                     h->d_Dx, h->d_Dy, h->d_rx, h->d_ry, h->d_minkey, h->d_lambda, h->d_stage, h->d_meanx,
-                    h->d_msums, h->d_fields};
+                    h->d_msums, h->d_fields, h->d_rmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (IndList& l : h->ind) ind_free(l);
@@ -437,6 +438,7 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
     h->m.new_individuals_code = nullptr;
     h->m.field_values = nullptr;
     h->m.set_field_code = nullptr;
+    h->m.reaction_mask = nullptr;
     if (any_ind) {
         h->ind.resize(model->num_species);
         for (int s = 0; s < model->num_species; ++s) h->ind[s].species = h->is_ind[s] ? s : -1;
@@ -528,6 +530,25 @@ int gpgmp_solver_create(const gpgmp_model_desc* model, int32_t num_realisations,
         CKC(cudaMalloc(&h->d_reactions, sizeof(gpgmp_reaction) * h->reactions.size()));
         CKC(cudaMemcpy(h->d_reactions, h->reactions.data(), sizeof(gpgmp_reaction) * h->reactions.size(),
                        cudaMemcpyHostToDevice));
+    }
+    if (model->reaction_mask && !h->reactions.empty()) {
+        // localised reactions (Solver.cpp:352-390 builds the same mask as a float image):
+        // one bit per reaction and cell, 32 reactions to a word, words cell-contiguous
+        const int nr = (int)h->reactions.size(), words = (nr + 31) / 32;
+        std::vector<uint32_t> bits((size_t)words * h->area, 0u);
+        bool all_on = true;
+        for (int r = 0; r < nr; ++r)
+            for (size_t c = 0; c < h->area; ++c) {
+                const bool on = model->reaction_mask[(size_t)r * h->area + c] != 0;
+                all_on = all_on && on;
+                if (on) bits[(size_t)(r >> 5) * h->area + c] |= 1u << (r & 31);
+            }
+        if (!all_on) {    // a mask that is on everywhere changes nothing: no masked kernels
+            CKC(cudaMalloc(&h->d_rmask, sizeof(uint32_t) * bits.size()));
+            CKC(cudaMemcpy(h->d_rmask, bits.data(), sizeof(uint32_t) * bits.size(), cudaMemcpyHostToDevice));
+            h->g.rmask = h->d_rmask;
+            h->g.rmask_words = words;
+        }
     }
     // stay probability and jump probability as the reference's header computes them
     const float stay = (float)(1.0 - (double)model->p0);

@@ -40,6 +40,31 @@ struct MassActionHazard {
     }
 };
 
+// Localised reactions: bit r of on[r / 32] says whether reaction r may fire in this
+// cell (Reaction::reactionMask, Reaction.cpp:216-235).  The reference multiplies the
+// law by the mask value 1 or 0 (Solver.cpp:852-854); a zero hazard is the same sum.
+struct CellReactions {
+    uint32_t on[4];
+    // rmask: [words][area] bits of the cells (words = ceil(reactions / 32)); NULL: all on
+    __device__ __forceinline__ void load(const uint32_t* __restrict__ rmask, int words, int area, int c) {
+        on[0] = on[1] = on[2] = on[3] = 0xFFFFFFFFu;
+        if (rmask)
+            for (int w = 0; w < words; ++w) on[w] = rmask[(int64_t)w * area + c];
+    }
+    __device__ __forceinline__ bool operator()(int r) const { return (on[r >> 5] >> (r & 31)) & 1u; }
+};
+struct AllReactions {
+    __device__ __forceinline__ bool operator()(int) const { return true; }
+};
+template <class HZ>
+struct GatedHazard {
+    HZ hz;
+    CellReactions on;
+    __device__ __forceinline__ float operator()(const gpgmp_reaction* rt, int r, const int* x, int stride) const {
+        return on(r) ? hz(rt, r, x, stride) : 0.0f;
+    }
+};
+
 // Runs one SSA window on the counts x[s * stride]; returns a GPGMP_SIM_* bit or 0.
 template <class HZ>
 __device__ __forceinline__ int ssa_cell_h(const gpgmp_reaction* rt, int R, int* x, int stride, Stream& st,
@@ -106,9 +131,11 @@ __device__ __forceinline__ void build_deps(const gpgmp_reaction* rt, int R, uint
 // and recomputed only where the fired reaction changed a reactant count.  The total
 // and the selection sum the same values in the same order as the full recomputation,
 // so the result is bit-identical.
+// ON(r) gates the reactions of localised models (CellReactions), as in ssa_cell_h.
+template <class ON = AllReactions>
 __device__ __forceinline__ int ssa_cell_inc(const gpgmp_reaction* rt, const uint32_t* deps, int R, int* x, int stride,
-                                            float* h, Stream& st, float window) {
-    for (int r = 0; r < R; ++r) h[r * stride] = hazard(rt[r], x, stride);
+                                            float* h, Stream& st, float window, const ON& on = ON{}) {
+    for (int r = 0; r < R; ++r) h[r * stride] = on(r) ? hazard(rt[r], x, stride) : 0.0f;
     float t = 0.0f;
     int events = 0;
     for (;;) {
@@ -138,7 +165,7 @@ __device__ __forceinline__ int ssa_cell_inc(const gpgmp_reaction* rt, const uint
                 while (m) {
                     const int q = w * 32 + __ffs(m) - 1;
                     m &= m - 1;
-                    h[q * stride] = hazard(rt[q], x, stride);
+                    h[q * stride] = on(q) ? hazard(rt[q], x, stride) : 0.0f;
                 }
             }
         }

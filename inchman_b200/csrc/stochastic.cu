@@ -29,10 +29,14 @@ __global__ void k_init_poisson(Planes planes, int S, int area, int R, uint32_t s
     }
 }
 
+// MASKED: localised reactions, rmask as GridDesc::rmask (the unmasked form is the
+// same code with every reaction on)
+template <bool MASKED>
 __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int area, int R,
                                                      const gpgmp_reaction* __restrict__ reactions, int nreac,
                                                      uint32_t seed, uint32_t step_seed, float window,
-                                                     int32_t* __restrict__ status) {
+                                                     int32_t* __restrict__ status,
+                                                     const uint32_t* __restrict__ rmask, int rmask_words) {
     extern __shared__ __align__(16) unsigned char smem[];
     gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
     uint32_t* deps = reinterpret_cast<uint32_t*>(smem + sizeof(gpgmp_reaction) * nreac);
@@ -51,8 +55,17 @@ __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int a
     Stream st;
     st.init(seed, (uint32_t)r, step_seed, (uint32_t)c, PH_SSA);
     // both forms give the same bits; the incremental one pays off for larger networks
-    const int e = nreac > kIncMinReactions ? ssa_cell_inc(rt, deps, nreac, x, kSsaThreads, hs + threadIdx.x, st, window)
-                                           : ssa_cell(rt, nreac, x, kSsaThreads, st, window);
+    int e;
+    if (MASKED) {
+        CellReactions on;
+        on.load(rmask, rmask_words, area, c);
+        e = nreac > kIncMinReactions ? ssa_cell_inc(rt, deps, nreac, x, kSsaThreads, hs + threadIdx.x, st, window, on)
+                                     : ssa_cell_h(rt, nreac, x, kSsaThreads, st, window,
+                                                  GatedHazard<MassActionHazard>{MassActionHazard{}, on});
+    } else {
+        e = nreac > kIncMinReactions ? ssa_cell_inc(rt, deps, nreac, x, kSsaThreads, hs + threadIdx.x, st, window)
+                                     : ssa_cell(rt, nreac, x, kSsaThreads, st, window);
+    }
     for (int s = 0; s < S; ++s) planes.p[s][((int64_t)r * S + s) * area + c] = x[s * kSsaThreads];
     if (e) atomicOr(&status[r], e);
 }
@@ -219,7 +232,7 @@ __global__ void k_det_diffuse(const float* __restrict__ in, float* __restrict__ 
 
 // Deterministic.cl:143-238: 20 classical RK4 substeps per window, clamp at 0.
 __global__ void k_rk4(float* state, int S, int area, int R, const gpgmp_reaction* __restrict__ reactions, int nreac,
-                      float deltat) {
+                      float deltat, const uint32_t* __restrict__ rmask, int rmask_words) {
     extern __shared__ unsigned char smem[];
     gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
     float* buf = reinterpret_cast<float*>(smem + sizeof(gpgmp_reaction) * nreac);
@@ -235,6 +248,8 @@ __global__ void k_rk4(float* state, int S, int area, int R, const gpgmp_reaction
     float* y = buf + (size_t)5 * S * B + threadIdx.x;
     float* sp = state + (int64_t)r * S * area + c;
     for (int s = 0; s < S; ++s) x[s * B] = sp[(int64_t)s * area];
+    CellReactions on;           // localised reactions contribute nothing where they are off
+    on.load(rmask, rmask_words, area, c);
     const int nmax = 20;
     const float h = deltat / (float)nmax;
     for (int it = 0; it < nmax; ++it) {
@@ -247,6 +262,7 @@ __global__ void k_rk4(float* state, int S, int area, int R, const gpgmp_reaction
                 kout[s * B] = 0.0f;
             }
             for (int q = 0; q < nreac; ++q) {
+                if (!on(q)) continue;
                 const gpgmp_reaction& rc = rt[q];
                 float law = rc.rate;
                 for (int j = 0; j < rc.num_reactants; ++j)
@@ -311,9 +327,10 @@ constexpr int kAqssMaxIter = 100000;    // corrector passes per cell and window 
 // (Reaction.cpp:145-162); a reaction adds |net| law to q (net > 0) or d (net < 0)
 // of each species whose net stoichiometry it changes (Solver.cpp:961-1004)
 __device__ __forceinline__ void aqss_rhs(const gpgmp_reaction* rt, int nreac, int S, const float* y, float* q,
-                                         float* d) {
+                                         float* d, const CellReactions& on) {
     for (int i = 0; i < S; ++i) { q[i] = 0.0f; d[i] = 0.0f; }
     for (int k = 0; k < nreac; ++k) {
+        if (!on(k)) continue;        // localised reaction, off in this cell
         const gpgmp_reaction& rc = rt[k];
         float law = rc.rate;
         for (int j = 0; j < rc.num_reactants; ++j)
@@ -351,7 +368,8 @@ __device__ __forceinline__ float aqss_alpha(float r) {
 // from zero can be rejected forever) and the corrector coefficient as printed
 // (`180.*+rtaub`, :424).  Returns GPGMP_SIM_EVENT_CAP if the step control did not
 // finish within kAqssMaxIter passes.
-__device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, float dtg, bool literal) {
+__device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, float dtg, bool literal,
+                         const CellReactions& on) {
     const float epsmin = 1e-2f, sqreps = 0.5f, epscl = 100.0f, epsmax = 10.0f, tfd = 1.000008f, dtmin = 1e-15f,
                 ymin = 1e-20f;
     constexpr int itermax = 2;
@@ -359,7 +377,7 @@ __device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, f
         rtaus[kAqssMaxSpecies], scr[kAqssMaxSpecies], y1[kAqssMaxSpecies];
     float tn = 0.0f;
     for (int i = 0; i < S; ++i) y[i] = fmaxf(y[i], ymin);
-    aqss_rhs(rt, nreac, S, y, q, d);
+    aqss_rhs(rt, nreac, S, y, q, d, on);
     float scrtch = 1e-25f;
     for (int i = 0; i < S; ++i) {
         const float ascr = fabsf(q[i]);
@@ -396,7 +414,7 @@ __device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, f
                     tn = ts + dt;
                     for (int i = 0; i < S; ++i) y1[i] = y[i];
                 }
-                aqss_rhs(rt, nreac, S, y, q, d);
+                aqss_rhs(rt, nreac, S, y, q, d, on);
                 eps = 1e-10f;
                 for (int i = 0; i < S; ++i) {
                     const float rtaub = 0.5f * (rtaus[i] + dt * d[i] / y[i]);
@@ -436,13 +454,14 @@ __device__ int aqss_cell(const gpgmp_reaction* rt, int nreac, int S, float* y, f
             dto = dt / dto;
             for (int i = 0; i < S; ++i) rtaus[i] *= dto;
         }
-        aqss_rhs(rt, nreac, S, y, q, d);
+        aqss_rhs(rt, nreac, S, y, q, d, on);
     }
     return 0;
 }
 
 __global__ void k_aqss(float* state, int S, int area, int R, const gpgmp_reaction* __restrict__ reactions, int nreac,
-                       float deltat, int literal, int32_t* status) {
+                       float deltat, int literal, int32_t* status, const uint32_t* __restrict__ rmask,
+                       int rmask_words) {
     extern __shared__ unsigned char smem[];
     gpgmp_reaction* rt = reinterpret_cast<gpgmp_reaction*>(smem);
     for (int i = threadIdx.x; i < nreac; i += blockDim.x) rt[i] = reactions[i];
@@ -454,7 +473,9 @@ __global__ void k_aqss(float* state, int S, int area, int R, const gpgmp_reactio
         float* sp = state + (int64_t)r * S * area + c;
         float y[kAqssMaxSpecies];
         for (int s = 0; s < S; ++s) y[s] = sp[(int64_t)s * area];
-        const int e = aqss_cell(rt, nreac, S, y, deltat, literal != 0);
+        CellReactions on;
+        on.load(rmask, rmask_words, area, c);
+        const int e = aqss_cell(rt, nreac, S, y, deltat, literal != 0, on);
         for (int s = 0; s < S; ++s) sp[(int64_t)s * area] = y[s];
         if (e) atomicOr(&status[r], e);
     }
@@ -484,12 +505,21 @@ cudaError_t launch_ssa(const GridDesc& g, Planes planes, const gpgmp_reaction* d
     const size_t smem = sizeof(gpgmp_reaction) * nreac + sizeof(uint32_t) * 4 * nreac +
                         sizeof(float) * (size_t)nreac * kSsaThreads + sizeof(int) * g.S * kSsaThreads;
     const unsigned blocks = (unsigned)((total + kSsaThreads - 1) / kSsaThreads);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_ssa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+    if (g.rmask) {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_ssa<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        k_ssa<true><<<blocks, kSsaThreads, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed,
+                                                        window, d_status, g.rmask, g.rmask_words);
+    } else {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_ssa<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        k_ssa<false><<<blocks, kSsaThreads, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed,
+                                                         window, d_status, nullptr, 0);
     }
-    k_ssa<<<blocks, kSsaThreads, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed, window,
-                                              d_status);
     return cudaGetLastError();
 }
 
@@ -541,7 +571,7 @@ cudaError_t launch_aqss(const GridDesc& g, float* state, const gpgmp_reaction* d
     const int threads = 128;
     const size_t smem = sizeof(gpgmp_reaction) * nreac;
     k_aqss<<<grid_for(total, threads), threads, smem, st>>>(state, g.S, area, g.R, d_reactions, nreac, deltat, literal,
-                                                             d_status);
+                                                             d_status, g.rmask, g.rmask_words);
     return cudaGetLastError();
 }
 
@@ -615,7 +645,7 @@ cudaError_t launch_rk4(const GridDesc& g, float* state, const gpgmp_reaction* d_
         if (e != cudaSuccess) return e;
     }
     k_rk4<<<(unsigned)((total + threads - 1) / threads), threads, smem, st>>>(state, g.S, area, g.R, d_reactions,
-                                                                             nreac, deltat);
+                                                                             nreac, deltat, g.rmask, g.rmask_words);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,10 @@ class Reaction:
     reactants: Dict[str, int]
     products: Dict[str, int]
     rate: float
+    # localisation (Reaction::addCompartment, Reaction.cpp:209-235): inclusive
+    # rectangles (x0, y0, x1, y1); the reaction fires only in cells inside one of them.
+    # Empty: everywhere.
+    regions: List[tuple] = field(default_factory=list)
 
 
 @dataclass
@@ -99,9 +103,28 @@ class DiffusionModel:
         self.species.append(Species(id, diffusion, initial, individual))
         return self
 
-    def add_reaction(self, id: str, reactants: Dict[str, int], products: Dict[str, int], rate: float):
-        self.reactions.append(Reaction(id, dict(reactants), dict(products), rate))
+    def add_reaction(self, id: str, reactants: Dict[str, int], products: Dict[str, int], rate: float,
+                     regions=None):
+        """regions: inclusive rectangles (x0, y0, x1, y1) the reaction is localised to
+        (its compartments), or None for everywhere."""
+        self.reactions.append(Reaction(id, dict(reactants), dict(products), rate,
+                                       [tuple(int(v) for v in r) for r in (regions or [])]))
         return self
+
+    def reaction_mask(self) -> Optional[np.ndarray]:
+        """[R][H][W] uint8, 1 where each reaction may fire (the reference's
+        reactionMask: inside one of its compartments, or everywhere if it has none);
+        None when every reaction may fire in every cell (no reaction localised, or
+        localised to compartments that cover the grid)."""
+        if not any(r.regions for r in self.reactions):
+            return None
+        mask = np.zeros((len(self.reactions), self.height, self.width), dtype=np.uint8)
+        for k, r in enumerate(self.reactions):
+            if not r.regions:
+                mask[k] = 1
+            for (x0, y0, x1, y1) in r.regions:
+                mask[k, max(y0, 0):y1 + 1, max(x0, 0):x1 + 1] = 1
+        return None if mask.all() else mask
 
     def add_compartment(self, comp: Compartment):
         self.compartments.append(comp)
@@ -200,6 +223,11 @@ class DiffusionModel:
                 b = self.set_field_code.encode()
                 keep.append(b)
                 d.set_field_code = b
+        rm = self.reaction_mask()
+        if rm is not None:
+            rm = np.ascontiguousarray(rm).reshape(-1)
+            keep.append(rm)
+            d.reaction_mask = rm.ctypes.data_as(C.POINTER(C.c_uint8))
         if self.custom_laws is not None:
             if len(self.custom_laws) != len(self.reactions):
                 raise ValueError("custom_laws needs one entry (or None) per reaction")

@@ -32,8 +32,11 @@ Field parameters (domain "field") are per-cell values, zero until set (the refer
 init scripts fill them): the model code reads them by name (F(f)), and the setField
 method, compiled at run time, updates them every step.
 
+Reactions localised to compartments fire only inside them (the reaction mask of
+Solver.cpp:352-390).
+
 Not supported (raises Unsupported): init and event scripts (Python run by the
-reference's executable), reactions localised to part of the grid.
+reference's executable).
 """
 from __future__ import annotations
 
@@ -402,26 +405,28 @@ def load(source: str, *, ignore_scripts: bool = False, overrides: Optional[Dict[
             return out
 
         reactants, products = refs("listOfReactants"), refs("listOfProducts")
+        # localisation (InchmanDiffusionModel.cpp:410-435): every compartment whose
+        # isAllowed is non-zero; a reaction with none fires everywhere
+        regions = []
         loc = r.find(f"{SB}annotation/{IM}reaction/{IM}listOfCompartmentParameters")
         if loc is not None:
-            allowed = []
             for cp in loc:
+                if cp.tag != IM + "compartmentParameters":
+                    continue
                 v = _num(cp, "isAllowed", env)
-                if v:
-                    allowed.append(cp.get("compartment"))
-            whole = any(comps.get(c) == (0, 0, W - 1, H - 1) for c in allowed)
-            if allowed and not whole:
-                raise Unsupported(f"reaction {rid!r} is localised to {allowed}")
+                cid = cp.get("compartment")
+                if v and cid in comps:
+                    regions.append(comps[cid])
         kl = r.find(f"{SB}kineticLaw/{MM}math")
         if kl is None:
             raise Unsupported(f"reaction {rid!r} has no kinetic law")
         tree = mathml(kl)
         rate = mass_action_rate(tree, reactants, spset, env)
         if rate is not None:
-            m.add_reaction(rid, reactants, products, float(rate))
+            m.add_reaction(rid, reactants, products, float(rate), regions)
             laws.append(None)
         else:
-            m.add_reaction(rid, reactants, products, 0.0)
+            m.add_reaction(rid, reactants, products, 0.0, regions)
             laws.append(to_c(tree, names))
     if any(l is not None for l in laws):
         m.custom_laws = laws

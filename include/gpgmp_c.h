@@ -158,6 +158,14 @@ typedef struct gpgmp_model_desc {
     int32_t num_fields;
     const float* field_values;
     const char* set_field_code;
+    /* Localised reactions (Reaction::addCompartment / reactionMask, Reaction.h:160-189,
+     * Reaction.cpp:209-235; the mask image of Solver.cpp:352-390): [num_reactions][H][W]
+     * bytes, non-zero where the reaction may fire -- the union of its compartments'
+     * inclusive rectangles, or every cell for a reaction with none.  The SSA hazard and
+     * the deterministic right-hand side (RK4, alpha-QSS) of a reaction are zero in the
+     * cells where its byte is 0 (the reference multiplies them by the mask,
+     * Solver.cpp:852-854, 946-948).  NULL: every reaction everywhere. */
+    const uint8_t* reaction_mask;
 } gpgmp_model_desc;
 
 typedef struct gpgmp_solver gpgmp_solver;
@@ -349,8 +357,17 @@ int gpgmp_population_maintain(const uint32_t* keys, const uint32_t* ids, int64_t
  * call on each device looks the array up (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  Every call on a device
  * shares the one array: calls whose kernels overlap on the GPU (other streams, other
- * host threads) race and must be serialised by the caller.  Allocates nothing. */
+ * host threads) race and must be serialised by the caller.  The looked-up address is
+ * kept for the life of the process: do not use this entry point across a
+ * cudaDeviceReset of that device.  Allocates nothing.  Like the scan above it returns
+ * before the kernel ends, so a look-back wait that gave up is reported by
+ * gpgmp_exclusive_scan_u32_noalloc_status, not by the return code. */
 int gpgmp_exclusive_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, void* stream);
+/* Waits for `stream`, then sets *status to GPGMP_ERR_TIMEOUT if the last
+ * gpgmp_exclusive_scan_u32_noalloc on this device gave up a look-back wait (its output
+ * is then wrong), else GPGMP_OK.  The next no-allocation scan clears the record, so
+ * call this before it.  Allocates nothing. */
+int gpgmp_exclusive_scan_u32_noalloc_status(void* stream, int32_t* status);
 
 /* ---- individual particles on the lattice: move, bin, react, compact ---------------
  * The reference's individual solver (IndividualSolver.cpp:416-712, 458-671) moves

@@ -63,7 +63,21 @@ typedef struct orc_model {
     int32_t num_fields;                /* field parameters (the product's F(f) in model code) */
     const float* field_values;
     const char* set_field_code;
+    const uint8_t* reaction_mask;      /* localised reactions: [R][H][W], 0 = off in that cell; NULL: none */
 } orc_model;
+
+/* Bit r of on[r / 32] is set when reaction r may fire in cell `cell` (Reaction::
+ * reactionMask, Reaction.cpp:216-235: 1 inside one of its compartments, or
+ * everywhere for a reaction that has none).  At most 128 reactions. */
+static inline void orc_cell_reactions(const orc_model* m, size_t cell, uint32_t on[4]) {
+    on[0] = on[1] = on[2] = on[3] = 0xFFFFFFFFu;
+    if (!m->reaction_mask) return;
+    const size_t area = (size_t)m->width * m->height;
+    on[0] = on[1] = on[2] = on[3] = 0u;
+    for (int r = 0; r < m->num_reactions && r < 128; ++r)
+        if (m->reaction_mask[(size_t)r * area + cell]) on[r >> 5] |= 1u << (r & 31);
+}
+static inline int orc_reaction_on(const uint32_t* on, int r) { return !on || ((on[r >> 5] >> (r & 31)) & 1u); }
 
 /* ---- generators and elementary functions ---------------------------------- */
 void orc_threefry2x32_20(const uint32_t ctr[2], const uint32_t key[2], uint32_t out[2]);

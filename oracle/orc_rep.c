@@ -71,7 +71,9 @@ typedef float (*orc_hazard_fn)(int r, const int32_t* x);
 static orc_hazard_fn g_custom_hazard = NULL;
 void orc_set_custom_hazard(orc_hazard_fn fn) { g_custom_hazard = fn; }
 
-static int rep_ssa_cell(const orc_model* m, int32_t* x, orc_stream* st, float window) {
+/* on: the reactions that may fire in this cell (localised reactions); a reaction that
+ * may not has hazard 0 */
+static int rep_ssa_cell(const orc_model* m, int32_t* x, orc_stream* st, float window, const uint32_t* on) {
     const int R = m->num_reactions;
     float H[128];
     float t = 0.0f;
@@ -79,7 +81,9 @@ static int rep_ssa_cell(const orc_model* m, int32_t* x, orc_stream* st, float wi
     for (;;) {
         float h0 = 0.0f;
         for (int r = 0; r < R; ++r) {
-            h0 = h0 + (g_custom_hazard ? g_custom_hazard(r, x) : rep_hazard(&m->reactions[r], x));
+            const float hr = !orc_reaction_on(on, r) ? 0.0f
+                             : (g_custom_hazard ? g_custom_hazard(r, x) : rep_hazard(&m->reactions[r], x));
+            h0 = h0 + hr;
             H[r] = h0;
         }
         if (!(h0 > 0.0f)) break;
@@ -113,7 +117,9 @@ void orc_rep_ssa(const orc_model* m, int32_t* state, int R, uint32_t seed, uint3
             for (int s = 0; s < S; ++s) x[s] = base[(size_t)s * area + c];
             orc_stream st;
             orc_stream_init(&st, seed, (uint32_t)r, step_seed, (uint32_t)c, ORC_PH_SSA);
-            int e = rep_ssa_cell(m, x, &st, window);
+            uint32_t on[4];
+            orc_cell_reactions(m, (size_t)c, on);
+            int e = rep_ssa_cell(m, x, &st, window, on);
             for (int s = 0; s < S; ++s) base[(size_t)s * area + c] = x[s];
             if (e && status) {
                 #pragma omp atomic

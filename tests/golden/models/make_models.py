@@ -35,12 +35,18 @@ def document(name, solver, W, L, time, out, params, comps, species, reactions, m
                   + ('<im:individual/>' if sid in individual else '') +
                   f'</im:species></annotation></species>')
     rs = []
-    for rid, (re_, pr, law) in reactions.items():
+    for rid, spec in reactions.items():
+        # (reactants, products, law[, {compartment: allowed}]): without the fourth entry
+        # the reaction is allowed in World, as the editor writes a global reaction
+        re_, pr, law = spec[:3]
+        allowed = spec[3] if len(spec) > 3 else {"World": True}
         rl = "".join(f'<speciesReference species="{s}" stoichiometry="{n}"/>' for s, n in re_.items())
         pl = "".join(f'<speciesReference species="{s}" stoichiometry="{n}"/>' for s, n in pr.items())
+        cps = "".join(f'<im:compartmentParameters compartment="{c}"><im:isAllowed>'
+                      f'<math xmlns="{MML}"><ci>{"true" if ok else "false"}</ci></math></im:isAllowed>'
+                      f'</im:compartmentParameters>' for c, ok in allowed.items())
         rs.append(f'      <reaction id="{rid}"><annotation><im:reaction xmlns:im="{IMNS}">'
-                  f'<im:listOfCompartmentParameters><im:compartmentParameters compartment="World"><im:isAllowed>'
-                  f'<math xmlns="{MML}"><ci>true</ci></math></im:isAllowed></im:compartmentParameters>'
+                  f'<im:listOfCompartmentParameters>{cps}'
                   f'</im:listOfCompartmentParameters></im:reaction></annotation>'
                   f'<listOfReactants>{rl}</listOfReactants><listOfProducts>{pl}</listOfProducts>'
                   f'<kineticLaw><math xmlns="{MML}">{law}</math></kineticLaw></reaction>')
@@ -146,8 +152,19 @@ def main():
         method="All->DiffusivityX = 0.4 + 0.0 * trace;\nAll->DiffusivityY = 0.4;\nAll->DriftX = 0.0;\n"
                "All->DriftY = 0.0;",
         fields=("trace",), set_field="trace = trace + rate * deltat * A;")
+    # localised reactions: A made only in a spot, A + B -> C only in the left part, C
+    # decays everywhere, B made by a saturating (custom) law only in the right part
+    loc = document(
+        "Localised reactions", "stochastic_homogeneous", 16, 16.0, 0.6, 0.2,
+        {"ks": 30.0, "kb": 0.02, "kd": 0.4, "vm": 12.0, "km": 10.0},
+        {"World": (0, 0, 16, 16), "Left": (0, 0, 6, 16), "Right": (10, 0, 6, 16), "Spot": (7, 7, 2, 2)},
+        {"A": (1.0, {"World": 16 * 16 * 10}), "B": (0.8, {"World": 16 * 16 * 10}), "C": (0.3, {})},
+        {"make": ({}, {"A": 1}, ci("ks"), {"World": False, "Spot": True}),
+         "bind": ({"A": 1, "B": 1}, {"C": 1}, times(times(ci("kb"), ci("A")), ci("B")), {"Left": True}),
+         "decay": ({"C": 1}, {}, times(ci("kd"), ci("C"))),
+         "bmake": ({}, {"B": 1}, divide(times(ci("vm"), ci("B")), plus(ci("km"), ci("B"))), {"Right": True})})
     for name, text in (("ab_drift.xml", ab), ("saturating.xml", mm), ("individual_a.xml", ind),
-                       ("nonlinear.xml", nl), ("field_trace.xml", fd)):
+                       ("nonlinear.xml", nl), ("field_trace.xml", fd), ("localised.xml", loc)):
         with open(os.path.join(HERE, name), "w") as f:
             f.write(text)
 

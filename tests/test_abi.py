@@ -70,6 +70,7 @@ int main(void) {
   P(gpgmp_model_desc, drift_params); P(orc_model, drift_params);
   P(gpgmp_model_desc, diffusion); P(orc_model, diffusion);
   P(gpgmp_model_desc, field_ry); P(orc_model, field_ry);
+  P(gpgmp_model_desc, reaction_mask); P(orc_model, reaction_mask);
   return 0;
 }
 '''

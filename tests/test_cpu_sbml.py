@@ -12,7 +12,8 @@ from inchman_b200.sbml import Unsupported
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = os.path.join(HERE, "golden", "models")
-REF_EXAMPLES = "/root/reference/doc/examples"
+# the reference checkout, when present: INCHMAN_REFERENCE names its root
+REF_EXAMPLES = os.path.join(os.environ.get("INCHMAN_REFERENCE", ""), "doc", "examples")
 
 
 def test_fixture_ab_drift():
@@ -107,3 +108,28 @@ def test_reference_examples_load_or_name_what_is_missing():
     # without its (Python 2) init script the Calcium model loads, with custom laws
     ca = sbml.load(os.path.join(REF_EXAMPLES, "Calcium.xml"), ignore_scripts=True).model
     assert ca.custom_laws is not None and sum(l is not None for l in ca.custom_laws) >= 3
+
+
+def test_fixture_localised_reactions():
+    """localised.xml: reactions allowed in some compartments (isAllowed true), others
+    (isAllowed false) left out; the mask is the union of the allowed rectangles, and a
+    reaction allowed in World fires everywhere (InchmanDiffusionModel.cpp:410-435,
+    Reaction.cpp:216-235)."""
+    m = sbml.load(os.path.join(MODELS, "localised.xml")).model
+    assert [r.id for r in m.reactions] == ["make", "bind", "decay", "bmake"]
+    assert m.reactions[0].regions == [(7, 7, 8, 8)]
+    assert m.reactions[1].regions == [(0, 0, 5, 15)]
+    assert m.reactions[2].regions == [(0, 0, 15, 15)]
+    assert m.reactions[3].regions == [(10, 0, 15, 15)]
+    mask = m.reaction_mask()
+    assert mask.shape == (4, 16, 16) and mask.dtype == np.uint8
+    assert mask[0].sum() == 4 and mask[0, 7:9, 7:9].all()
+    assert mask[1, :, :6].all() and not mask[1, :, 6:].any()
+    assert mask[2].all()
+    assert mask[3, :, 10:].all() and not mask[3, :, :10].any()
+    assert m.custom_laws[3] is not None and m.custom_laws[0] is None
+    desc, keep = m.to_desc()
+    assert bool(desc.reaction_mask)
+    # without localised reactions the descriptor carries no mask
+    m2 = sbml.load(os.path.join(MODELS, "saturating.xml")).model
+    assert m2.reaction_mask() is None and not bool(m2.to_desc()[0].reaction_mask)
