@@ -114,6 +114,11 @@ def ref():
             "gref_threefry2x32": (None, [vp, vp, vp]),
             "gref_philox4x32": (None, [vp, vp, vp]),
         }
+        # model-specific kernels generated from the reference's templates (ref/gen_models.py)
+        for m in ("abc", "dimer", "abcloc"):
+            sig[f"gref_ssa_{m}"] = (None, [vp, C.c_int, f32, vp])
+        for m in ("gs", "gsloc"):
+            sig[f"gref_rk4_{m}"] = (None, [vp, f32, vp])
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
             fn.restype = res

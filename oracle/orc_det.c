@@ -2,8 +2,8 @@
  * oracle/orc_det.c -- TEST INFRASTRUCTURE ONLY (the oracle).
  *
  * Deterministic reaction-diffusion oracles:
- *  - Gray-Scott, forward Euler, 5-point periodic Laplacian (h = 1), in float and
- *    double, and the double-precision discrete adjoint of the loss
+ *  - Gray-Scott, forward Euler, 5-point periodic Laplacian (h = 1), in float (in
+ *    the GPU kernels' operation order, bit-exact) and double, and the double-precision discrete adjoint of the loss
  *    L = sum (u_N - u*)^2 + (v_N - v*)^2 with respect to (F, k, Du, Dv, vx, vy), with
  *    checkpoints every `checkpoint_every` steps and per-segment recomputation.
  *    The network is the reference's Gray-Scott model (exec/src/tests/
@@ -31,29 +31,92 @@
 
 #define IDX(x, y, N) ((size_t)(((y) + (N)) % (N)) * (N) + (size_t)(((x) + (N)) % (N)))
 
-void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float vx, float vy, float dt,
-                        float* u, float* v) {
-    const size_t n = (size_t)N * N;
-    float* u2 = (float*)malloc(sizeof(float) * n);
-    float* v2 = (float*)malloc(sizeof(float) * n);
-    for (int s = 0; s < steps; ++s) {
-        #pragma omp parallel for schedule(static)
-        for (int y = 0; y < N; ++y)
-            for (int x = 0; x < N; ++x) {
-                size_t i = (size_t)y * N + x;
-                float uc = u[i], vc = v[i];
-                float lu = u[IDX(x - 1, y, N)] + u[IDX(x + 1, y, N)] + u[IDX(x, y - 1, N)] + u[IDX(x, y + 1, N)] - 4.0f * uc;
-                float lv = v[IDX(x - 1, y, N)] + v[IDX(x + 1, y, N)] + v[IDX(x, y - 1, N)] + v[IDX(x, y + 1, N)] - 4.0f * vc;
-                float uvv = uc * vc * vc;
-                float au = vx * (u[IDX(x + 1, y, N)] - u[IDX(x - 1, y, N)]) * 0.5f + vy * (u[IDX(x, y + 1, N)] - u[IDX(x, y - 1, N)]) * 0.5f;
-                float av = vx * (v[IDX(x + 1, y, N)] - v[IDX(x - 1, y, N)]) * 0.5f + vy * (v[IDX(x, y + 1, N)] - v[IDX(x, y - 1, N)]) * 0.5f;
-                u2[i] = uc + dt * (Du * lu - au - uvv + F * (1.0f - uc));
-                v2[i] = vc + dt * (Dv * lv - av + uvv - (F + k) * vc);
-            }
-        memcpy(u, u2, sizeof(float) * n);
-        memcpy(v, v2, sizeof(float) * n);
+/* The float32 forward as the GPU's packed-FP32x2 kernels compute it (gs_update2f in
+ * inchman_b200/csrc/gs_f32x2.cuh, used by the register-resident, column-walk and batched
+ * float32 kernels): the same float operations in the same order, each fused
+ * multiply-add an fmaf, so the two agree bit for bit.  Per cell, with L/R the x-1/x+1
+ * and U/D the y-1/y+1 neighbours (periodic):
+ *   lu = fma(-4, u, (uL + uR) + (uU + uD)),  uvv = u * (v * v)
+ *   a  = fma(dt Du, lu, fma(-(dt F), u, dt F)),  b = fma(-(dt (F + k)), v, (dt Dv) * lv)
+ *   drift: a = fma(hx, uL - uR, fma(hy, uU - uD, a)) (b likewise), hx = (dt vx) 0.5
+ *   u' = u + fma(-dt, uvv, a),  v' = v + fma(dt, uvv, b)
+ * This is the explicit Euler step of Deterministic.cl:17-65 plus the Gray-Scott
+ * right-hand side of GrayScottModel.cpp:14-60 (Reaction.cpp:145-162 laws). */
+static inline void gs_cell_f32x(float du, float dv, float hx, float hy, float dt, float mdt, float dtF, float mdtF,
+                                float mdtFk, int drift, float uL, float uR, float uU, float uC, float uD, float vL,
+                                float vR, float vU, float vC, float vD, float* un, float* vn) {
+    const float uvv = uC * (vC * vC);
+    const float lu = fmaf(-4.0f, uC, (uL + uR) + (uU + uD));
+    const float lv = fmaf(-4.0f, vC, (vL + vR) + (vU + vD));
+    float a = fmaf(du, lu, fmaf(mdtF, uC, dtF));
+    float b = fmaf(mdtFk, vC, dv * lv);
+    if (drift) {
+        a = fmaf(hx, uL - uR, fmaf(hy, uU - uD, a));
+        b = fmaf(hx, vL - vR, fmaf(hy, vU - vD, b));
     }
-    free(u2); free(v2);
+    *un = uC + fmaf(mdt, uvv, a);
+    *vn = vC + fmaf(dt, uvv, b);
+}
+
+/* One row y of the step; the interior columns have no wrap-around, so the compiler
+ * vectorises them (the fma clone uses the CPU's fused multiply-add instructions). */
+__attribute__((target_clones("fma", "default")))
+static void gs_row_f32x(int N, int y, float du, float dv, float hx, float hy, float dt, float mdt, float dtF,
+                        float mdtF, float mdtFk, int drift, const float* restrict u, const float* restrict v,
+                        float* restrict u2, float* restrict v2) {
+    const float* restrict uc = u + (size_t)y * N;
+    const float* restrict vc = v + (size_t)y * N;
+    const float* restrict uu = u + (size_t)((y + N - 1) % N) * N;
+    const float* restrict vu = v + (size_t)((y + N - 1) % N) * N;
+    const float* restrict ud = u + (size_t)((y + 1) % N) * N;
+    const float* restrict vd = v + (size_t)((y + 1) % N) * N;
+    float* restrict uo = u2 + (size_t)y * N;
+    float* restrict vo = v2 + (size_t)y * N;
+    if (drift) {
+        for (int x = 1; x < N - 1; ++x)
+            gs_cell_f32x(du, dv, hx, hy, dt, mdt, dtF, mdtF, mdtFk, 1, uc[x - 1], uc[x + 1], uu[x], uc[x], ud[x],
+                         vc[x - 1], vc[x + 1], vu[x], vc[x], vd[x], &uo[x], &vo[x]);
+    } else {
+        for (int x = 1; x < N - 1; ++x)
+            gs_cell_f32x(du, dv, hx, hy, dt, mdt, dtF, mdtF, mdtFk, 0, uc[x - 1], uc[x + 1], uu[x], uc[x], ud[x],
+                         vc[x - 1], vc[x + 1], vu[x], vc[x], vd[x], &uo[x], &vo[x]);
+    }
+    const int edge[2] = {0, N - 1};
+    for (int e = 0; e < (N > 1 ? 2 : 1); ++e) {
+        const int x = edge[e], xl = (x + N - 1) % N, xr = (x + 1) % N;
+        gs_cell_f32x(du, dv, hx, hy, dt, mdt, dtF, mdtF, mdtFk, drift, uc[xl], uc[xr], uu[x], uc[x], ud[x], vc[xl],
+                     vc[xr], vu[x], vc[x], vd[x], &uo[x], &vo[x]);
+    }
+}
+
+void orc_gs_forward_f32(int N, int steps, float F, float k, float Du, float Dv, float vx, float vy, float dt,
+                         float* u, float* v) {
+    const size_t n = (size_t)N * N;
+    /* coefficients as the kernels form them from the float parameters (GSCoef2) */
+    const float du = dt * Du, dv = dt * Dv, hx = dt * vx * 0.5f, hy = dt * vy * 0.5f;
+    const float mdt = -dt, dtF = dt * F, mdtF = -(dt * F), mdtFk = -(dt * (F + k));
+    const int drift = vx != 0.0f || vy != 0.0f;
+    float* buf = (float*)malloc(sizeof(float) * 2 * n);
+    float *cu = u, *cv = v, *nu = buf, *nv = buf + n;
+    /* one parallel region for the whole solve: each thread keeps the same rows every
+     * step, and the barrier at the end of the loop over rows separates the steps */
+    #pragma omp parallel firstprivate(cu, cv, nu, nv)
+    for (int s = 0; s < steps; ++s) {
+        #pragma omp for schedule(static)
+        for (int y = 0; y < N; ++y)
+            gs_row_f32x(N, y, du, dv, hx, hy, dt, mdt, dtF, mdtF, mdtFk, drift, cu, cv, nu, nv);
+        float* t = cu; cu = nu; nu = t;
+        t = cv; cv = nv; nv = t;
+    }
+    if (steps % 2 == 1) {    /* the result is in the work buffer */
+        cu = buf;
+        cv = buf + n;
+    }
+    if (cu != u) {
+        memcpy(u, cu, sizeof(float) * n);
+        memcpy(v, cv, sizeof(float) * n);
+    }
+    free(buf);
 }
 
 static void gs_step_f64(int N, double F, double k, double Du, double Dv, double vx, double vy, double dt,
@@ -203,10 +266,11 @@ void orc_det_sweep(const orc_model* m, const float* in, float* out, int species,
  * coefficient as printed (`180.*+rtaub`, :424).  Returns 1 if the step control did
  * not finish within ORC_AQSS_MAX_ITER corrector passes. */
 #define ORC_AQSS_MAX_ITER 100000
-static void orc_aqss_rhs(const orc_model* m, const float* y, float* q, float* d) {
+static void orc_aqss_rhs(const orc_model* m, const uint32_t* on, const float* y, float* q, float* d) {
     const int S = m->num_species;
     for (int i = 0; i < S; ++i) { q[i] = 0.0f; d[i] = 0.0f; }
     for (int k = 0; k < m->num_reactions; ++k) {
+        if (!orc_reaction_on(on, k)) continue;     /* localised reaction, off in this cell */
         const orc_reaction* rc = &m->reactions[k];
         float law = rc->rate;
         for (int j = 0; j < rc->num_reactants; ++j)
@@ -233,7 +297,7 @@ static void orc_aqss_rhs(const orc_model* m, const float* y, float* q, float* d)
 static float orc_aqss_alpha(float r) {
     return (180.0f + r * (60.0f + r * (11.0f + r))) / (360.0f + r * (60.0f + r * (12.0f + r)));
 }
-int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
+static int orc_aqss_cell_on(const orc_model* m, const uint32_t* on, float* y, float dtg, int literal) {
     const int S = m->num_species;
     const float epsmin = 1e-2f, sqreps = 0.5f, epscl = 100.0f, epsmax = 10.0f, tfd = 1.000008f, dtmin = 1e-15f,
                 ymin = 1e-20f;
@@ -241,7 +305,7 @@ int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
     float q[64], d[64], ys[64], qs[64], ds[64], rtaus[64], scr[64], y1[64];
     float tn = 0.0f;
     for (int i = 0; i < S; ++i) y[i] = fmaxf(y[i], ymin);
-    orc_aqss_rhs(m, y, q, d);
+    orc_aqss_rhs(m, on, y, q, d);
     float scrtch = 1e-25f;
     for (int i = 0; i < S; ++i) {
         const float ascr = fabsf(q[i]);
@@ -269,7 +333,7 @@ int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
             for (int it = 0; it < itermax; ++it) {
                 for (int i = 0; i < S; ++i) y[i] = fmaxf(ys[i] + dt * scr[i], ymin);
                 if (it == 0) { tn = ts + dt; for (int i = 0; i < S; ++i) y1[i] = y[i]; }
-                orc_aqss_rhs(m, y, q, d);
+                orc_aqss_rhs(m, on, y, q, d);
                 eps = 1e-10f;
                 for (int i = 0; i < S; ++i) {
                     const float rtaub = 0.5f * (rtaus[i] + dt * d[i] / y[i]);
@@ -305,9 +369,12 @@ int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
             dto = dt / dto;
             for (int i = 0; i < S; ++i) rtaus[i] *= dto;
         }
-        orc_aqss_rhs(m, y, q, d);
+        orc_aqss_rhs(m, on, y, q, d);
     }
     return 0;
+}
+int orc_aqss_cell(const orc_model* m, float* y, float dtg, int literal) {
+    return orc_aqss_cell_on(m, NULL, y, dtg, literal);
 }
 /* one alpha-QSS window for every cell of one realisation's state [S][area] */
 int orc_aqss(const orc_model* m, float* state, float dtg, int literal) {
@@ -318,8 +385,10 @@ int orc_aqss(const orc_model* m, float* state, float dtg, int literal) {
     #pragma omp parallel for schedule(dynamic, 64) reduction(|:bad)
     for (int64_t c = 0; c < (int64_t)area; ++c) {
         float y[64];
+        uint32_t on[4];
+        orc_cell_reactions(m, (size_t)c, on);
         for (int i = 0; i < S; ++i) y[i] = state[c + (size_t)i * area];
-        bad |= orc_aqss_cell(m, y, dtg, literal);
+        bad |= orc_aqss_cell_on(m, on, y, dtg, literal);
         for (int i = 0; i < S; ++i) state[c + (size_t)i * area] = y[i];
     }
     return bad;

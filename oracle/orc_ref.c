@@ -184,6 +184,8 @@ void orc_ref_gillespie(const orc_model* m, int32_t* state, int32_t seed, float d
     for (int64_t gid = 0; gid < (int64_t)area; ++gid) {
         int32_t x[64];
         float h[130];
+        uint32_t on[4];
+        orc_cell_reactions(m, (size_t)gid, on);
         for (int s = 0; s < S; ++s) x[s] = state[gid + (size_t)s * area];
         ref_rng g = {{0, 0}, {0, 0}, {0, 0}};
         ref_rng_init(&g, (uint32_t)gid, seed);
@@ -191,14 +193,19 @@ void orc_ref_gillespie(const orc_model* m, int32_t* state, int32_t seed, float d
         while (t < deltat) {
             h[0] = 0.f;
             for (int i = 0; i < R; ++i) {
-                h[i + 1] = (float)((double)h[0] + ref_kinetic_law(&m->reactions[i], lit[i], x));
+                /* a localised reaction's law is multiplied by the cell's mask value, 1 or 0
+                 * (Solver.cpp:852-854) */
+                const double law = orc_reaction_on(on, i) ? ref_kinetic_law(&m->reactions[i], lit[i], x) : 0.0;
+                h[i + 1] = (float)((double)h[0] + law);
                 h[0] = h[i + 1];
             }
             if (h[0] == 0) break;
             ref_rng_draw(&g);
             float r1 = (float)(g.r[0] * M_RAN_INVM32 + 0.5);
             float r2 = (float)((g.r[1] * M_RAN_INVM32 + 0.5) * h[0]);
-            float dt = (float)(log((double)(1.f / r1)) / (double)h[0]);
+            /* OpenCL's log of a float argument is the float logarithm (the overload
+             * for float; Gillespie.cl:72 `log(1.f/_r1) / _h[0]`, all in float) */
+            float dt = logf(1.f / r1) / h[0];
             t += dt;
             if (t < deltat) {
                 for (int i = 0; i < R; ++i) {
@@ -331,12 +338,14 @@ void orc_ref_det_diffuse(const orc_model* m, const float* in, float* out, float 
 
 /* Deterministic.cl:143-238 with the right-hand side Solver.cpp:922-959 generates:
  * d_i = 0. (+|-) |nu|. * rate * A * B ..., laws from Reaction.cpp:145-162. */
-static void ref_rhs(const orc_model* m, const double* lit, float* xs, float* deriv, float off, const float* rk) {
+static void ref_rhs(const orc_model* m, const double* lit, const uint32_t* on, float* xs, float* deriv, float off,
+                    const float* rk) {
     const int S = m->num_species, R = m->num_reactions;
     for (int j = 0; j < S; ++j) { deriv[j] = 0.f; xs[j] += off * rk[j]; }
     for (int i = 0; i < S; ++i) {
         double acc = 0.;
         for (int r = 0; r < R; ++r) {
+            if (!orc_reaction_on(on, r)) continue;      /* mask 0 in this cell (Solver.cpp:946-948) */
             const orc_reaction* rc = &m->reactions[r];
             int net = 0;
             for (int j = 0; j < rc->num_products; ++j) if (rc->product_species[j] == i) net += rc->product_stoich[j];
@@ -361,14 +370,16 @@ void orc_ref_rk4(const orc_model* m, float* state, float deltat) {
     #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < (int64_t)area; ++c) {
         float xs[64], k1[64], k2[64], k3[64], k4[64];
+        uint32_t on[4];
+        orc_cell_reactions(m, (size_t)c, on);
         for (int i = 0; i < S; ++i) { xs[i] = state[c + (size_t)i * area]; k1[i] = 0.f; }
         const int nmax = 20;
         float dtc = deltat / (float)nmax;
         for (int it = 0; it < nmax; ++it) {
-            ref_rhs(m, lit, xs, k1, 0.f, k1);
-            ref_rhs(m, lit, xs, k2, (float)(dtc / 2.), k1);
-            ref_rhs(m, lit, xs, k3, (float)(dtc / 2.), k2);
-            ref_rhs(m, lit, xs, k4, dtc, k3);
+            ref_rhs(m, lit, on, xs, k1, 0.f, k1);
+            ref_rhs(m, lit, on, xs, k2, (float)(dtc / 2.), k1);
+            ref_rhs(m, lit, on, xs, k3, (float)(dtc / 2.), k2);
+            ref_rhs(m, lit, on, xs, k4, dtc, k3);
             for (int j = 0; j < S; ++j) {
                 xs[j] = (float)(xs[j] + dtc / 6. * (k1[j] + 2. * k2[j] + 2. * k3[j] + k4[j]));
                 if (xs[j] < 0.) xs[j] = 0.f;

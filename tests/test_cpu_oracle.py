@@ -132,3 +132,65 @@ def test_replay_matches_reference_statistics():
     lo, hi = stats.f.ppf(alpha / 2, R - 1, R - 1), stats.f.isf(alpha / 2, R - 1, R - 1)
     ok = (b.var(0) == 0) | ((f > lo) & (f < hi))
     assert ok.all()
+
+
+def test_localised_replay_matches_reference_statistics():
+    """Localised reactions (the reference's reaction mask): the replay and the
+    reference-exact restatement agree in per-cell mean and variance, and both leave
+    the reactions off outside their regions."""
+    from scipy import stats
+    from inchman_b200 import _lib
+    from inchman_b200.model import DiffusionModel
+    m = DiffusionModel(width=6, height=5, physical_length=6.0, p0=0.1, max_time=0.3, output_interval=0.2,
+                       solver=_lib.STOCHASTIC_HOMOGENEOUS)
+    m.add_species("A", 1.0, 40.0).add_species("B", 1.0, 30.0).add_species("C", 0.5, 5.0)
+    m.add_reaction("bind", {"A": 1, "B": 1}, {"C": 1}, 0.02, regions=[(0, 0, 2, 4)])
+    m.add_reaction("unbind", {"C": 1}, {"A": 1, "B": 1}, 0.3, regions=[(4, 1, 5, 2)])
+    m.add_reaction("src", {}, {"C": 1}, 15.0, regions=[(5, 4, 5, 4)])
+    desc, keep = m.to_desc()
+    R = 1200
+    lam = [s.initial for s in m.species]
+    init = oracle.init_poisson(m.width, m.height, m.num_species, 1, 7, lam)
+    st, _, _, _, _ = oracle.rep_solve(desc, np.repeat(init, R, axis=0), R, 99, 1)
+    rep = st.astype(np.int64)
+    ref = np.zeros_like(rep)
+    for r in range(R):
+        s2, _, _, _ = oracle.ref_solve(desc, init, 5000 + r, 1)
+        ref[r] = s2[0]
+    a, b = rep.reshape(R, -1).astype(np.float64), ref.reshape(R, -1).astype(np.float64)
+    se = np.sqrt(a.var(0, ddof=1) / R + b.var(0, ddof=1) / R) + 1e-12
+    z = np.abs(a.mean(0) - b.mean(0)) / se
+    alpha = 1e-3 / z.size
+    assert (z < stats.norm.isf(alpha / 2)).all(), z.max()
+    f = a.var(0, ddof=1) / np.maximum(b.var(0, ddof=1), 1e-12)
+    lo, hi = stats.f.ppf(alpha / 2, R - 1, R - 1), stats.f.isf(alpha / 2, R - 1, R - 1)
+    assert ((b.var(0) == 0) | ((f > lo) & (f < hi))).all()
+
+
+def test_localised_reactions_stay_off_outside_their_regions_on_the_cpu():
+    """One reaction window: cells outside a reaction's region keep their counts in the
+    reference-exact restatement, the replay and the deterministic RK4."""
+    from inchman_b200 import _lib
+    from inchman_b200.model import DiffusionModel
+    W = H = 8
+    m = DiffusionModel(width=W, height=H, physical_length=8.0, p0=0.1, max_time=0.5, output_interval=0.5,
+                       solver=_lib.STOCHASTIC_HOMOGENEOUS)
+    m.add_species("A", 0.0, 30.0).add_species("B", 0.0, 0.0)
+    m.add_reaction("conv", {"A": 1}, {"B": 1}, 3.0, regions=[(1, 1, 3, 2)])
+    desc, keep = m.to_desc()
+    inside = m.reaction_mask()[0].astype(bool)
+    init = np.zeros((1, 2, H, W), np.int32)
+    init[0, 0] = 30
+    st = init.copy()
+    oracle.orc().orc_rep_ssa(oracle.model_ptr(desc), oracle.ptr(st), 1, 3, 0, 0.5, None)
+    assert (st[0, 0][~inside] == 30).all() and (st[0, 0][inside] < 30).all()
+    assert (st[0, 1][~inside] == 0).all() and (st[0].sum(axis=0) == 30).all()
+    st = init.copy()
+    oracle.orc().orc_ref_gillespie(oracle.model_ptr(desc), oracle.ptr(st), 17, 0.5)
+    assert (st[0, 0][~inside] == 30).all() and (st[0, 0][inside] < 30).all()
+    m.solver = _lib.DETERMINISTIC_RK4
+    desc, keep = m.to_desc()
+    fs = np.ascontiguousarray(init[0].astype(np.float32))
+    oracle.orc().orc_ref_rk4(oracle.model_ptr(desc), oracle.ptr(fs), 0.5)
+    assert (fs[0][~inside] == 30).all() and (fs[0][inside] < 30).all()
+    np.testing.assert_allclose(fs.sum(axis=0), 30.0, rtol=1e-6)
