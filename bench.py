@@ -313,6 +313,34 @@ def bench_gray_scott(args, rank, world):
     t_grad = ga.elapsed_time(gb) / 1e3 / nrep
     # forward + backward over forward-only time
     ratio = t_grad / t_launch
+    # the same ratio in float64, the precision whose gradient meets 1e-4 against
+    # finite differences and equals the oracle's float64 CPU adjoint
+    u064, v064 = u0.double(), v0.double()
+    ut64, vt64 = ut.double(), vt.double()
+
+    def grad64_once():
+        u, v = GS.apply(u064, v064, th, steps, cfg.dt, cfg.checkpoint_every)
+        loss = ((u - ut64) ** 2 + (v - vt64) ** 2).sum()
+        loss.backward()
+        return loss
+
+    gs.forward(u064, v064, p)
+    grad64_once()
+    torch.cuda.synchronize()
+    fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nrep64 = max(1, min(args.steps, 3))
+    fa.record(stream)
+    for _ in range(nrep64):
+        gs.forward(u064, v064, p)
+    fb.record(stream)
+    torch.cuda.synchronize()
+    t_fwd64 = fa.elapsed_time(fb) / 1e3 / nrep64
+    fa.record(stream)
+    for _ in range(nrep64):
+        grad64_once()
+    fb.record(stream)
+    torch.cuda.synchronize()
+    t_grad64 = fa.elapsed_time(fb) / 1e3 / nrep64
     peak, peak_kind = load_peaks()
     alg_bytes = 16.0 * cell_steps
     achieved = alg_bytes / t_launch / 1e9
@@ -322,6 +350,7 @@ def bench_gray_scott(args, rank, world):
         for ln in open(prof):
             if ln.startswith("traffic_bytes_per_launch:"):
                 traffic = float(ln.split(":")[1])
+    clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_total / args.steps * 1e3, "higher_is_better": True,
@@ -332,19 +361,61 @@ def bench_gray_scott(args, rank, world):
                    "l2": "flushed between timed iterations (256 MB write)",
                    "parallelism": f"replicas x{world}"},
         "adjoint_forward_ratio": ratio,
-        "batched": batched,
+        "adjoint_forward_ratio_f64": t_grad64 / t_fwd64,
         "gradient_ms": t_grad * 1e3,
+        "gradient_ms_f64": t_grad64 * 1e3, "forward_ms_f64": t_fwd64 * 1e3,
+        "batched_fd_solves": batched,
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": 2 * n * n * 4},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
-                     "note": "16 B/cell-step algorithmic; the lattice stays in cluster shared memory"},
+                     "note": "16 B/cell-step algorithmic; the lattice stays in the registers of one 16-CTA cluster "
+                             "(16 of 148 SMs), so DRAM traffic is the initial read and final write only",
+                     "sm_bound": sm_bound(t_launch, steps, n, clocks.get("sm_mhz"))},
         "gpu_launches": args.steps,   # one k_gs_forward_rr launch per timed solve
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline_gray_scott(cfg)
+        if not getattr(args, "headline_only", False):
+            paths = path_blocks(args)
+            line["paths"] = paths
+            line["batched_over_plain"] = {"c4_ensemble_4096": paths["c4_ensemble_4096"]["batched_over_plain"],
+                                          "c1_ssa_plain_32x32": paths["c1_ssa_plain_32x32"]["batched_over_plain"],
+                                          "same_stats": "bit-identical final states, plain vs batched"}
     return line
+
+
+def sm_bound(t_solve, steps, n, clock_mhz, sms=16, ops_per_cell=18):
+    """The compute bound of the forward solve on the SMs it occupies: one 16-CTA
+    cluster, 18 FP32 lane operations per cell-step (an FMA counts once), 128 FP32
+    lanes per SM at the median SM clock sampled during the timed solves."""
+    clk = float(clock_mhz or 1965.0) * 1e6
+    bound = n * n * ops_per_cell / (sms * 128 * clk)
+    per = t_solve / steps
+    return {"sms_used": sms, "fp32_ops_per_cell_step": ops_per_cell, "sm_clock_hz": clk,
+            "bound_us_per_step": bound * 1e6, "achieved_us_per_step": per * 1e6, "frac": bound / per}
+
+
+def path_blocks(args):
+    """The other hot-path workloads, each measured once in the default line (a bounded
+    form of bench.py --workload <name>): C1 plain vs batched SSA, C3 drift-diffusion
+    SSA (t in [0, 0.5]), C4 batched ensemble vs plain, C5 particle binning, and the
+    scan / sort primitives."""
+    from types import SimpleNamespace
+    from inchman_b200 import workloads
+    ns = SimpleNamespace(steps=max(3, min(args.steps, 20)), warmup=max(3, args.warmup), instances=4096,
+                         plain_sample=24, t_sample=0.5, workload="")
+    drop = {"metric", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "data"}
+    out = {}
+    for key, fn in (("c1_ssa_plain_32x32", workloads.ssa_plain), ("c3_drift_diffusion_512x512", workloads.lotka_volterra),
+                    ("c4_ensemble_4096", workloads.ensemble), ("c5_particles_2p22", workloads.particles),
+                    ("scan_sort", workloads.scan_sort)):
+        t0 = time.perf_counter()
+        d = fn(ns, 0, 1)
+        out[key] = {k: v for k, v in d.items() if k not in drop}
+        out[key]["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def cpu_baseline_particles(steps=3):
@@ -364,52 +435,81 @@ def cpu_baseline_particles(steps=3):
             "sample": f"{steps} steps of the same {n} particles (oracle, OpenMP)"}
 
 
-def cpu_baseline_gray_scott(cfg, steps=None):
+def _gs_cpu_sample(explicit_steps: int, reps: int, warm: int = 1):
+    """Runs in a child process that imports only numpy and the oracle (no torch, no CUDA
+    context, one OpenMP runtime): times `reps` forward solves of `explicit_steps` steps
+    of the Gray-Scott lattice with the oracle's float32 port (vectorised C, OpenMP over
+    rows) after `warm` untimed ones; prints one JSON line."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    n = cfg.n
+    from inchman_b200.gray_scott import GrayScottConfig
+    cfg = GrayScottConfig()
     u0, v0 = cfg.initial_state(np.float32)
-    cores = os.cpu_count() or 1
-    k = steps or 200
-    u, v = u0.copy(), v0.copy()
-    t0 = time.perf_counter()
-    oracle.orc().orc_gs_forward_f32(n, k, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt, oracle.ptr(u),
-                                    oracle.ptr(v))
-    t = time.perf_counter() - t0
-    if t < 5.0 and steps is None:
-        k = int(min(20000, max(200, k * 10.0 / max(t, 1e-3))))
+    L = oracle.orc()
+
+    def one():
         u, v = u0.copy(), v0.copy()
+        L.orc_gs_forward_f32(cfg.n, explicit_steps, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt,
+                             oracle.ptr(u), oracle.ptr(v))
+
+    for _ in range(warm):
+        one()
+    times = []
+    for _ in range(reps):
         t0 = time.perf_counter()
-        oracle.orc().orc_gs_forward_f32(n, k, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt, oracle.ptr(u),
-                                        oracle.ptr(v))
-        t = time.perf_counter() - t0
-    return {"value": n * n * k / t, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-            "sample": f"{k} explicit steps of the 256x256 lattice (OpenMP, {cores} threads)"}
+        one()
+        times.append(time.perf_counter() - t0)
+    print(json.dumps({"times": times, "threads": os.environ.get("OMP_NUM_THREADS") or os.cpu_count()}), flush=True)
+
+
+def gs_cpu_times(explicit_steps: int, reps: int, warm: int = 1):
+    """Per-solve seconds of the CPU port, measured in a clean child process (the same
+    measurement for the reported cpu_baseline and for the reference arm)."""
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--gs-cpu-sample",
+                          f"{explicit_steps},{reps},{warm}"], capture_output=True, text=True, env=env, check=True)
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    return d["times"], int(d["threads"])
+
+
+# The CPU measures the whole 10,000-step solve, not a prefix of it: the port's speed
+# changes along the trajectory (as v decays, many values become subnormal and the
+# CPU's arithmetic on them is slow), so a shorter sample would not stand for the
+# workload.  One solve takes about a second on a 16-core host.
+CPU_SAMPLE_STEPS = 10_000
+
+
+def cpu_baseline_gray_scott(cfg, reps=3):
+    times, threads = gs_cpu_times(CPU_SAMPLE_STEPS, reps)
+    t = sum(times)
+    return {"value": cfg.n * cfg.n * CPU_SAMPLE_STEPS * reps / t, "unit": "cell-steps/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{reps} full solves of the workload ({CPU_SAMPLE_STEPS} explicit steps of the 256x256 "
+                      f"lattice) by the oracle's vectorised float32 port, bit-identical to the GPU kernel; "
+                      f"OpenMP, {threads} threads, clean child process"}
 
 
 def reference_gray_scott(args, rank, world):
-    """The reference's CPU implementation of the path: the oracle restatement (the
-    reference's deterministic reaction kernels need generated code, so the reference
-    itself does not build for this network), all host threads."""
+    """The reference's CPU implementation of the path: the oracle's port of the explicit
+    step (the reference's deterministic reaction kernel is code it generates per model,
+    so the reference itself does not build for this network), all host threads; each
+    bench step is one full solve of the workload (CPU_SAMPLE_STEPS explicit steps),
+    timed in the same clean child process as the other arm's cpu_baseline."""
     from inchman_b200.gray_scott import GrayScottConfig
     cfg = GrayScottConfig()
-    sample = 100
-    for _ in range(args.warmup):
-        cpu_baseline_gray_scott(cfg, steps=10)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        cpu_baseline_gray_scott(cfg, steps=sample)
-    t = time.perf_counter() - t0
-    v = cfg.n * cfg.n * sample * args.steps / t
-    cores = os.cpu_count() or 1
+    times, cores = gs_cpu_times(CPU_SAMPLE_STEPS, args.steps, warm=max(1, min(args.warmup, 2)))
+    t = sum(times)
+    v = cfg.n * cfg.n * CPU_SAMPLE_STEPS * args.steps / t
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
             "config": {"workload": "gray_scott_256x256_periodic_fp32_10000_steps",
-                       "sample_explicit_steps_per_bench_step": sample},
+                       "sample_explicit_steps_per_bench_step": CPU_SAMPLE_STEPS},
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-                             "sample": f"{sample} explicit steps of the 256x256 lattice per bench step"},
+                             "sample": f"one full solve ({CPU_SAMPLE_STEPS} explicit steps of the 256x256 "
+                                       f"lattice) per bench step"},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -423,7 +523,14 @@ def main(argv=None):
     ap.add_argument("--instances", type=int, default=4096, help="ensemble workload: number of instances")
     ap.add_argument("--plain-sample", type=int, default=24, help="ensemble workload: instances timed plain")
     ap.add_argument("--t-sample", type=float, default=0.5, help="lotka_volterra workload: simulated time")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="default workload: only the Gray-Scott line, without the other paths' blocks")
+    ap.add_argument("--gs-cpu-sample", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
+    if args.gs_cpu_sample:
+        k, reps, warm = (int(v) for v in args.gs_cpu_sample.split(","))
+        _gs_cpu_sample(k, reps, warm)
+        return 0
     args.warmup = max(args.warmup, 3) if args.impl != "reference" else args.warmup
     rank, world, local = dist_setup(args)
     if args.impl == "reference":

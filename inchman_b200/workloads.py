@@ -32,22 +32,28 @@ def _base(args, world, metric_value, unit, workload, cfg, ms_per_step, extra):
 
 def ssa_plain(args, rank, world):
     """Homogeneous SSA + diffusion, 32 x 32, A+B<->C, 16 realisations, t = 10:
-    the reference's structure (one solver per realisation, wait after every launch)
-    against one launch per kernel for all 16 realisations."""
+    the reference's structure (one solver per realisation, a wait after every launch)
+    against the persistent batched kernel and the wide solver (one launch per kernel
+    for all 16 realisations).  Plain realisation r and batched instance r use the same
+    random streams (key (seed + r, 0)), so their final states are bit-identical: the
+    same statistics by construction; the wide solver keys realisation r as (seed, r)."""
     import torch
     from .model import plain_ssa_model
     from .solver import Solver
     m = plain_ssa_model(width=32, max_time=10.0)
     R, seed = 16, 1234
     lam = [100.0, 100.0, 0.0]
+    finals = {}
 
     def run_plain():
-        steps = 0
+        steps, out = 0, []
         for r in range(R):
             with Solver(m, realisations=1, seed=seed + r, sync_each_launch=True) as s:
                 s.init_poisson(lam)
                 _, _, n = s.solve(count_only=True)
+                out.append(s.get_state()[0])
                 steps += n
+        finals["plain"] = np.stack(out)
         return steps
 
     def run_wide():
@@ -56,8 +62,8 @@ def ssa_plain(args, rank, world):
             _, _, n = s.solve(count_only=True)
         return n * R
 
-    from .ensemble import Ensemble, autotune, replicate
-    specs = replicate(m, lam, R, seed)
+    from .ensemble import Ensemble, InstanceSpec, autotune
+    specs = [InstanceSpec(m, list(lam), seed + r, 0) for r in range(R)]
     (thr, cps), _ = autotune(specs)
     ens = Ensemble(specs)
     ens.configure(thr, cps)
@@ -67,31 +73,39 @@ def ssa_plain(args, rank, world):
         ens.init_poisson(est)
         ens.run(est)
         _, st, _ = ens.results()
+        finals["batched"] = est.view(R, m.num_species, m.height, m.width).cpu().numpy()
         return int(st.sum())
 
     res = {}
     for name, fn in (("plain", run_plain), ("wide", run_wide), ("batched", run_batched)):
-        for _ in range(1):
-            fn()
+        fn()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         steps = fn()
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
         res[name] = (m.area * steps / t, t)
+    same = bool(np.array_equal(finals["plain"], finals["batched"]))
     return _base(args, world, res["batched"][0], "cell-steps/s", "ssa_homogeneous_32x32_ABC_16real_t10",
-                 {"grid": [32, 32], "realisations": R, "t_end": 10.0}, res["batched"][1] * 1e3,
+                 {"grid": [32, 32], "realisations": R, "t_end": 10.0,
+                  "launch": {"threads": thr, "ctas_per_sm": cps}}, res["batched"][1] * 1e3,
                  {"plain": {"value": res["plain"][0], "seconds": res["plain"][1]},
                   "wide": {"value": res["wide"][0], "seconds": res["wide"][1]},
                   "batched_over_plain": res["batched"][0] / res["plain"][0],
-                  "wide_over_plain": res["wide"][0] / res["plain"][0]})
+                  "wide_over_plain": res["wide"][0] / res["plain"][0],
+                  "same_stats": "bit-identical final states (plain vs batched)" if same else "MISMATCH",
+                  "bit_identical": same})
 
 
 def ensemble(args, rank, world):
     """4096 random heterogeneous instances (side 16..128, 4..12 species, 8..32
     reactions), t = 5, in one persistent kernel (launch shape from the autotuner),
     against the reference's structure -- one solver per instance, a wait after every
-    launch -- timed on a sample of the instances and compared per cell-step."""
+    launch -- timed on a sample of the instances and compared per cell-step.  A plain
+    instance runs the same random streams as in the batch, so its final state must be
+    bit-identical to the batched one (checked for every sampled instance).  The
+    persistent kernel is warmed up on a 64-instance ensemble, then the whole ensemble
+    runs once, timed (one launch of 20 s: launch overheads do not show)."""
     import torch
     from .ensemble import Ensemble, autotune, random_ensemble
     from .solver import Solver
@@ -99,16 +113,21 @@ def ensemble(args, rank, world):
     n = max(1, n)
     specs = random_ensemble(n, seed=2024, max_time=5.0)
     (thr, cps), tune = autotune(specs)
+    warm = Ensemble(specs[:64])
+    warm.configure(thr, cps)
+    ws = warm.alloc_state()
+    for _ in range(max(1, int(getattr(args, "warmup", 3)))):
+        warm.init_poisson(ws)
+        warm.run(ws)
+    torch.cuda.synchronize()
+    del warm, ws
     ens = Ensemble(specs)
     ens.configure(thr, cps)
     state = ens.alloc_state()
     ens.init_poisson(state)
-    ens.run(state)                    # capture + warm-up
-    torch.cuda.synchronize()
-    ens.init_poisson(state)
     a, b = _events()
     a.record()
-    ens.run(state)
+    ens.run(state)                    # graph capture (no work) + one replay
     b.record()
     torch.cuda.synchronize()
     t = a.elapsed_time(b) / 1e3
@@ -117,8 +136,8 @@ def ensemble(args, rank, world):
     batched = cs / t
     # plain: the reference's structure on a sample of the instances
     k = int(getattr(args, "plain_sample", 24))
-    pick = np.random.default_rng(1).choice(n, size=k, replace=False)
-    pcs, pt = 0, 0.0
+    pick = np.random.default_rng(1).choice(n, size=min(k, n), replace=False)
+    pcs, pt, same = 0, 0.0, True
     for i in pick:
         sp = specs[int(i)]
         with Solver(sp.model, realisations=1, seed=sp.seed, sync_each_launch=True) as s:
@@ -129,13 +148,19 @@ def ensemble(args, rank, world):
             torch.cuda.synchronize()
             pt += time.perf_counter() - t0
             pcs += sp.model.area * nsteps
+            fin = s.get_state()[0]
+        same = same and nsteps == int(steps[int(i)]) and \
+            np.array_equal(fin, ens.instance_state(state, int(i)).cpu().numpy())
     plain = pcs / pt
     return _base(args, world, batched, "cell-steps/s", "ensemble_4096_random_instances_t5",
                  {"instances": n, "launch": {"threads": thr, "ctas_per_sm": cps}, "autotune_ms": tune.get("ms")},
                  t * 1e3,
-                 {"plain": {"value": plain, "sample_instances": k, "seconds": pt},
+                 {"plain": {"value": plain, "sample_instances": len(pick), "seconds": pt},
                   "batched_over_plain": batched / plain, "instances_with_status": int((status != 0).sum()),
-                  "cell_steps": cs})
+                  "same_stats": ("bit-identical final states on the sampled instances" if same else "MISMATCH"),
+                  "bit_identical": bool(same), "cell_steps": cs,
+                  # the graph holds two memset nodes and one k_ensemble launch
+                  "gpu_launches": 1})
 
 
 def lotka_volterra(args, rank, world):
