@@ -104,6 +104,11 @@ void orc_ref_rk4(const orc_model* m, float* state, float deltat);
 int orc_ref_solve(const orc_model* m, int32_t* state, uint32_t seed_base,
                   int32_t* snapshots, float* snap_times, int max_snapshots, int* num_snapshots, int64_t* steps);
 void orc_ref_solve_many(const orc_model* m, const int32_t* init, int R, uint32_t seed_base, int32_t* finals);
+int orc_ref_solve_inhom(const orc_model* m, int32_t* state, uint32_t seed_base, const float* Dx, const float* Dy,
+                        const float* rx, const float* ry, int32_t* snaps, float* snap_times, int max_snaps,
+                        int* nsnap, int64_t* steps);
+void orc_ref_solve_many_snaps(const orc_model* m, const int32_t* init, int R, uint32_t seed_base, const float* Dx,
+                              const float* Dy, const float* rx, const float* ry, int max_snaps, int32_t* snaps);
 
 /* ---- replay of the CUDA algorithms --------------------------------------------- */
 void orc_rep_init_poisson(int W, int H, int S, int R, uint32_t seed, const float* lambda_per_species, int32_t* state);

@@ -60,6 +60,8 @@ def orc():
             "orc_ref_rk4": (None, [vp, vp, f32]),
             "orc_ref_solve": (C.c_int, [vp, vp, u32, vp, vp, C.c_int, P(C.c_int), P(i64)]),
             "orc_ref_solve_many": (None, [vp, vp, C.c_int, u32, vp]),
+            "orc_ref_solve_inhom": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_int, P(C.c_int), P(i64)]),
+            "orc_ref_solve_many_snaps": (None, [vp, vp, C.c_int, u32, vp, vp, vp, vp, C.c_int, vp]),
             "orc_rep_init_poisson": (None, [C.c_int, C.c_int, C.c_int, C.c_int, u32, vp, vp]),
             "orc_rep_ssa": (None, [vp, vp, C.c_int, u32, u32, f32, vp]),
             "orc_rep_homog_diffuse": (None, [vp, vp, C.c_int, u32, C.c_int, u32]),

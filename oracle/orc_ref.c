@@ -298,10 +298,12 @@ float orc_ref_timestep(const orc_model* m, int species, int sweep_y,
         } else if (diffHere == 0) {
             timeStep = (float)(deltax / fabs(rx));
         } else {
+            /* tanh and sinh of the float epsx are the float functions in OpenCL C
+             * (overloads), and their products with floats stay float */
             float epsx = (float)(deltax * rx / (2. * diffHere));
-            float temp = (float)(1. + (-1. / (tanh(epsx) * epsx) + 1. / (sinh(epsx) * sinh(epsx))));
+            float temp = (float)(1. + (-1. / (tanhf(epsx) * epsx) + 1. / (sinhf(epsx) * sinhf(epsx))));
             if (temp <= 0) temp = (float)(1. / 3.);
-            timeStep = (float)(deltax / rx * tanh(epsx) * temp);
+            timeStep = deltax / rx * tanhf(epsx) * temp;
         }
         if (per_cell) per_cell[c] = timeStep;
         best = fminf(best, timeStep);
@@ -457,6 +459,101 @@ int orc_ref_solve(const orc_model* m, int32_t* state, uint32_t seed_base,
     *steps_out = n;
     free(dtv); free(next); free(lost);
     return 0;
+}
+
+/* DiffusionModel.cpp:1414-1603 for stochastic_inhomogeneous with a linear drift /
+ * diffusivity field (Dx, Dy, rx, ry: [S][H][W], the arrays computeDiffusivityDrift
+ * fills once): first time steps per species and direction from the per-cell
+ * minimum (InhomogeneousSolver.cpp:193-212, StochasticInhomogeneousDriftDiffusion.cl:
+ * 124-151 and the block reduction), next diffusion time of a species = the earlier of
+ * its x and y clocks (:238-252), diffuse() sweeps x when its clock is due, then y
+ * (:254-427), each sweep with the step's seed, which then advances; the time steps
+ * stay fixed (no nonlinear method).  Seeds as orc_ref_solve. */
+int orc_ref_solve_inhom(const orc_model* m, int32_t* state, uint32_t seed_base, const float* Dx, const float* Dy,
+                        const float* rx, const float* ry, int32_t* snaps, float* snap_times, int max_snaps,
+                        int* nsnap, int64_t* steps_out) {
+    const int S = m->num_species;
+    const size_t area = (size_t)m->width * m->height;
+    float* dtx = (float*)malloc(sizeof(float) * S);
+    float* dty = (float*)malloc(sizeof(float) * S);
+    float* nx = (float*)malloc(sizeof(float) * S);
+    float* ny = (float*)malloc(sizeof(float) * S);
+    int32_t* lost = (int32_t*)malloc(sizeof(int32_t) * 4 * area);
+    for (int i = 0; i < S; ++i) {
+        dtx[i] = orc_ref_timestep(m, i, 0, Dx, Dy, rx, ry, NULL);
+        dty[i] = orc_ref_timestep(m, i, 1, Dx, Dy, rx, ry, NULL);
+        nx[i] = dtx[i];
+        ny[i] = dty[i];
+    }
+    int ns = 0;
+#define SNAP(t) do { if (ns < max_snaps) { memcpy(snaps + (size_t)ns * S * area, state, sizeof(int32_t) * S * area); \
+                      snap_times[ns] = (t); } ns++; } while (0)
+    SNAP(0.f);
+    float simTime = 0.f, outputLast = 0.f;
+    int64_t n = 0;
+    while ((m->max_steps < 0 || n < m->max_steps) && simTime < m->max_time) {
+        int32_t seed = (int32_t)(orc_hash32(seed_base, (uint32_t)n) & 0x7fffffffu);
+        n++;
+        float mindt = nx[0] < ny[0] ? nx[0] : ny[0];
+        int minspec = 0;
+        for (int i = 1; i < S; ++i) {
+            const float t = nx[i] < ny[i] ? nx[i] : ny[i];
+            if (t < mindt) { mindt = t; minspec = i; }
+        }
+        int ev = 0;
+        const float mo = outputLast + m->output_interval;
+        if (mo < mindt) { mindt = mo; ev = 1; }
+        const float deltat = mindt - simTime;
+        if (m->num_reactions > 0) { orc_ref_gillespie(m, state, seed, deltat); seed++; }
+        if (ev == 0) {
+            for (int i = 0; i < S; ++i) {
+                const float t = nx[i] < ny[i] ? nx[i] : ny[i];
+                if (!(i == minspec || t <= mindt) || !(t > 0)) continue;
+                if (nx[i] <= mindt) {
+                    orc_ref_inhomog_diffuse(m, state, i, seed, dtx[i], 0, Dx, Dy, rx, ry, lost);
+                    seed++;
+                    nx[i] += dtx[i];
+                }
+                if (ny[i] <= mindt) {
+                    orc_ref_inhomog_diffuse(m, state, i, seed, dty[i], 1, Dx, Dy, rx, ry, lost);
+                    seed++;
+                    ny[i] += dty[i];
+                }
+            }
+        } else if (simTime >= outputLast + m->output_interval) {
+            SNAP(mindt);
+            outputLast += m->output_interval;
+        }
+        simTime = mindt;
+    }
+    SNAP(simTime);
+#undef SNAP
+    *nsnap = ns;
+    *steps_out = n;
+    free(dtx); free(dty); free(nx); free(ny); free(lost);
+    return 0;
+}
+
+/* R reference-exact runs (homogeneous, or inhomogeneous with fields when Dx is not
+ * NULL) from one initial state, OpenMP over the runs (seed base seed_base + 7919 r);
+ * every run's first max_snaps snapshots go to snaps [R][max_snaps][S][H][W]. */
+void orc_ref_solve_many_snaps(const orc_model* m, const int32_t* init, int R, uint32_t seed_base, const float* Dx,
+                              const float* Dy, const float* rx, const float* ry, int max_snaps, int32_t* snaps) {
+    const size_t block = (size_t)m->num_species * m->width * m->height;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < R; ++r) {
+        int32_t* st = (int32_t*)malloc(sizeof(int32_t) * block);
+        memcpy(st, init, sizeof(int32_t) * block);
+        float* t = (float*)malloc(sizeof(float) * (size_t)max_snaps);
+        int ns;
+        int64_t steps;
+        int32_t* out = snaps + (size_t)r * max_snaps * block;
+        if (Dx) orc_ref_solve_inhom(m, st, seed_base + (uint32_t)r * 7919u, Dx, Dy, rx, ry, out, t, max_snaps, &ns,
+                                    &steps);
+        else orc_ref_solve(m, st, seed_base + (uint32_t)r * 7919u, out, t, max_snaps, &ns, &steps);
+        free(st);
+        free(t);
+    }
 }
 
 /* R independent reference-exact runs from the same initial state (OpenMP over the

@@ -194,3 +194,68 @@ def test_localised_reactions_stay_off_outside_their_regions_on_the_cpu():
     oracle.orc().orc_ref_rk4(oracle.model_ptr(desc), oracle.ptr(fs), 0.5)
     assert (fs[0][~inside] == 30).all() and (fs[0][inside] < 30).all()
     np.testing.assert_allclose(fs.sum(axis=0), 30.0, rtol=1e-6)
+
+
+def _c3_shaped(W=6, max_time=0.3, seed=3):
+    """Lotka-Volterra kinetics, lognormal(0, 0.5) diffusivity and a sinusoidal drift
+    kept away from zero (0.25 +- 0.1), reflecting walls: the drift-diffusion model of
+    the 512 x 512 workload at test size.  The fields are symmetric under x <-> y (D
+    symmetric, rx = f(y), ry = f(x)), so the smallest time steps of the two directions
+    are the same number in the reference's float formula and in the solver's double
+    one, and both sweep x and y in the same events; with unequal steps the order of
+    the two clocks' events depends on the last bits of the time steps."""
+    H = W
+    from inchman_b200 import _lib
+    from inchman_b200.model import DiffusionModel
+    m = DiffusionModel(width=W, height=H, physical_length=float(W), p0=0.1, max_time=max_time,
+                       output_interval=max_time / 2, solver=_lib.STOCHASTIC_INHOMOGENEOUS,
+                       drift_method=_lib.DRIFT_FIELD)
+    m.add_species("X", 1.0, 30.0).add_species("Y", 1.0, 30.0)
+    m.add_reaction("birth", {"X": 1}, {"X": 2}, 1.0)
+    m.add_reaction("predation", {"X": 1, "Y": 1}, {"Y": 2}, 0.005)
+    m.add_reaction("death", {"Y": 1}, {}, 0.6)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    D = rng.lognormal(0.0, 0.5, size=(H, W))
+    D = np.triu(D) + np.triu(D, 1).T
+    D = D.astype(np.float32)
+    y, x = np.meshgrid(np.arange(H, dtype=np.float64), np.arange(W, dtype=np.float64), indexing="ij")
+    rx = (0.25 + 0.1 * np.sin(2 * np.pi * y / H)).astype(np.float32)
+    ry = (0.25 + 0.1 * np.sin(2 * np.pi * x / W)).astype(np.float32)
+    m.field_dx = np.stack([D, D]); m.field_dy = np.stack([D, D])
+    m.field_rx = np.stack([rx, rx]); m.field_ry = np.stack([ry, ry])
+    return m
+
+
+def _ref_many(m, init, R, seed_base, max_snaps):
+    desc, keep = m.to_desc()
+    block = m.num_species * m.area
+    snaps = np.zeros((R, max_snaps, block), np.int32)
+    f = [np.ascontiguousarray(a, np.float32) for a in (m.field_dx, m.field_dy, m.field_rx, m.field_ry)]
+    oracle.orc().orc_ref_solve_many_snaps(oracle.model_ptr(desc), oracle.ptr(np.ascontiguousarray(init[0])), R,
+                                          seed_base, *[oracle.ptr(a) for a in f], max_snaps, oracle.ptr(snaps))
+    return snaps
+
+
+def test_inhomogeneous_replay_matches_reference_statistics():
+    """Drift-diffusion: the replay (binomial sweeps, Philox) and the reference-exact
+    restatement of the inhomogeneous event loop (one Threefry uniform per particle and
+    sweep, the reference's time steps and seeding) agree in per-cell mean and variance
+    at both output windows."""
+    from scipy import stats
+    m = _c3_shaped()
+    desc, keep = m.to_desc()
+    R = 1500
+    init = oracle.init_poisson(m.width, m.height, 2, 1, 11, [30.0, 30.0])
+    st, rs, rt, rsteps, _ = oracle.rep_solve(desc, np.repeat(init, R, axis=0), R, 77, 8)
+    ref = _ref_many(m, init, R, 5000, 3)
+    assert rs.shape[0] == 3
+    for w in (1, 2):
+        a = rs[w].reshape(R, -1).astype(np.float64)
+        b = ref[:, w].astype(np.float64)
+        se = np.sqrt(a.var(0, ddof=1) / R + b.var(0, ddof=1) / R) + 1e-12
+        z = np.abs(a.mean(0) - b.mean(0)) / se
+        alpha = 1e-3 / z.size
+        assert (z < stats.norm.isf(alpha / 2)).all(), (w, z.max())
+        f = a.var(0, ddof=1) / np.maximum(b.var(0, ddof=1), 1e-12)
+        lo, hi = stats.f.ppf(alpha / 2, R - 1, R - 1), stats.f.isf(alpha / 2, R - 1, R - 1)
+        assert ((b.var(0) == 0) | ((f > lo) & (f < hi))).all(), w

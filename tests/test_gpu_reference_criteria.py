@@ -60,40 +60,101 @@ def test_homogeneous_point_source_diffusion(gpgmp):
     assert rmsex <= 5e-4 and rmsey <= 5e-4, (rmsex, rmsey)
 
 
-def test_statistics_match_reference_exact_restatement_1e4_realisations(gpgmp):
-    """A+B <-> C with diffusion on an 8 x 8 lattice (one absorbing wall), t = 0.2,
-    10,000 realisations from one initial state: per-cell, per-species mean (z-test),
-    variance (F-test) and distribution (two-sample KS) of the GPU solver against the
-    reference-exact restatement (Threefry keyed per cell, one uniform per particle,
-    the reference's seeding pattern), Bonferroni-corrected alpha = 1e-3."""
+def _compare_windows(gpu, ref, windows, label):
+    """Per-cell, per-species mean (z-test), variance (F-test) and distribution
+    (two-sample KS) of each output window, Bonferroni over cells, species, windows
+    and the three tests; alpha = 1e-3 in all."""
     from scipy import stats
-    from helpers import small_homog
+    R = gpu.shape[0]
+    k = gpu.shape[2] * len(windows)
+    alpha = 1e-3 / (3 * k)
+    for w in windows:
+        a = gpu[:, w].astype(np.float64)
+        b = ref[:, w].astype(np.float64)
+        se = np.sqrt(a.var(0, ddof=1) / R + b.var(0, ddof=1) / R) + 1e-12
+        z = np.abs(a.mean(0) - b.mean(0)) / se
+        assert (z < stats.norm.isf(alpha / 2)).all(), (label, w, z.max())
+        va, vb = a.var(0, ddof=1), b.var(0, ddof=1)
+        ok = (va == 0) & (vb == 0)
+        f = va / np.where(vb > 0, vb, 1)
+        lo, hi = stats.f.ppf(alpha / 2, R - 1, R - 1), stats.f.isf(alpha / 2, R - 1, R - 1)
+        assert (ok | ((f > lo) & (f < hi))).all(), (label, w)
+        pmin = min(stats.ks_2samp(a[:, j], b[:, j]).pvalue for j in range(a.shape[1]) if not ok[j])
+        assert pmin > alpha, (label, w, pmin)
+
+
+def _gpu_windows(m, init, R, seed, nsnap):
     from inchman_b200.solver import Solver
-    m = small_homog(W=8, H=8, max_time=0.2, bmask=(0, 1, 0, 0))
-    for sp, lam in zip(m.species, (20.0, 15.0, 3.0)):
-        sp.initial = lam
+    with Solver(m, realisations=R, seed=seed) as s:
+        s.set_state(np.repeat(init, R, axis=0))
+        snaps, times, steps = s.solve(max_snapshots=nsnap)
+        assert (s.status() == 0).all()
+    return snaps.reshape(snaps.shape[0], R, -1).transpose(1, 0, 2), times
+
+
+def test_statistics_match_reference_exact_restatement_1e4_realisations(gpgmp):
+    """Config 1's network and shape (A + B <-> C, k1 = 0.01, k2 = 0.1, D = (1, 1, 0.5),
+    32 x 32, h = 1, p0 = 0.1, reflecting walls) at lower counts (A, B ~ Poisson(60),
+    about ten reaction events per cell) and t = 0.3 with outputs every 0.1 -- three
+    output windows -- over 10,000
+    realisations from one initial state: the GPU solver against the reference-exact
+    restatement (Threefry keyed per cell, one uniform per particle, the reference's
+    seeding pattern and event loop), every window compared."""
+    from inchman_b200.model import plain_ssa_model
+    m = plain_ssa_model(width=32, max_time=0.3)
+    m.output_interval = 0.1
     desc, keep = m.to_desc()
     R = 10_000
-    init = oracle.init_poisson(m.width, m.height, m.num_species, 1, 5, [s.initial for s in m.species])
-    with Solver(m, realisations=R, seed=4242) as s:
-        s.set_state(np.repeat(init, R, axis=0))
-        s.solve(count_only=True)
-        gpu = s.get_state().reshape(R, -1).astype(np.float64)
-    ref = np.zeros((R,) + init.shape[1:], np.int32)
-    oracle.orc().orc_ref_solve_many(oracle.model_ptr(desc), oracle.ptr(init), R, 1000, oracle.ptr(ref))
-    ref = ref.reshape(R, -1).astype(np.float64)
-    k = gpu.shape[1]
-    alpha = 1e-3 / (3 * k)
-    se = np.sqrt(gpu.var(0, ddof=1) / R + ref.var(0, ddof=1) / R) + 1e-12
-    z = np.abs(gpu.mean(0) - ref.mean(0)) / se
-    assert (z < stats.norm.isf(alpha / 2)).all(), z.max()
-    vg, vr = gpu.var(0, ddof=1), ref.var(0, ddof=1)
-    ok = (vr == 0) & (vg == 0)
-    f = vg / np.where(vr > 0, vr, 1)
-    lo, hi = stats.f.ppf(alpha / 2, R - 1, R - 1), stats.f.isf(alpha / 2, R - 1, R - 1)
-    assert (ok | ((f > lo) & (f < hi))).all()
-    pmin = min(stats.ks_2samp(gpu[:, j], ref[:, j]).pvalue for j in range(k))
-    assert pmin > alpha, pmin
+    init = oracle.init_poisson(m.width, m.height, m.num_species, 1, 5, [60.0, 60.0, 0.0])
+    gpu, times = _gpu_windows(m, init, R, 4242, 4)
+    nw = gpu.shape[1]
+    assert nw == 4 and np.allclose(times, [0.0, 0.1, 0.2, 0.3], atol=1e-5)
+    block = m.num_species * m.area
+    ref = np.zeros((R, nw, block), np.int32)
+    oracle.orc().orc_ref_solve_many_snaps(oracle.model_ptr(desc), oracle.ptr(np.ascontiguousarray(init[0])), R, 1000,
+                                          None, None, None, None, nw, oracle.ptr(ref))
+    _compare_windows(gpu, ref, [1, 2, 3], "homogeneous")
+
+
+def test_drift_diffusion_statistics_match_reference_exact_restatement_1e4_realisations(gpgmp):
+    """The drift-diffusion workload's model (Lotka-Volterra X -> 2X 1.0, X + Y -> 2Y
+    0.005, Y -> 0 0.6; lognormal(0, 0.5) diffusivity; sinusoidal drift, here 0.25 +-
+    0.1 so that no cell's drift is near zero, where the reference's float time-step
+    formula loses its digits; reflecting walls) on 12 x 12 cells, X, Y ~ Poisson(40),
+    t = 0.4 with two output windows, 10,000 realisations: the GPU solver's binomial
+    sweeps against the reference-exact restatement of the inhomogeneous event loop
+    (InhomogeneousSolver.cpp:254-427 with one uniform per particle and sweep,
+    StochasticInhomogeneousDriftDiffusion.cl:426-723).  The fields are symmetric under
+    x <-> y so that both implementations' x and y time steps are equal and their
+    sweeps fall in the same events."""
+    from inchman_b200 import _lib
+    from inchman_b200.model import DiffusionModel
+    W = 12
+    m = DiffusionModel(width=W, height=W, physical_length=float(W), p0=0.1, max_time=0.4, output_interval=0.2,
+                       solver=_lib.STOCHASTIC_INHOMOGENEOUS, drift_method=_lib.DRIFT_FIELD)
+    m.add_species("X", 1.0).add_species("Y", 1.0)
+    m.add_reaction("birth", {"X": 1}, {"X": 2}, 1.0)
+    m.add_reaction("predation", {"X": 1, "Y": 1}, {"Y": 2}, 0.005)
+    m.add_reaction("death", {"Y": 1}, {}, 0.6)
+    rng = np.random.Generator(np.random.PCG64(12))
+    D = rng.lognormal(0.0, 0.5, size=(W, W))
+    D = (np.triu(D) + np.triu(D, 1).T).astype(np.float32)
+    y, x = np.meshgrid(np.arange(W, dtype=np.float64), np.arange(W, dtype=np.float64), indexing="ij")
+    rx = (0.25 + 0.1 * np.sin(2 * np.pi * y / W)).astype(np.float32)
+    ry = (0.25 + 0.1 * np.sin(2 * np.pi * x / W)).astype(np.float32)
+    m.field_dx = np.stack([D, D]); m.field_dy = np.stack([D, D])
+    m.field_rx = np.stack([rx, rx]); m.field_ry = np.stack([ry, ry])
+    desc, keep = m.to_desc()
+    R = 10_000
+    init = oracle.init_poisson(W, W, 2, 1, 8, [40.0, 40.0])
+    gpu, times = _gpu_windows(m, init, R, 99, 3)
+    nw = gpu.shape[1]
+    assert nw == 3
+    f = [np.ascontiguousarray(a, np.float32) for a in (m.field_dx, m.field_dy, m.field_rx, m.field_ry)]
+    ref = np.zeros((R, nw, 2 * W * W), np.int32)
+    oracle.orc().orc_ref_solve_many_snaps(oracle.model_ptr(desc), oracle.ptr(np.ascontiguousarray(init[0])), R, 77,
+                                          *[oracle.ptr(a) for a in f], nw, oracle.ptr(ref))
+    _compare_windows(gpu, ref, [1, 2], "drift-diffusion")
 
 
 def test_homogeneous_drift_diffusion(gpgmp):
