@@ -132,6 +132,10 @@ SIGNATURES = {
     "gpgmp_solve_with_callback": (C.c_int, [vp, vp, P(f32), i32, P(i32), P(i64), vp, vp]),
     "gpgmp_get_individuals": (C.c_int, [vp, i32, vp, vp, vp, i64, P(i64)]),
     "gpgmp_set_individual_properties": (C.c_int, [vp, i32, vp, i64, i64]),
+    "gpgmp_solver_launch_choices": (C.c_int, [P(i32), P(i32), P(i32), P(i32), P(i32)]),
+    "gpgmp_solver_set_launch": (C.c_int, [vp, i32, i32, i32]),
+    "gpgmp_solver_get_launch": (C.c_int, [vp, P(i32), P(i32), P(i32)]),
+    "gpgmp_solver_autotune": (C.c_int, [vp, f32, i32, P(f32), P(f32)]),
 }
 
 

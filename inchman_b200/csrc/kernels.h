@@ -7,6 +7,8 @@
 namespace gpgmp {
 
 constexpr int kMaxSpecies = 32;
+constexpr int kNumDiffusionTiles = 6;     // diffusion tile shapes (diffusion_tile_shape)
+constexpr int kNumSsaThreadChoices = 3;   // SSA block sizes (ssa_thread_choice)
 
 // Per-species plane bases: species s of realisation r, cell c lives at
 // planes.p[s][(r * S + s) * area + c].  The two state buffers alternate per
@@ -25,7 +27,14 @@ struct GridDesc {
     // cell set where reaction r may fire; NULL when every reaction fires everywhere
     const uint32_t* rmask;
     int rmask_words;
+    // launch shapes: index of the diffusion tile shape and of the SSA block size (0:
+    // the defaults, 32 x 16 cells and 128 threads); the results do not depend on them
+    int tile;
+    int ssa_threads;
 };
+// the tile of shape index i is w x h cells; SSA block size choice i is that many threads
+void diffusion_tile_shape(int index, int* w, int* h);
+int ssa_thread_choice(int index);
 
 cudaError_t launch_init_poisson(const GridDesc& g, Planes planes, uint32_t seed, const float* d_lambda,
                                 cudaStream_t st);

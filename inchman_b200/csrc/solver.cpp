@@ -812,6 +812,149 @@ int gpgmp_next_diffusion_time(gpgmp_solver* h, float* out) {
     return GPGMP_OK;
 }
 
+int gpgmp_solver_set_launch(gpgmp_solver* h, int32_t tile_w, int32_t tile_h, int32_t ssa_threads) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    int tile = -1, ssa = -1;
+    for (int i = 0; i < kNumDiffusionTiles; ++i) {
+        int w, hh;
+        diffusion_tile_shape(i, &w, &hh);
+        if (w == tile_w && hh == tile_h) tile = i;
+    }
+    for (int i = 0; i < kNumSsaThreadChoices; ++i)
+        if (ssa_thread_choice(i) == ssa_threads) ssa = i;
+    if (tile < 0) return set_error(GPGMP_ERR_INVALID, "no diffusion tile of %d x %d cells", tile_w, tile_h);
+    if (ssa < 0) return set_error(GPGMP_ERR_INVALID, "no SSA block of %d threads", ssa_threads);
+    h->g.tile = tile;
+    h->g.ssa_threads = ssa;
+    return GPGMP_OK;
+}
+
+int gpgmp_solver_get_launch(gpgmp_solver* h, int32_t* tile_w, int32_t* tile_h, int32_t* ssa_threads) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    int w, hh;
+    diffusion_tile_shape(h->g.tile, &w, &hh);
+    if (tile_w) *tile_w = w;
+    if (tile_h) *tile_h = hh;
+    if (ssa_threads) *ssa_threads = ssa_thread_choice(h->g.ssa_threads);
+    return GPGMP_OK;
+}
+
+int gpgmp_solver_launch_choices(int32_t* n_tiles, int32_t* tile_w, int32_t* tile_h, int32_t* n_ssa,
+                                int32_t* ssa_threads) {
+    if (n_tiles) *n_tiles = kNumDiffusionTiles;
+    if (n_ssa) *n_ssa = kNumSsaThreadChoices;
+    for (int i = 0; i < kNumDiffusionTiles; ++i) {
+        int w, hh;
+        diffusion_tile_shape(i, &w, &hh);
+        if (tile_w) tile_w[i] = w;
+        if (tile_h) tile_h[i] = hh;
+    }
+    for (int i = 0; i < kNumSsaThreadChoices; ++i)
+        if (ssa_threads) ssa_threads[i] = ssa_thread_choice(i);
+    return GPGMP_OK;
+}
+
+// Times every diffusion tile shape on species 0's jumps (homogeneous) or x sweep
+// (inhomogeneous), and every SSA block size on one reaction window of `window`, on
+// the solver's current state, and keeps the fastest of each.  The kernels write only
+// the spare half of the state buffers (the diffusion kernels write out of place; the
+// SSA runs on a copy there) and a scratch status array, so the state, the clocks and
+// the status stay as they were.
+int gpgmp_solver_autotune(gpgmp_solver* h, float window, int32_t reps, float* ms_tiles, float* ms_ssa) {
+    if (!h) return set_error(GPGMP_ERR_INVALID, "handle is NULL");
+    if (h->deterministic) return GPGMP_OK;     // the deterministic kernels have no launch choices
+    if (reps < 1) reps = 1;
+    if (!(window > 0.f)) {
+        window = h->m.max_time;
+        for (int i = 0; i < h->g.S; ++i) {
+            const float d = h->inhom ? std::min(h->smallX[i], h->smallY[i]) : h->dt[i];
+            if (d > 0.f && d < window) window = d;
+        }
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    int32_t* d_st = nullptr;
+    int rc = GPGMP_OK;
+    auto fail = [&](cudaError_t e, const char* what) {
+        rc = set_error(GPGMP_ERR_CUDA, "autotune %s: %s", what, cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaMalloc(&d_st, sizeof(int32_t) * (size_t)h->R);
+    if (e != cudaSuccess) fail(e, "set-up");
+    const GridDesc keep = h->g;
+    const float dxw = h->m.physical_length / (float)h->m.width;
+    const int c0 = h->cur[0];
+    // one diffusion launch of tile shape i (in: species 0's current plane, out: the spare one)
+    auto diffusion = [&](GridDesc& g) -> cudaError_t {
+        if (!h->inhom)
+            return launch_homog_diffuse(g, h->d_buf[c0], h->d_buf[1 - c0], 0, h->seed, 1u, h->pmove, h->stream);
+        return launch_sweep(g, h->d_buf[c0], h->d_buf[1 - c0], 0, 0, h->seed, 1u, h->d_Dx, h->d_rx,
+                            h->ddX[0] > 0.f ? h->ddX[0] : h->smallX[0], dxw, h->stream, h->fpe ? 1 : 0);
+    };
+    auto time_it = [&](auto&& launch, float* ms) -> cudaError_t {
+        cudaError_t ee = launch();                               // warm-up (module load, caches)
+        if (ee == cudaSuccess) ee = cudaEventRecord(a, h->stream);
+        for (int k = 0; k < reps && ee == cudaSuccess; ++k) ee = launch();
+        if (ee == cudaSuccess) ee = cudaEventRecord(b, h->stream);
+        if (ee == cudaSuccess) ee = cudaEventSynchronize(b);
+        if (ee == cudaSuccess) ee = cudaEventElapsedTime(ms, a, b);
+        return ee;
+    };
+    int best_tile = keep.tile, best_ssa = keep.ssa_threads;
+    float best = 0.f;
+    for (int i = 0; rc == GPGMP_OK && i < kNumDiffusionTiles; ++i) {
+        GridDesc g = keep;
+        g.tile = i;
+        float ms = 0.f;
+        e = time_it([&] { return diffusion(g); }, &ms);
+        if (e != cudaSuccess) { fail(e, "diffusion"); break; }
+        if (ms_tiles) ms_tiles[i] = ms / reps;
+        if (i == 0 || ms < best) { best = ms; best_tile = i; }
+    }
+    // SSA: a copy of the state in the spare buffers (every species' plane of every
+    // realisation), restored before each block size so each runs the same window
+    const int nreac = (int)h->reactions.size();
+    if (rc == GPGMP_OK && nreac > 0 && !h->jit_ssa) {
+        Planes spare{};
+        for (int s = 0; s < h->g.S; ++s) spare.p[s] = h->d_buf[1 - h->cur[s]];
+        const size_t plane = h->area * sizeof(int32_t);
+        auto restore = [&]() -> cudaError_t {
+            for (int s = 0; s < h->g.S; ++s) {
+                cudaError_t ee = cudaMemcpy2DAsync((char*)spare.p[s] + s * plane, plane * h->g.S,
+                                                   (const char*)h->d_buf[h->cur[s]] + s * plane, plane * h->g.S,
+                                                   plane, (size_t)h->R, cudaMemcpyDeviceToDevice, h->stream);
+                if (ee != cudaSuccess) return ee;
+            }
+            return cudaSuccess;
+        };
+        best = 0.f;
+        for (int i = 0; i < kNumSsaThreadChoices; ++i) {
+            GridDesc g = keep;
+            g.ssa_threads = i;
+            float ms = 0.f, total = 0.f;
+            e = cudaSuccess;
+            for (int k = 0; k < reps && e == cudaSuccess; ++k) {
+                e = restore();
+                if (e == cudaSuccess)
+                    e = time_it([&] { return launch_ssa(g, spare, h->d_reactions, nreac, h->seed, 7u, window, d_st,
+                                                        h->stream); }, &ms);
+                total += ms;
+            }
+            if (e != cudaSuccess) { fail(e, "SSA"); break; }
+            if (ms_ssa) ms_ssa[i] = total / reps;
+            if (i == 0 || total < best) { best = total; best_ssa = i; }
+        }
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (d_st) cudaFree(d_st);
+    if (rc == GPGMP_OK) {
+        h->g.tile = best_tile;
+        h->g.ssa_threads = best_ssa;
+    }
+    return rc;
+}
+
 int gpgmp_timesteps(gpgmp_solver* h, float* dtx, float* dty) {
     if (!h || !dtx || !dty) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (!h->inhom) return set_error(GPGMP_ERR_INVALID, "time steps per direction exist for the inhomogeneous solver");

@@ -162,22 +162,48 @@ struct Radix {
     static constexpr int kDigitWarps = kDigitThreads / 32;
 };
 
-// one pass over the keys counts every digit position: hist[pass][DIG]
+// One pass over the keys counts every digit position: hist[pass][DIG].  A few CTAs
+// per SM each count a long stretch of keys into shared memory (16-byte loads, two in
+// flight per thread), then add their counts to the global histogram once: with one
+// CTA per few thousand keys, the global atomics of the flush (passes x DIG per CTA)
+// cost more than the counting.
+constexpr int kHistThreads = 512;
 template <int RB>
-__global__ void __launch_bounds__(256) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n, int passes,
-                                                         uint32_t* __restrict__ hist) {
+__global__ void __launch_bounds__(kHistThreads) k_radix_histogram(const uint32_t* __restrict__ keys, int64_t n,
+                                                                  int passes, uint32_t* __restrict__ hist) {
     using R = Radix<RB>;
     __shared__ uint32_t s_h[kHistWords];
     for (int i = threadIdx.x; i < passes * R::DIG; i += blockDim.x) s_h[i] = 0;
     __syncthreads();
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
+    auto count = [&](uint32_t k) {
         for (int p = 0; p < passes; ++p) atomicAdd(&s_h[p * R::DIG + ((k >> (RB * p)) & R::MASK)], 1u);
+    };
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    // 16-byte loads where the pointer allows them; the head before the first 16-byte
+    // boundary and the tail after the last whole quad take single loads
+    const int head = (int)((16 - ((uintptr_t)keys & 15)) & 15) / 4;
+    const int64_t h = head < n ? head : n;
+    const uint4* q = reinterpret_cast<const uint4*>(keys + h);
+    const int64_t nq = ((uintptr_t)keys & 3) ? 0 : (n - h) / 4;
+    int64_t i = t0;
+    for (; i + stride < nq; i += 2 * stride) {
+        const uint4 a = __ldg(q + i), b = __ldg(q + i + stride);
+        count(a.x); count(a.y); count(a.z); count(a.w);
+        count(b.x); count(b.y); count(b.z); count(b.w);
     }
+    for (; i < nq; i += stride) {
+        const uint4 a = __ldg(q + i);
+        count(a.x); count(a.y); count(a.z); count(a.w);
+    }
+    const int64_t done = nq > 0 ? h + 4 * nq : 0;
+    if (nq > 0)
+        for (int64_t j = t0; j < h; j += stride) count(keys[j]);
+    for (int64_t j = done + t0; j < n; j += stride) count(keys[j]);
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * R::DIG; i += blockDim.x) {
-        const uint32_t c = s_h[i];
-        if (c) atomicAdd(&hist[i], c);
+    for (int i2 = threadIdx.x; i2 < passes * R::DIG; i2 += blockDim.x) {
+        const uint32_t c = s_h[i2];
+        if (c) atomicAdd(&hist[i2], c);
     }
 }
 
@@ -560,8 +586,12 @@ cudaError_t radix_sort_pairs_u32(const uint32_t* kin, const uint32_t* vin, uint3
     if (e != cudaSuccess) return e;
     const SortLayout L = sort_layout(n, key_bits);
     uint32_t* hist = radix_sort_hist(n, key_bits, scratch);
-    if (L.digit_bits == 10) k_radix_histogram<10><<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
-    else k_radix_histogram<8><<<grid_cap(n, 256), 256, 0, st>>>(kin, n, L.passes, hist);
+    // about 16 keys per thread, at most two CTAs per SM
+    int64_t hb = (n + (int64_t)kHistThreads * 16 - 1) / ((int64_t)kHistThreads * 16);
+    if (hb < 1) hb = 1;
+    if (hb > 148 * 2) hb = 148 * 2;
+    if (L.digit_bits == 10) k_radix_histogram<10><<<(unsigned)hb, kHistThreads, 0, st>>>(kin, n, L.passes, hist);
+    else k_radix_histogram<8><<<(unsigned)hb, kHistThreads, 0, st>>>(kin, n, L.passes, hist);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return radix_sort_finish(kin, vin, kout, vout, n, key_bits, scratch, st, cell_count, ncells);

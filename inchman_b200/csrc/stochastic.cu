@@ -12,9 +12,17 @@ namespace gpgmp {
 
 namespace {
 
-constexpr int kSsaThreads = 128;
 constexpr int kIncMinReactions = 6;   // networks above this size keep per-reaction hazards
-constexpr int TW = 32, TH = 16, NT = 256;
+constexpr int NT = 256;               // threads of a diffusion tile block
+
+// Launch shapes the autotuner chooses from (GridDesc::tile, GridDesc::ssa_threads):
+// diffusion tiles of TW x TH cells for 256 threads (1, 2 or 4 cells per thread in the
+// gather; the one-cell halo is recomputed, so wider tiles recompute less), and SSA
+// blocks of 64, 128 or 256 threads (one cell per thread).  Every draw is keyed by its
+// cell, so all shapes give the same bits.
+constexpr int kTileW[kNumDiffusionTiles] = {32, 32, 64, 16, 64, 32};
+constexpr int kTileH[kNumDiffusionTiles] = {16, 8, 8, 16, 16, 32};
+constexpr int kSsaThreadChoices[kNumSsaThreadChoices] = {128, 64, 256};
 
 __global__ void k_init_poisson(Planes planes, int S, int area, int R, uint32_t seed, const float* __restrict__ lam) {
     const int64_t total = (int64_t)R * area;
@@ -31,7 +39,7 @@ __global__ void k_init_poisson(Planes planes, int S, int area, int R, uint32_t s
 
 // MASKED: localised reactions, rmask as GridDesc::rmask (the unmasked form is the
 // same code with every reaction on)
-template <bool MASKED>
+template <bool MASKED, int kSsaThreads>
 __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int area, int R,
                                                      const gpgmp_reaction* __restrict__ reactions, int nreac,
                                                      uint32_t seed, uint32_t step_seed, float window,
@@ -74,7 +82,7 @@ __global__ void __launch_bounds__(kSsaThreads) k_ssa(Planes planes, int S, int a
 // A block owns a TW x TH tile, samples the lost counts of the tile and of its
 // one-cell halo (recomputed, the streams are keyed by cell) into shared memory,
 // then gathers.  Reads `in`, writes `out`: no block reads what another writes.
-template <int MODE>
+template <int MODE, int TW, int TH>
 __global__ void __launch_bounds__(NT) k_diffuse_tile(const int* __restrict__ in, int* __restrict__ out, int W, int H,
                                                      int S, int species, uint32_t seed, uint32_t step_seed,
                                                      float pmove, int4 bm4, const float* __restrict__ Df,
@@ -497,39 +505,79 @@ cudaError_t launch_init_poisson(const GridDesc& g, Planes planes, uint32_t seed,
     return cudaGetLastError();
 }
 
-cudaError_t launch_ssa(const GridDesc& g, Planes planes, const gpgmp_reaction* d_reactions, int nreac,
-                       uint32_t seed, uint32_t step_seed, float window, int32_t* d_status, cudaStream_t st) {
-    if (nreac <= 0) return cudaSuccess;
+namespace {
+template <bool MASKED, int NTH>
+cudaError_t launch_ssa_t(const GridDesc& g, Planes planes, const gpgmp_reaction* d_reactions, int nreac,
+                         uint32_t seed, uint32_t step_seed, float window, int32_t* d_status, cudaStream_t st) {
     const int area = g.W * g.H;
     const int64_t total = (int64_t)g.R * area;
     const size_t smem = sizeof(gpgmp_reaction) * nreac + sizeof(uint32_t) * 4 * nreac +
-                        sizeof(float) * (size_t)nreac * kSsaThreads + sizeof(int) * g.S * kSsaThreads;
-    const unsigned blocks = (unsigned)((total + kSsaThreads - 1) / kSsaThreads);
-    if (g.rmask) {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_ssa<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        k_ssa<true><<<blocks, kSsaThreads, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed,
-                                                        window, d_status, g.rmask, g.rmask_words);
-    } else {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_ssa<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        k_ssa<false><<<blocks, kSsaThreads, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed,
-                                                         window, d_status, nullptr, 0);
+                        sizeof(float) * (size_t)nreac * NTH + sizeof(int) * g.S * NTH;
+    const unsigned blocks = (unsigned)((total + NTH - 1) / NTH);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_ssa<MASKED, NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
     }
+    k_ssa<MASKED, NTH><<<blocks, NTH, smem, st>>>(planes, g.S, area, g.R, d_reactions, nreac, seed, step_seed, window,
+                                                  d_status, g.rmask, g.rmask_words);
     return cudaGetLastError();
+}
+template <bool MASKED>
+cudaError_t launch_ssa_m(const GridDesc& g, Planes planes, const gpgmp_reaction* d_reactions, int nreac,
+                         uint32_t seed, uint32_t step_seed, float window, int32_t* d_status, cudaStream_t st) {
+    switch (kSsaThreadChoices[g.ssa_threads]) {
+        case 64: return launch_ssa_t<MASKED, 64>(g, planes, d_reactions, nreac, seed, step_seed, window, d_status, st);
+        case 256: return launch_ssa_t<MASKED, 256>(g, planes, d_reactions, nreac, seed, step_seed, window, d_status, st);
+        default: return launch_ssa_t<MASKED, 128>(g, planes, d_reactions, nreac, seed, step_seed, window, d_status, st);
+    }
+}
+
+template <int MODE, int TW, int TH>
+cudaError_t launch_tile_t(const GridDesc& g, const int32_t* in, int32_t* out, int species, uint32_t seed,
+                          uint32_t step_seed, float pmove, const float* d_D, const float* d_r, float dt, float dx,
+                          int fpe, cudaStream_t st) {
+    dim3 grid((g.W + TW - 1) / TW, (g.H + TH - 1) / TH, g.R);
+    const int4 bm = make_int4(g.bmask[0], g.bmask[1], g.bmask[2], g.bmask[3]);
+    k_diffuse_tile<MODE, TW, TH><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, pmove, bm,
+                                                      d_D, d_r, dt, dx, fpe);
+    return cudaGetLastError();
+}
+template <int MODE>
+cudaError_t launch_tile(const GridDesc& g, const int32_t* in, int32_t* out, int species, uint32_t seed,
+                        uint32_t step_seed, float pmove, const float* d_D, const float* d_r, float dt, float dx,
+                        int fpe, cudaStream_t st) {
+#define GPGMP_TILE(I)                                                                                              \
+    case I:                                                                                                        \
+        return launch_tile_t<MODE, kTileW[I], kTileH[I]>(g, in, out, species, seed, step_seed, pmove, d_D, d_r, dt, \
+                                                          dx, fpe, st);
+    switch (g.tile) {
+        GPGMP_TILE(1)
+        GPGMP_TILE(2)
+        GPGMP_TILE(3)
+        GPGMP_TILE(4)
+        GPGMP_TILE(5)
+        default: GPGMP_TILE(0)
+    }
+#undef GPGMP_TILE
+}
+}  // namespace
+
+void diffusion_tile_shape(int index, int* w, int* h) {
+    *w = kTileW[index];
+    *h = kTileH[index];
+}
+int ssa_thread_choice(int index) { return kSsaThreadChoices[index]; }
+
+cudaError_t launch_ssa(const GridDesc& g, Planes planes, const gpgmp_reaction* d_reactions, int nreac,
+                       uint32_t seed, uint32_t step_seed, float window, int32_t* d_status, cudaStream_t st) {
+    if (nreac <= 0) return cudaSuccess;
+    return g.rmask ? launch_ssa_m<true>(g, planes, d_reactions, nreac, seed, step_seed, window, d_status, st)
+                   : launch_ssa_m<false>(g, planes, d_reactions, nreac, seed, step_seed, window, d_status, st);
 }
 
 cudaError_t launch_homog_diffuse(const GridDesc& g, const int32_t* in, int32_t* out, int species, uint32_t seed,
                                  uint32_t step_seed, float pmove, cudaStream_t st) {
-    dim3 grid((g.W + TW - 1) / TW, (g.H + TH - 1) / TH, g.R);
-    int4 bm = make_int4(g.bmask[0], g.bmask[1], g.bmask[2], g.bmask[3]);
-    k_diffuse_tile<0><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, pmove, bm, nullptr,
-                                            nullptr, 0.f, 0.f, 0);
-    return cudaGetLastError();
+    return launch_tile<0>(g, in, out, species, seed, step_seed, pmove, nullptr, nullptr, 0.f, 0.f, 0, st);
 }
 
 cudaError_t launch_source(const GridDesc& g, int32_t* plane_base, int species, uint32_t seed, uint32_t step_seed,
@@ -542,15 +590,8 @@ cudaError_t launch_source(const GridDesc& g, int32_t* plane_base, int species, u
 cudaError_t launch_sweep(const GridDesc& g, const int32_t* in, int32_t* out, int species, int sweep_y,
                          uint32_t seed, uint32_t step_seed, const float* d_D, const float* d_r, float dt, float dx,
                          cudaStream_t st, int fpe) {
-    dim3 grid((g.W + TW - 1) / TW, (g.H + TH - 1) / TH, g.R);
-    int4 bm = make_int4(g.bmask[0], g.bmask[1], g.bmask[2], g.bmask[3]);
-    if (!sweep_y)
-        k_diffuse_tile<1><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, 0.f, bm, d_D, d_r,
-                                                dt, dx, fpe);
-    else
-        k_diffuse_tile<2><<<grid, NT, 0, st>>>(in, out, g.W, g.H, g.S, species, seed, step_seed, 0.f, bm, d_D, d_r,
-                                                dt, dx, fpe);
-    return cudaGetLastError();
+    return sweep_y ? launch_tile<2>(g, in, out, species, seed, step_seed, 0.f, d_D, d_r, dt, dx, fpe, st)
+                   : launch_tile<1>(g, in, out, species, seed, step_seed, 0.f, d_D, d_r, dt, dx, fpe, st);
 }
 
 cudaError_t launch_det_sweep(const GridDesc& g, const float* in, float* out, int species, int sweep_y,

@@ -14,12 +14,25 @@ model's solver type, as oclSolve picks them (DiffusionModel.cpp:1425-1440).
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 from typing import Optional, Sequence
 
 import numpy as np
 
 from . import _lib
 from .model import DiffusionModel
+
+
+TUNE_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_tune")
+
+
+def _device_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name().replace(" ", "_")
+    except Exception:
+        return "gpu"
 
 
 class Solver:
@@ -59,6 +72,52 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+    # -- launch shapes ----------------------------------------------------------
+    @staticmethod
+    def launch_choices():
+        """([(tile_w, tile_h), ...], [ssa_threads, ...]): the shapes the kernels can run."""
+        nt, ns = C.c_int32(), C.c_int32()
+        tw, th, st = (C.c_int32 * 8)(), (C.c_int32 * 8)(), (C.c_int32 * 8)()
+        _lib.call("gpgmp_solver_launch_choices", C.byref(nt), tw, th, C.byref(ns), st)
+        return [(tw[i], th[i]) for i in range(nt.value)], [st[i] for i in range(ns.value)]
+
+    def set_launch(self, tile=(32, 16), ssa_threads: int = 128):
+        _lib.call("gpgmp_solver_set_launch", self._h, int(tile[0]), int(tile[1]), int(ssa_threads))
+
+    def get_launch(self):
+        w, h, t = C.c_int32(), C.c_int32(), C.c_int32()
+        _lib.call("gpgmp_solver_get_launch", self._h, C.byref(w), C.byref(h), C.byref(t))
+        return (w.value, h.value), t.value
+
+    def autotune(self, window: float = 0.0, reps: int = 3, cache: bool = True):
+        """Picks the fastest diffusion tile shape and SSA block size for this solver's
+        model on the current state (gpgmp_solver_autotune) and returns
+        {"tile": (w, h), "ssa_threads": n, "ms_tiles": {...}, "ms_ssa": {...}}.  The choice
+        is cached per GPU and workload signature (grid, realisations, species,
+        reactions, solver type) under inchman_b200/_tune/ and taken from there next
+        time; the results do not depend on it."""
+        tiles, ssas = self.launch_choices()
+        m = self.model
+        key = f"solver_{_device_name()}_{m.solver}_{m.width}x{m.height}_R{self.R}_S{m.num_species}" \
+              f"_N{len(m.reactions)}{'_masked' if m.reaction_mask() is not None else ''}"
+        path = os.path.join(TUNE_DIR, key + ".json")
+        if cache and os.path.exists(path):
+            with open(path) as f:
+                d = json.load(f)
+            self.set_launch(tuple(d["tile"]), d["ssa_threads"])
+            return d
+        mt, ms = (C.c_float * len(tiles))(), (C.c_float * len(ssas))()
+        _lib.call("gpgmp_solver_autotune", self._h, float(window), int(reps), mt, ms)
+        tile, thr = self.get_launch()
+        d = {"tile": list(tile), "ssa_threads": thr,
+             "ms_tiles": {f"{w}x{h}": mt[i] for i, (w, h) in enumerate(tiles)},
+             "ms_ssa": {str(t): ms[i] for i, t in enumerate(ssas)}}
+        if cache:
+            os.makedirs(TUNE_DIR, exist_ok=True)
+            with open(path, "w") as f:
+                json.dump(d, f, indent=1)
+        return d
 
     # -- state --------------------------------------------------------------------
     def set_state(self, state: np.ndarray):

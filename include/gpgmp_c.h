@@ -215,6 +215,25 @@ int gpgmp_synchronize(gpgmp_solver* h);
 void* gpgmp_device_state(gpgmp_solver* h);
 /* computeTimestepX/Y + reduceBlocks + readback -- InhomogeneousSolver.cpp:468-500 */
 int gpgmp_timesteps(gpgmp_solver* h, float* dt_x, float* dt_y);
+/* Launch shapes of the stochastic kernels (the reference fixes its work-group shape,
+ * Globals.h:24-28, Solver.cpp:30-33): the diffusion kernels' tile of tile_w x tile_h
+ * cells (256 threads) and the SSA kernel's block of ssa_threads threads, one cell each.
+ * Every draw is keyed by its cell, so the results do not depend on the shape.
+ *  gpgmp_solver_launch_choices: the shapes there are (arrays of at least 8 entries,
+ *                               any may be NULL);
+ *  gpgmp_solver_set_launch / get_launch: choose one (GPGMP_ERR_INVALID for a shape
+ *                               not among the choices) / read the current one;
+ *  gpgmp_solver_autotune: times every tile shape on species 0's diffusion and every
+ *                               block size on one SSA window of length `window` (<= 0:
+ *                               the smallest diffusion time step) on the current state,
+ *                               reps launches each, and keeps the fastest; the state,
+ *                               clocks and status do not change.  ms_tiles / ms_ssa
+ *                               (may be NULL) receive the mean milliseconds per launch. */
+int gpgmp_solver_launch_choices(int32_t* n_tiles, int32_t* tile_w, int32_t* tile_h, int32_t* n_ssa,
+                                int32_t* ssa_threads);
+int gpgmp_solver_set_launch(gpgmp_solver* h, int32_t tile_w, int32_t tile_h, int32_t ssa_threads);
+int gpgmp_solver_get_launch(gpgmp_solver* h, int32_t* tile_w, int32_t* tile_h, int32_t* ssa_threads);
+int gpgmp_solver_autotune(gpgmp_solver* h, float window, int32_t reps, float* ms_tiles, float* ms_ssa);
 /* Field parameters (Solver.h:59, :85-100): one setField pass (deltat, simtime), and
  * the fields [num_fields][H][W] to and from the host. */
 int gpgmp_update_fields(gpgmp_solver* h, float deltat, float simtime);

@@ -71,6 +71,24 @@ def test_sort_pairs_stable_bit_exact(gpgmp, n, bits):
     assert ind.scratch_status(scratch, 1, n, bits) == 0
 
 
+@pytest.mark.parametrize("offset,n", [(1, 100_003), (2, 5), (3, 4 * 7680 + 3)])
+def test_sort_of_unaligned_views(gpgmp, offset, n):
+    """Keys and values that start 4, 8 or 12 bytes past a 16-byte boundary (views into
+    larger buffers): the histogram's 16-byte loads start after the head, the result is
+    the same stable sort."""
+    from inchman_b200 import individual as ind
+    rng = np.random.default_rng(offset)
+    keys = rng.integers(0, 1 << 20, size=n + offset, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n + offset, dtype=np.uint32)
+    wk, wv = keys[offset:].copy(), vals[offset:].copy()
+    oracle.orc().orc_sort_pairs_u32(oracle.ptr(wk), oracle.ptr(wv), n)
+    tk, tv = _t(keys)[offset:], _t(vals)[offset:]
+    assert tk.data_ptr() % 16 != 0
+    ko, vo, scratch = ind.sort_pairs_u32(tk, tv, 20)
+    assert np.array_equal(_np(ko), wk) and np.array_equal(_np(vo), wv)
+    assert ind.scratch_status(scratch, 1, n, 20) == 0
+
+
 def test_sort_full_32_bit_keys_with_duplicates(gpgmp):
     from inchman_b200 import individual as ind
     rng = np.random.default_rng(11)
