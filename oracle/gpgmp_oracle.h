@@ -93,6 +93,9 @@ void orc_poisson_many(uint32_t k0, uint32_t k1, const float* lam, int32_t* out, 
 float orc_ref_stay_probability(const orc_model* m);
 float orc_ref_cell_width(const orc_model* m);
 void orc_ref_homog_diffuse(const orc_model* m, int32_t* state, int species, int32_t seed, int32_t* lost4);
+/* 1: homogeneous diffusion keyed per cell and species (the reference's defect A.1,
+ * identical uniforms for species diffused in the same event, corrected); 0: literal */
+void orc_ref_set_species_streams(int independent);
 void orc_ref_source_boundary(const orc_model* m, int32_t* state, int species, int32_t seed, int boundary, int source);
 void orc_ref_gillespie(const orc_model* m, int32_t* state, int32_t seed, float deltat);
 void orc_ref_inhomog_diffuse(const orc_model* m, int32_t* state, int species, int32_t seed, float dt, int sweep_y,

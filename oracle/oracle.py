@@ -60,6 +60,7 @@ def orc():
             "orc_ref_rk4": (None, [vp, vp, f32]),
             "orc_ref_solve": (C.c_int, [vp, vp, u32, vp, vp, C.c_int, P(C.c_int), P(i64)]),
             "orc_ref_solve_many": (None, [vp, vp, C.c_int, u32, vp]),
+            "orc_ref_set_species_streams": (None, [C.c_int]),
             "orc_ref_solve_inhom": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, C.c_int, P(C.c_int), P(i64)]),
             "orc_ref_solve_many_snaps": (None, [vp, vp, C.c_int, u32, vp, vp, vp, vp, C.c_int, vp]),
             "orc_rep_init_poisson": (None, [C.c_int, C.c_int, C.c_int, C.c_int, u32, vp, vp]),

@@ -86,6 +86,15 @@ static inline void ref_rng_draw(ref_rng* g) {
 }
 
 /* StochasticHomogeneousDiffusion.cl:8-103 (diffuse) and :105-124 (updateState). */
+/* The reference keys each cell's Threefry stream on the cell alone
+ * (StochasticHomogeneousDiffusion.cl:19-20) and diffuse() does not advance the seed,
+ * so species diffused in the same event draw the same uniforms (its defect A.1).
+ * orc_ref_set_species_streams(1) keys the stream on cell + species * area instead, as
+ * the reference's inhomogeneous sweeps do (StochasticInhomogeneousDriftDiffusion.cl:
+ * 448-452): the restatement with that one defect corrected. */
+static int g_species_streams = 0;
+void orc_ref_set_species_streams(int independent) { g_species_streams = independent; }
+
 void orc_ref_homog_diffuse(const orc_model* m, int32_t* state, int species, int32_t seed, int32_t* lost) {
     const int W = m->width, H = m->height;
     const size_t area = (size_t)W * H;
@@ -98,7 +107,7 @@ void orc_ref_homog_diffuse(const orc_model* m, int32_t* state, int species, int3
         for (int x = 0; x < W; ++x) {
             const int gid = x + y * W;
             ref_rng g = {{0, 0}, {0, 0}, {0, 0}};
-            ref_rng_init(&g, (uint32_t)gid, seed);
+            ref_rng_init(&g, (uint32_t)gid + (g_species_streams ? (uint32_t)(species * area) : 0u), seed);
             int my_state = st[gid];
             size_t mask[4];
             mask[0] = (x == 0) ? (size_t)m->boundary_mask[0] : 1;
