@@ -293,3 +293,37 @@ def autotune(specs: List[InstanceSpec], sample: int = 256, seed: int = 0, cache:
         with open(path, "w") as f:
             json.dump(d, f, indent=1)
     return (thr, cps), d
+
+
+def main(argv=None):
+    """Runs a random heterogeneous ensemble (the batched workload's generator) twice
+    and prints the time and cell-steps/s of each run:
+        python -m inchman_b200.ensemble [--instances N] [--max-time T] [--threads K]"""
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--instances", type=int, default=296)
+    ap.add_argument("--max-time", type=float, default=0.5)
+    ap.add_argument("--threads", type=int, default=1024)
+    ap.add_argument("--ctas-per-sm", type=int, default=1)
+    ap.add_argument("--seed", type=int, default=2024)
+    a = ap.parse_args(argv)
+    ens = Ensemble(random_ensemble(a.instances, seed=a.seed, max_time=a.max_time))
+    ens.configure(a.threads, a.ctas_per_sm)
+    state = ens.alloc_state()
+    for k in range(2):
+        ens.init_poisson(state)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        ens.run(state)
+        t1.record()
+        torch.cuda.synchronize()
+        status, steps, _ = ens.results()
+        ms = t0.elapsed_time(t1)
+        print(f"run {k}: {ms:.1f} ms, {ens.cell_steps(steps) / ms * 1e3:.3e} cell-steps/s, "
+              f"{int((status != 0).sum())} instances with status bits")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
