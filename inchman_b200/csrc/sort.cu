@@ -38,18 +38,25 @@ constexpr int kScanTile = kScanThreads * kScanItems;   // 16384
 // scratch: [0] tile counter, [1] error word, then one status word per tile:
 // (flag << 32) | value, flag 0 = not ready, 1 = tile aggregate, 2 = inclusive prefix.
 // A tile is 512 threads x 32 consecutive values (16384: fewer tiles, a shorter
-// look-back chain).  A full tile whose pointers are 16-byte aligned (vec) moves
-// through shared memory: warp-contiguous 16-byte loads and stores (every HBM request
-// coalesced), one uint4 of padding per eight so that the threads' 128-byte rows read
-// and write without bank conflicts.  The last, partial tile and unaligned pointers
-// take plain loads and stores.
+// look-back chain).  Every tile moves through shared memory, one uint4 of padding per
+// eight so that a thread's 128-byte row reads and writes without bank conflicts: a
+// full tile whose pointers are 16-byte aligned (vec) with warp-contiguous 16-byte loads
+// and stores (every HBM request coalesced), a partial tile or unaligned pointers with
+// coalesced element loads and stores.  A thread sums its row from shared memory, and
+// after the look-back writes its row's exclusive prefixes back in place: the values
+// never sit in registers, so three CTAs fit on an SM (shared memory is the limit)
+// instead of two (registers were), and more loads are in flight while tiles wait in
+// the look-back.
 constexpr int kScanQuads = kScanTile / 4;                 // uint4 per tile
 __device__ __forceinline__ int scan_pad(int i4) { return i4 + (i4 >> 3); }
+// word index of value i of the tile in the padded layout
+__device__ __forceinline__ int scan_word(int i) { return 4 * scan_pad(i >> 2) + (i & 3); }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t* __restrict__ in,
-                                                                 uint32_t* __restrict__ out, int64_t n,
-                                                                 uint64_t* __restrict__ scratch, int vec) {
+__global__ void __launch_bounds__(kScanThreads, 3) k_scan_exclusive(const uint32_t* __restrict__ in,
+                                                                    uint32_t* __restrict__ out, int64_t n,
+                                                                    uint64_t* __restrict__ scratch, int vec) {
     extern __shared__ uint4 s_io[];   // kScanQuads + kScanQuads / 8 (dynamic: 72 KB)
+    uint32_t* s_w32 = reinterpret_cast<uint32_t*>(s_io);
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[kScanThreads / 32];
     __shared__ uint32_t s_prefix;
@@ -61,8 +68,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
     const uint32_t tile = s_tile;
     const int64_t tbase = (int64_t)tile * kScanTile;
     const bool full = vec && tbase + kScanTile <= n;    // the same in every thread of the block
-    const int64_t base = tbase + (int64_t)threadIdx.x * kScanItems;
-    uint32_t v[kScanItems];
     if (full) {
         const uint4* src = reinterpret_cast<const uint4*>(in + tbase);
 #pragma unroll
@@ -70,19 +75,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
             const int i4 = q * kScanThreads + threadIdx.x;
             s_io[scan_pad(i4)] = src[i4];
         }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < kScanItems / 4; ++q) {
-            const uint4 w = s_io[scan_pad(threadIdx.x * (kScanItems / 4) + q)];
-            v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
-        }
     } else {
-#pragma unroll
-        for (int q = 0; q < kScanItems; ++q) v[q] = base + q < n ? in[base + q] : 0u;
+        for (int q = 0; q < kScanItems; ++q) {
+            const int i = q * kScanThreads + threadIdx.x;
+            s_w32[scan_word(i)] = tbase + i < n ? in[tbase + i] : 0u;
+        }
     }
+    __syncthreads();
+    // the thread's row: values threadIdx.x * 32 .. + 31 of the tile
+    const int row = threadIdx.x * (kScanItems / 4);
     uint32_t sum = 0;
 #pragma unroll
-    for (int q = 0; q < kScanItems; ++q) sum += v[q];
+    for (int q = 0; q < kScanItems / 4; ++q) {
+        const uint4 w = s_io[scan_pad(row + q)];
+        sum += w.x + w.y + w.z + w.w;
+    }
     // block exclusive scan of the thread sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t incl = sum;
@@ -112,19 +119,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
         if (lane == 0) s_prefix = exclusive;
     }
     __syncthreads();
+    // the row's exclusive prefixes, in place
     uint32_t run = s_prefix + thread_excl;
-    if (full) {
-        // every thread read its inputs from s_io before the barriers above
 #pragma unroll
-        for (int q = 0; q < kScanItems / 4; ++q) {
-            uint4 w;
-            w.x = run; run += v[4 * q];
-            w.y = run; run += v[4 * q + 1];
-            w.z = run; run += v[4 * q + 2];
-            w.w = run; run += v[4 * q + 3];
-            s_io[scan_pad(threadIdx.x * (kScanItems / 4) + q)] = w;
-        }
-        __syncthreads();
+    for (int q = 0; q < kScanItems / 4; ++q) {
+        const uint4 v = s_io[scan_pad(row + q)];
+        uint4 w;
+        w.x = run; run += v.x;
+        w.y = run; run += v.y;
+        w.z = run; run += v.z;
+        w.w = run; run += v.w;
+        s_io[scan_pad(row + q)] = w;
+    }
+    __syncthreads();
+    if (full) {
         uint4* dst = reinterpret_cast<uint4*>(out + tbase);
 #pragma unroll
         for (int q = 0; q < kScanItems / 4; ++q) {
@@ -132,10 +140,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(const uint32_t*
             dst[i4] = s_io[scan_pad(i4)];
         }
     } else {
-#pragma unroll
         for (int q = 0; q < kScanItems; ++q) {
-            if (base + q < n) out[base + q] = run;
-            run += v[q];
+            const int i = q * kScanThreads + threadIdx.x;
+            if (tbase + i < n) out[tbase + i] = s_w32[scan_word(i)];
         }
     }
 }
