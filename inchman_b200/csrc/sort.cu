@@ -11,10 +11,12 @@
 //  - exclusive scan: single pass with decoupled look-back (Merrill & Garland 2016);
 //  - radix sort: onesweep (Adinets & Merrill 2022): one histogram kernel for every
 //    digit position, then one kernel per digit (8 bits, or 10 where that saves a
-//    pass: 17-20 and 25-30 key bits) that ranks its tile (peer masks from ballots),
-//    publishes per-digit tile counts, looks back for the prefix, scans the pass's
-//    digit counts into the digits' global starts itself and scatters through shared
-//    memory; stable;
+//    pass: 17-20 and 25-30 key bits) that ranks its tile (peer masks from shared-memory
+//    atomicOr on the digit's low 8 bits, ballots for the rest),
+//    publishes per-digit tile counts, looks back for the prefix and scatters through
+//    shared memory; tile 0 scans the pass's digit counts into the digits' global
+//    starts and publishes them inside its inclusive prefix, so no other tile (and no
+//    separate launch) turns counts into offsets; stable;
 //  - cell offsets: key histogram + exclusive scan (start), count; the reference's
 //    left/right indices follow from them.
 // Every look-back spin has an iteration limit; exceeding it sets the error word
@@ -152,7 +154,13 @@ constexpr int kSortThreads = 512;
 constexpr int kSortItems = 15;
 constexpr int kSortTile = kSortThreads * kSortItems;   // 7680: fewer tiles, a shorter look-back chain
 static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "a thread per digit (8-bit digits)");
-constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
+// Keys and values of a tile in sorted order; 8-bit passes add a third region into which
+// the values are copied asynchronously while the tile ranks (the 10-bit passes' digit
+// arrays leave no room for it at two CTAs per SM, so their values are read at staging).
+template <int RB>
+constexpr bool kValuePrefetch = RB == 8;
+template <int RB>
+constexpr int kSortStagingBytes = (kValuePrefetch<RB> ? 3 : 2) * kSortTile * (int)sizeof(uint32_t);
 constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
 constexpr int kLookWindow = 4;   // predecessor tiles read per look-back step
@@ -228,63 +236,142 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     using R = Radix<RB>;
     constexpr int DIG = R::DIG;
     constexpr int DPT = R::kDPT;
-    // per warp and digit: the warp's count, then its offset among the tile's warps
-    // (at most 7680, so 16 bits)
+    // per warp and digit: the warp's count, then the tile-local position of the warp's
+    // first key of that digit (at most 7680, so 16 bits)
     __shared__ uint16_t s_warp_hist[kWarps][DIG];
     __shared__ uint32_t s_count[DIG];        // the tile's count of each digit
-    __shared__ uint32_t s_tile_off[DIG];     // exclusive offset of each digit inside the tile
-    __shared__ uint32_t s_global[DIG];       // global start of each digit's run of this tile
+    __shared__ uint32_t s_delta[DIG];        // global start minus tile-local start of each digit
     __shared__ uint32_t s_w[R::kDigitWarps];
     __shared__ uint32_t s_hw[R::kDigitWarps];
-    extern __shared__ uint32_t s_staging[];  // keys then values in tile-sorted order (dynamic: 60 KB)
+    extern __shared__ uint32_t s_staging[];  // keys, values in tile-sorted order [, values as loaded]
     uint32_t* s_keys = s_staging;
     uint32_t* s_vals = s_staging + kSortTile;
+    uint32_t* s_vraw = s_staging + 2 * kSortTile;   // only with kValuePrefetch<RB>
     __shared__ uint32_t s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int i = threadIdx.x; i < kWarps * DIG / 2; i += kSortThreads)
         reinterpret_cast<uint32_t*>(&s_warp_hist[0][0])[i] = 0;
     for (int i = threadIdx.x; i < DIG; i += kSortThreads) s_count[i] = 0;
+    // ranking: per warp and value of a digit's low 8 bits, the lanes holding it (in the
+    // keys' staging area, which is free until the staging step)
+    static_assert(kWarps * 256 <= kSortTile, "match words fit in the keys' staging area");
+    uint32_t* s_match = s_staging;
+    for (int i = threadIdx.x; i < kWarps * 256; i += kSortThreads) s_match[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const int64_t tbase = (int64_t)tile * kSortTile;
     const int64_t wbase = tbase + (int64_t)warp * 32 * kSortItems;
-    // values stay in memory until the staging step (fewer registers, more warps per SM)
+    // item j of this lane is in range iff j * 32 < rem
+    const int64_t rem64 = n - (wbase + lane);
+    const int rem = rem64 < kSortTile ? (int)rem64 : kSortTile;
+    // values are not held in registers (fewer registers, more warps per SM): 8-bit passes
+    // copy them into shared memory with cp.async while the tile ranks, 10-bit passes read
+    // them at the staging step
     uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t idx = wbase + j * 32 + lane;
-        key[j] = idx < n ? kin[idx] : 0xffffffffu;
+        const bool ok = j * 32 < rem;
+        key[j] = ok ? kin[idx] : 0xffffffffu;
+        if constexpr (kValuePrefetch<RB>) {
+            if (ok) {
+                const uint32_t dst =
+                    (uint32_t)__cvta_generic_to_shared(s_vraw + warp * 32 * kSortItems + j * 32 + lane);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(vin + idx) : "memory");
+            }
+        }
     }
+    if constexpr (kValuePrefetch<RB>) asm volatile("cp.async.commit_group;\n" ::: "memory");
     // the tile's digit counts first (order-free shared-memory atomics), published
     // before the ranking so that the look-back of later tiles can start early
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j)
-        if (wbase + j * 32 + lane < n) atomicAdd(&s_count[(key[j] >> shift) & R::MASK], 1u);
+        if (j * 32 < rem) atomicAdd(&s_count[(key[j] >> shift) & R::MASK], 1u);
     __syncthreads();
     // digit thread t owns digits t*DPT .. t*DPT + DPT - 1
     const bool digit_thread = threadIdx.x < R::kDigitThreads;
     const int d0 = threadIdx.x * DPT;
     uint32_t tile_count[DPT];
     uint32_t* lk = look + (size_t)tile * DIG;
+    // exclusive scan of the tile's counts over the digits (tile-local starts): the digit
+    // warps' totals here, the scan itself after the ranking (the counts are re-read from
+    // shared memory then, so nothing of this stays live across the ranking)
+    const auto warp_scan = [&](uint32_t& mine) {
+        mine = 0;
 #pragma unroll
-    for (int q = 0; q < DPT; ++q) {
-        tile_count[q] = digit_thread ? s_count[d0 + q] : 0u;
-        if (digit_thread) st_relaxed_u32(&lk[d0 + q], (tile == 0 ? kFlagP : kFlagA) | tile_count[q]);
+        for (int q = 0; q < DPT; ++q) {
+            tile_count[q] = digit_thread ? s_count[d0 + q] : 0u;
+            mine += tile_count[q];
+        }
+        uint32_t incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        return incl;
+    };
+    if (digit_thread) {
+        uint32_t mine;
+        const uint32_t incl = warp_scan(mine);
+        if (lane == 31) s_w[warp] = incl;
+#pragma unroll
+        for (int q = 0; q < DPT; ++q)
+            if (tile > 0) st_relaxed_u32(&lk[d0 + q], kFlagA | tile_count[q]);
     }
-    // warp-level ranking (stable): the lanes holding the same digit, from RB ballots
+    // tile 0 alone scans the pass's digit counts into the digits' global starts and
+    // publishes start + its own count as its inclusive prefix, so every later tile's
+    // look-back sum already holds its digit's global start
+    if (tile == 0) {
+        uint32_t hc[DPT], hmine = 0;
+#pragma unroll
+        for (int q = 0; q < DPT; ++q) {
+            hc[q] = digit_thread ? bins[d0 + q] : 0u;
+            hmine += hc[q];
+        }
+        uint32_t hincl = hmine;
+        if (digit_thread) {
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, hincl, o);
+                if (lane >= o) hincl += t;
+            }
+            if (lane == 31) s_hw[warp] = hincl;
+        }
+        __syncthreads();
+        if (digit_thread) {
+            uint32_t hoff = hincl - hmine;
+            for (int w = 0; w < warp; ++w) hoff += s_hw[w];
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                st_relaxed_u32(&lk[d0 + q], kFlagP | ((hoff + tile_count[q]) & kValMask));
+                s_delta[d0 + q] = hoff;   // this tile's exclusive prefix
+                hoff += hc[q];
+            }
+        }
+    }
+    // warp-level ranking (stable): the lanes holding the same digit, as the lanes that
+    // set their bit in the word of the digit's low 8 bits (shared-memory atomicOr) and,
+    // for 10-bit digits, agree on the top bits by ballot
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const int64_t idx = wbase + j * 32 + lane;
-        const bool ok = idx < n;
+        const bool ok = j * 32 < rem;
         const uint32_t dj = (key[j] >> shift) & R::MASK;
-        unsigned peers = __ballot_sync(0xffffffffu, ok);
+        uint32_t* m = s_match + warp * 256 + (dj & 255u);
+        if (ok) atomicOr(m, 1u << lane);
+        __syncwarp();
+        const unsigned low = ok ? *m : 0u;
+        __syncwarp();
+        unsigned peers = low;
 #pragma unroll
-        for (int b = 0; b < RB; ++b) {
+        for (int b = 8; b < RB; ++b) {
             const unsigned bal = __ballot_sync(0xffffffffu, (dj >> b) & 1u);
             peers &= ((dj >> b) & 1u) ? bal : ~bal;
         }
+        // the lowest lane holding a low-8-bit value clears its word for the next item
+        if (ok && lane == __ffs(low) - 1) *m = 0u;
         // the lowest lane of each group adds the group to the warp's digit count; the
         // count before it comes back to the whole group by one full-warp shuffle
         const int leader = peers ? __ffs(peers) - 1 : lane;
@@ -298,25 +385,31 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
         __syncwarp();
     }
     __syncthreads();
-    // per digit: counts over warps -> warp offsets (in place)
+    // per digit: tile-local start, then the start of each warp's keys of that digit (in
+    // place of the warp's count)
+    uint32_t toff[DPT], excl[DPT];
     if (digit_thread) {
+        uint32_t mine;
+        uint32_t o = warp_scan(mine) - mine;
+        for (int w = 0; w < warp; ++w) o += s_w[w];
 #pragma unroll
         for (int q = 0; q < DPT; ++q) {
-            uint32_t run = 0;
+            toff[q] = o;
+            uint32_t run = o;
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) {
                 const uint32_t c = s_warp_hist[w][d0 + q];
                 s_warp_hist[w][d0 + q] = (uint16_t)run;
                 run += c;
             }
+            o += tile_count[q];
         }
     }
     // look back for the prefix of each owned digit: kLookWindow tiles at a time (the
     // loads of all owned digits in flight together), summing the counts up to and
-    // including the nearest inclusive prefix
-    uint32_t excl[DPT];
+    // including the nearest inclusive prefix (tile 0's holds the digit's global start)
 #pragma unroll
-    for (int q = 0; q < DPT; ++q) excl[q] = 0;
+    for (int q = 0; q < DPT; ++q) excl[q] = (digit_thread && tile == 0) ? s_delta[d0 + q] : 0u;
     if (digit_thread && tile > 0) {
         bool done[DPT];
 #pragma unroll
@@ -361,59 +454,24 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
 #pragma unroll
         for (int q = 0; q < DPT; ++q) st_relaxed_u32(&lk[d0 + q], kFlagP | ((excl[q] + tile_count[q]) & kValMask));
     }
-    // tile-local digit offsets (exclusive scan of the tile counts over the digits) and
-    // the digits' global starts (exclusive scan of the pass's digit counts in bins; every
-    // tile scans them itself, so no separate launch turns counts into offsets)
-    {
-        uint32_t mine = 0, hmine = 0, hc[DPT];
+    if (digit_thread) {
 #pragma unroll
-        for (int q = 0; q < DPT; ++q) {
-            hc[q] = digit_thread ? bins[d0 + q] : 0u;
-            mine += tile_count[q];
-            hmine += hc[q];
-        }
-        uint32_t incl = mine, hincl = hmine;
-        if (digit_thread) {
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                const uint32_t ht = __shfl_up_sync(0xffffffffu, hincl, o);
-                if (lane >= o) {
-                    incl += t;
-                    hincl += ht;
-                }
-            }
-            if (lane == 31) {
-                s_w[warp] = incl;
-                s_hw[warp] = hincl;
-            }
-        }
-        __syncthreads();
-        if (digit_thread) {
-            uint32_t off = incl - mine, hoff = hincl - hmine;
-            for (int w = 0; w < warp; ++w) {
-                off += s_w[w];
-                hoff += s_hw[w];
-            }
-#pragma unroll
-            for (int q = 0; q < DPT; ++q) {
-                s_tile_off[d0 + q] = off;
-                s_global[d0 + q] = hoff + excl[q];
-                off += tile_count[q];
-                hoff += hc[q];
-            }
-        }
+        for (int q = 0; q < DPT; ++q) s_delta[d0 + q] = excl[q] - toff[q];
     }
+    // each thread reads back only the values it copied itself, so its own wait suffices
+    if constexpr (kValuePrefetch<RB>) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     // stage keys and values in tile-sorted order
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const int64_t idx = wbase + j * 32 + lane;
-        if (idx < n) {
+        if (j * 32 < rem) {
             const uint32_t dd = (key[j] >> shift) & R::MASK;
-            const uint32_t lp = s_tile_off[dd] + s_warp_hist[warp][dd] + rank[j];
+            const uint32_t lp = s_warp_hist[warp][dd] + rank[j];
             s_keys[lp] = key[j];
-            s_vals[lp] = vin[idx];
+            if constexpr (kValuePrefetch<RB>)
+                s_vals[lp] = s_vraw[warp * 32 * kSortItems + j * 32 + lane];
+            else
+                s_vals[lp] = vin[wbase + j * 32 + lane];
         }
     }
     __syncthreads();
@@ -421,8 +479,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     if (!cell_count) {
         for (int i = threadIdx.x; i < valid; i += kSortThreads) {
             const uint32_t k = s_keys[i];
-            const uint32_t dd = (k >> shift) & R::MASK;
-            const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
+            const uint32_t g = s_delta[(k >> shift) & R::MASK] + (uint32_t)i;
             kout[g] = k;
             vout[g] = s_vals[i];
         }
@@ -436,8 +493,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
         const bool ok = i < valid;
         const uint32_t k = ok ? s_keys[i] : 0xffffffffu;
         if (ok) {
-            const uint32_t dd = (k >> shift) & R::MASK;
-            const uint32_t g = s_global[dd] + (uint32_t)i - s_tile_off[dd];
+            const uint32_t g = s_delta[(k >> shift) & R::MASK] + (uint32_t)i;
             kout[g] = k;
             vout[g] = s_vals[i];
         }
@@ -538,9 +594,9 @@ cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_
     const SortLayout L = sort_layout(n, key_bits);
     cudaError_t e = L.digit_bits == 10
                         ? cudaFuncSetAttribute(k_onesweep<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes)
+                                               kSortStagingBytes<10>)
                         : cudaFuncSetAttribute(k_onesweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes);
+                                               kSortStagingBytes<8>);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(scratch, 0,
                            L.off_look + sizeof(uint32_t) * ((size_t)1 << L.digit_bits) * (size_t)L.tiles * L.passes, st);
@@ -571,11 +627,11 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
         uint32_t* lp = look + (size_t)dig * L.tiles * p;
         uint32_t* cc = p == L.passes - 1 ? cell_count : nullptr;
         if (rb == 10)
-            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes<10>, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         else
-            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes<8>, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         cudaError_t e = cudaGetLastError();
