@@ -154,13 +154,13 @@ constexpr int kSortThreads = 512;
 constexpr int kSortItems = 15;
 constexpr int kSortTile = kSortThreads * kSortItems;   // 7680: fewer tiles, a shorter look-back chain
 static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "a thread per digit (8-bit digits)");
-// Keys and values of a tile in sorted order; 8-bit passes add a third region into which
-// the values are copied asynchronously while the tile ranks (the 10-bit passes' digit
-// arrays leave no room for it at two CTAs per SM, so their values are read at staging).
+// Keys and values of a tile in sorted order (dynamic shared memory, 60 KB).  8-bit passes
+// copy the values asynchronously into the values' area while the tile ranks and stage
+// them in two steps (through registers); 10-bit passes read them at the staging step,
+// which measured faster for them than the extra barrier of the two-step form.
 template <int RB>
 constexpr bool kValuePrefetch = RB == 8;
-template <int RB>
-constexpr int kSortStagingBytes = (kValuePrefetch<RB> ? 3 : 2) * kSortTile * (int)sizeof(uint32_t);
+constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
 constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
 constexpr int kLookWindow = 4;   // predecessor tiles read per look-back step
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     extern __shared__ uint32_t s_staging[];  // keys, values in tile-sorted order [, values as loaded]
     uint32_t* s_keys = s_staging;
     uint32_t* s_vals = s_staging + kSortTile;
-    uint32_t* s_vraw = s_staging + 2 * kSortTile;   // only with kValuePrefetch<RB>
+    uint32_t* s_vraw = s_vals;   // values as loaded, until the staging step
     __shared__ uint32_t s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -266,8 +266,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     const int64_t rem64 = n - (wbase + lane);
     const int rem = rem64 < kSortTile ? (int)rem64 : kSortTile;
     // values are not held in registers (fewer registers, more warps per SM): 8-bit passes
-    // copy them into shared memory with cp.async while the tile ranks, 10-bit passes read
-    // them at the staging step
+    // copy them into the values' area with cp.async while the tile ranks, 10-bit passes
+    // read them at the staging step
     uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
@@ -461,17 +461,34 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
     // each thread reads back only the values it copied itself, so its own wait suffices
     if constexpr (kValuePrefetch<RB>) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    // stage keys and values in tile-sorted order
+    if constexpr (kValuePrefetch<RB>) {
+        // stage keys in tile-sorted order, taking each thread's values out of the values'
+        // area (into the keys' registers) and their positions (into the ranks' registers)
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        if (j * 32 < rem) {
-            const uint32_t dd = (key[j] >> shift) & R::MASK;
-            const uint32_t lp = s_warp_hist[warp][dd] + rank[j];
-            s_keys[lp] = key[j];
-            if constexpr (kValuePrefetch<RB>)
-                s_vals[lp] = s_vraw[warp * 32 * kSortItems + j * 32 + lane];
-            else
+        for (int j = 0; j < kSortItems; ++j) {
+            if (j * 32 < rem) {
+                const uint32_t dd = (key[j] >> shift) & R::MASK;
+                const uint32_t lp = s_warp_hist[warp][dd] + rank[j];
+                s_keys[lp] = key[j];
+                rank[j] = lp;
+                key[j] = s_vraw[warp * 32 * kSortItems + j * 32 + lane];
+            }
+        }
+        __syncthreads();
+        // then the values
+#pragma unroll
+        for (int j = 0; j < kSortItems; ++j)
+            if (j * 32 < rem) s_vals[rank[j]] = key[j];
+    } else {
+        // stage keys and values in tile-sorted order
+#pragma unroll
+        for (int j = 0; j < kSortItems; ++j) {
+            if (j * 32 < rem) {
+                const uint32_t dd = (key[j] >> shift) & R::MASK;
+                const uint32_t lp = s_warp_hist[warp][dd] + rank[j];
+                s_keys[lp] = key[j];
                 s_vals[lp] = vin[wbase + j * 32 + lane];
+            }
         }
     }
     __syncthreads();
@@ -594,9 +611,9 @@ cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_
     const SortLayout L = sort_layout(n, key_bits);
     cudaError_t e = L.digit_bits == 10
                         ? cudaFuncSetAttribute(k_onesweep<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes<10>)
+                                               kSortStagingBytes)
                         : cudaFuncSetAttribute(k_onesweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes<8>);
+                                               kSortStagingBytes);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(scratch, 0,
                            L.off_look + sizeof(uint32_t) * ((size_t)1 << L.digit_bits) * (size_t)L.tiles * L.passes, st);
@@ -627,11 +644,11 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
         uint32_t* lp = look + (size_t)dig * L.tiles * p;
         uint32_t* cc = p == L.passes - 1 ? cell_count : nullptr;
         if (rb == 10)
-            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes<10>, st>>>(
+            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         else
-            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes<8>, st>>>(
+            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         cudaError_t e = cudaGetLastError();
