@@ -21,6 +21,7 @@
 //    left/right indices follow from them.
 // Every look-back spin has an iteration limit; exceeding it sets the error word
 // (GPGMP_ERR_TIMEOUT for the caller) and the kernel continues without waiting.
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include <cuda_runtime.h>
@@ -150,29 +151,37 @@ __global__ void __launch_bounds__(kScanThreads, 3) k_scan_exclusive(const uint32
 }
 
 // ---- radix sort ------------------------------------------------------------------
-constexpr int kSortThreads = 512;
+// A tile is kThreads threads x kSortItems keys.  8-bit passes run 256-thread tiles, four
+// CTAs per SM (one CTA's barriers overlap the others' work); 10-bit passes 512-thread
+// tiles, two per SM (with 256 threads each would own four digits and spill registers).
 constexpr int kSortItems = 15;
-constexpr int kSortTile = kSortThreads * kSortItems;   // 7680: fewer tiles, a shorter look-back chain
-static_assert(kSortThreads >= 256 && kSortThreads % 32 == 0, "a thread per digit (8-bit digits)");
-// Keys and values of a tile in sorted order (dynamic shared memory, 60 KB).  8-bit passes
-// copy the values asynchronously into the values' area while the tile ranks and stage
-// them in two steps (through registers); 10-bit passes read them at the staging step,
-// which measured faster for them than the extra barrier of the two-step form.
+template <int RB>
+struct SortShape {
+    static constexpr int kThreads = RB == 8 ? 256 : 512;
+    static constexpr int kMinBlocks = RB == 8 ? 4 : 2;
+    static constexpr int kTile = kThreads * kSortItems;   // 3840 / 7680 keys
+    static constexpr int kWarps = kThreads / 32;
+    // keys and values of a tile in sorted order (dynamic shared memory: 30 / 60 KB)
+    static constexpr int kStagingBytes = 2 * kTile * (int)sizeof(uint32_t);
+    static_assert(kThreads >= 256 && kThreads % 32 == 0, "a thread per digit (8-bit digits)");
+};
+// 8-bit passes copy the values asynchronously into the values' staging area while the
+// tile ranks and stage them in two steps (through registers); 10-bit passes read them at
+// the staging step, which measured faster for them than the extra barrier of the
+// two-step form.
 template <int RB>
 constexpr bool kValuePrefetch = RB == 8;
-constexpr int kSortStagingBytes = 2 * kSortTile * (int)sizeof(uint32_t);
-constexpr int kWarps = kSortThreads / 32;
 constexpr uint32_t kFlagA = 1u << 30, kFlagP = 2u << 30, kValMask = (1u << 30) - 1;
 constexpr int kLookWindow = 4;   // predecessor tiles read per look-back step
 constexpr int kHistWords = 3 * 1024;   // digit counts of every pass: 4 x 256 or up to 3 x 1024
 
 // Digits of RB bits: DIG values, owned kDPT at a time by the first kDigitThreads threads
-// in the digit phases (8 bits: threads 0-255, one each; 10 bits: all 512, two each).
+// in the digit phases (8 bits: all 256 threads, one each; 10 bits: all 512, two each).
 template <int RB>
 struct Radix {
     static constexpr int DIG = 1 << RB;
     static constexpr uint32_t MASK = (uint32_t)DIG - 1u;
-    static constexpr int kDigitThreads = DIG < kSortThreads ? DIG : kSortThreads;
+    static constexpr int kDigitThreads = DIG < SortShape<RB>::kThreads ? DIG : SortShape<RB>::kThreads;
     static constexpr int kDPT = DIG / kDigitThreads;
     static constexpr int kDigitWarps = kDigitThreads / 32;
 };
@@ -226,7 +235,7 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_histogram(const uint32_t
 // in a warp-striped layout (item j of lane l is key j*32 + l), so processing items in
 // order and lanes in order is index order: the ranks are stable.
 template <int RB>
-__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __restrict__ kin,
+__global__ void __launch_bounds__(SortShape<RB>::kThreads, SortShape<RB>::kMinBlocks) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin,
                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            int64_t n, int shift, const uint32_t* __restrict__ bins,
@@ -234,6 +243,9 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const uint32_t* __
                                                            int* err, uint32_t* __restrict__ cell_count,
                                                            uint32_t ncells) {
     using R = Radix<RB>;
+    constexpr int kSortThreads = SortShape<RB>::kThreads;
+    constexpr int kSortTile = SortShape<RB>::kTile;
+    constexpr int kWarps = SortShape<RB>::kWarps;
     constexpr int DIG = R::DIG;
     constexpr int DPT = R::kDPT;
     // per warp and digit: the warp's count, then the tile-local position of the warp's
@@ -593,13 +605,17 @@ SortLayout sort_layout(int64_t n, int key_bits) {
     // 10-bit digits where they save a pass (17-20 and 25-30 key bits)
     L.digit_bits = (key_bits > 16 && key_bits <= 30 && p10 < p8) ? 10 : 8;
     L.passes = L.digit_bits == 10 ? p10 : p8;
-    L.tiles = (n + kSortTile - 1) / kSortTile;
+    const int tile = L.digit_bits == 10 ? SortShape<10>::kTile : SortShape<8>::kTile;
+    L.tiles = (n + tile - 1) / tile;
     size_t off = 0;
     L.off_hist = off;    off += align256(sizeof(uint32_t) * kHistWords);
     L.off_counters = off; off += align256(sizeof(uint32_t) * 8);     // tile counters [4], error word [4]
-    // look-back words for the widest layout (3 passes x 1024 digits >= 4 x 256), so that
-    // the scratch size does not depend on key_bits
-    L.off_look = off;    off += align256(sizeof(uint32_t) * kHistWords * (size_t)(L.tiles > 0 ? L.tiles : 1));
+    // look-back words for the widest layout (4 passes x 256 digits x 3840-key tiles, or
+    // 3 x 1024 x 7680-key tiles), so that the scratch size does not depend on key_bits
+    const int64_t t8 = (n + SortShape<8>::kTile - 1) / SortShape<8>::kTile;
+    const int64_t t10 = (n + SortShape<10>::kTile - 1) / SortShape<10>::kTile;
+    const int64_t look_words = std::max<int64_t>(std::max<int64_t>(4 * 256 * t8, 3 * 1024 * t10), 3 * 1024);
+    L.off_look = off;    off += align256(sizeof(uint32_t) * (size_t)look_words);
     L.off_alt_keys = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.off_alt_vals = off; off += align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
     L.bytes = off;
@@ -611,9 +627,9 @@ cudaError_t radix_sort_begin(int64_t n, int key_bits, void* scratch, cudaStream_
     const SortLayout L = sort_layout(n, key_bits);
     cudaError_t e = L.digit_bits == 10
                         ? cudaFuncSetAttribute(k_onesweep<10>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes)
+                                               SortShape<10>::kStagingBytes)
                         : cudaFuncSetAttribute(k_onesweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSortStagingBytes);
+                                               SortShape<8>::kStagingBytes);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(scratch, 0,
                            L.off_look + sizeof(uint32_t) * ((size_t)1 << L.digit_bits) * (size_t)L.tiles * L.passes, st);
@@ -644,11 +660,11 @@ cudaError_t radix_sort_finish(const uint32_t* kin, const uint32_t* vin, uint32_t
         uint32_t* lp = look + (size_t)dig * L.tiles * p;
         uint32_t* cc = p == L.passes - 1 ? cell_count : nullptr;
         if (rb == 10)
-            k_onesweep<10><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+            k_onesweep<10><<<(unsigned)L.tiles, SortShape<10>::kThreads, SortShape<10>::kStagingBytes, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         else
-            k_onesweep<8><<<(unsigned)L.tiles, kSortThreads, kSortStagingBytes, st>>>(
+            k_onesweep<8><<<(unsigned)L.tiles, SortShape<8>::kThreads, SortShape<8>::kStagingBytes, st>>>(
                 sk, sv, dk, dv, n, rb * p, hist + dig * p, lp, counters + p, (int*)(counters + 4), cc,
                 (uint32_t)ncells);
         cudaError_t e = cudaGetLastError();

@@ -35,7 +35,7 @@ def test_sort_scratch_size_does_not_depend_on_key_bits(gpgmp):
     alike), so a caller may size it once for n."""
     from inchman_b200 import _lib
     L = _lib.lib()
-    for n in (1, 7680, 7681, 1 << 22):
+    for n in (1, 3840, 3841, 7680, 7681, 1 << 22):
         sizes = set()
         for bits in range(1, 33):
             b = C.c_size_t(0)

@@ -55,7 +55,8 @@ def test_exclusive_scan_of_an_unaligned_view(gpgmp, offset):
 
 @pytest.mark.parametrize("n,bits", [(1, 32), (3839, 8), (3841, 20), (65536, 32), (1_000_003, 21), (1 << 22, 20),
                                     (7681, 10), (200_000, 16), (200_001, 17), (777_777, 26), (123_457, 30),
-                                    (1 << 20, 24), (7680, 20), (2 * 7680 + 1, 20), (7680, 8)])
+                                    (1 << 20, 24), (7680, 20), (2 * 7680 + 1, 20), (7680, 8), (3840, 8),
+                                    (3841, 32), (2 * 3840 - 1, 16)])
 def test_sort_pairs_stable_bit_exact(gpgmp, n, bits):
     from inchman_b200 import individual as ind
     rng = np.random.default_rng(bits + n)
