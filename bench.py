@@ -208,6 +208,7 @@ def bench_gray_scott(args, rank, world):
     u0 = torch.tensor(u0h, device=dev)
     v0 = torch.tensor(v0h, device=dev)
     p = cfg.params()
+    kernel = forward_kernel(n)    # what the automatic choice (variant 0) runs here
     l2 = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -369,10 +370,10 @@ def bench_gray_scott(args, rank, world):
                 "d2h_bytes_per_step": 2 * n * n * 4},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
-                     "note": "16 B/cell-step algorithmic; the lattice stays in the registers of one 16-CTA cluster "
-                             "(16 of 148 SMs), so DRAM traffic is the initial read and final write only",
-                     "sm_bound": sm_bound(t_launch, steps, n, clocks.get("sm_mhz"))},
-        "gpu_launches": args.steps,   # one k_gs_forward_rr launch per timed solve
+                     "note": kernel_note(kernel),
+                     "sm_bound": sm_bound(t_launch, steps, n, clocks.get("sm_mhz"), kernel)},
+        "kernel": kernel,
+        "gpu_launches": args.steps,   # one forward-kernel launch per timed solve
         "clocks": clocks,
     }
     if rank == 0 and world == 1:
@@ -386,15 +387,48 @@ def bench_gray_scott(args, rank, world):
     return line
 
 
-def sm_bound(t_solve, steps, n, clock_mhz, sms=16, ops_per_cell=18):
-    """The compute bound of the forward solve on the SMs it occupies: one 16-CTA
-    cluster, 18 FP32 lane operations per cell-step (an FMA counts once), 128 FP32
-    lanes per SM at the median SM clock sampled during the timed solves."""
+def forward_kernel(n):
+    """The float32 forward kernel that the automatic choice runs for an n x n lattice
+    on this GPU: its variant, 16-CTA clusters, SMs and rows computed per step (band
+    plus ghost rows for the multi-cluster kernel)."""
+    from inchman_b200 import gray_scott as gs
+    v = gs.auto_variant(n)
+    if v in gs.MULTI_CLUSTER:
+        c, g = gs.MULTI_CLUSTER[v]
+        return {"variant": v, "name": f"k_gs_forward_mc<{n},{c},{g},{(n // c + 2 * g) // 16}>", "clusters": c,
+                "ghost_rows": g, "sms": 16 * c, "rows_per_step": n + 2 * g * c}
+    if v > 10:
+        return {"variant": v, "name": f"k_gs_forward_rr<{n},{v - 10}>", "clusters": 1, "ghost_rows": 0, "sms": 16,
+                "rows_per_step": n}
+    return {"variant": v, "name": "shared-memory column walk", "clusters": 1, "ghost_rows": 0, "sms": 16,
+            "rows_per_step": n}
+
+
+def kernel_note(kernel):
+    c, g = kernel["clusters"], kernel["ghost_rows"]
+    if c > 1:
+        return (f"16 B/cell-step algorithmic; the lattice stays in the registers of {c} 16-CTA clusters "
+                f"({16 * c} of 148 SMs; each cluster its band plus {g} ghost rows per side, swapped through "
+                f"global memory every {g} steps), so DRAM traffic is the initial read, the final write and "
+                f"the ghost-row swaps")
+    return ("16 B/cell-step algorithmic; the lattice stays in the registers of one 16-CTA cluster "
+            "(16 of 148 SMs), so DRAM traffic is the initial read and final write only")
+
+
+def sm_bound(t_solve, steps, n, clock_mhz, kernel, ops_per_cell=18):
+    """The compute bound of the forward solve on the SMs it occupies: 18 FP32 lane
+    operations per cell-step (an FMA counts once), 128 FP32 lanes per SM at the median
+    SM clock sampled during the timed solves, over the lattice's n x n cells
+    (`frac`) and over the rows the kernel actually computes, ghost rows included
+    (`frac_with_ghost_rows`)."""
     clk = float(clock_mhz or 1965.0) * 1e6
+    sms = kernel["sms"]
     bound = n * n * ops_per_cell / (sms * 128 * clk)
+    bound_all = kernel["rows_per_step"] * n * ops_per_cell / (sms * 128 * clk)
     per = t_solve / steps
     return {"sms_used": sms, "fp32_ops_per_cell_step": ops_per_cell, "sm_clock_hz": clk,
-            "bound_us_per_step": bound * 1e6, "achieved_us_per_step": per * 1e6, "frac": bound / per}
+            "bound_us_per_step": bound * 1e6, "achieved_us_per_step": per * 1e6, "frac": bound / per,
+            "rows_computed_per_step": kernel["rows_per_step"], "frac_with_ghost_rows": bound_all / per}
 
 
 def path_blocks(args):

@@ -21,6 +21,8 @@
 #include <cooperative_groups.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
+#include <type_traits>
 #include <vector>
 #include <cuda_runtime.h>
 #include "gs_kernels.h"
@@ -525,6 +527,7 @@ __global__ void __launch_bounds__(512, 1) k_gs_adjoint_cw(GSArgs<T> a, const T* 
 
 #include "gs_f32x2.cuh"
 #include "gs_rr.cuh"
+#include "gs_mc.cuh"
 
 // register-resident forward kernel for an n x n float32 lattice with *wpc warps per
 // CTA (*wpc = 0: the default split, written back), or NULL where the lattice does
@@ -541,6 +544,106 @@ const void* rr_kernel(int n, int* wpc, bool drift, size_t* smem) {
     GS_RR_CASE(256, 4) GS_RR_CASE(256, 8) GS_RR_CASE(256, 16)
 #undef GS_RR_CASE
     return nullptr;
+}
+
+// Multi-cluster forward kernels (gs_mc.cuh): variant 40 + index.  Each spreads one
+// lattice over `clusters` 16-CTA clusters with `ghost` ghost rows per band side.
+struct MCConfig {
+    int n, clusters, ghost, wpc;
+    const void* k[2];   // without / with drift
+    uint32_t smem;
+    size_t xfloats, flags;
+};
+template <int N, int C, int G, int W>
+MCConfig mc_config() {
+    using S = MCShape<N, C, G, W>;
+    return {N, C, G, W, {(const void*)k_gs_forward_mc<N, C, G, W, 0>, (const void*)k_gs_forward_mc<N, C, G, W, 1>},
+            S::kSmem, S::kXFloats, S::kFlags};
+}
+constexpr int kMCVariant = 40;
+constexpr int kMCConfigs = 7;
+// the automatic choice for n = 256: 4 clusters, 16 ghost rows (0.63 us per step
+// against 0.74 for the single-cluster kernel; (4, 8) and (4, 32) within 1 %)
+constexpr int kMCDefault = 2;
+const MCConfig& mc_table(int i) {
+    static const MCConfig t[kMCConfigs] = {mc_config<256, 2, 8, 9>(),   mc_config<256, 4, 8, 5>(),
+                                           mc_config<256, 4, 16, 6>(),  mc_config<256, 8, 8, 3>(),
+                                           mc_config<256, 8, 16, 4>(),  mc_config<256, 4, 32, 8>(),
+                                           mc_config<256, 2, 32, 12>()};
+    return t[i];
+}
+
+void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, cudaStream_t st) {
+    *cfg = {};
+    cfg->gridDim = dim3(kRRCluster * m.clusters, 1, 1);
+    cfg->blockDim = dim3(32 * m.wpc, 1, 1);
+    cfg->dynamicSmemBytes = m.smem;
+    cfg->stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kRRCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg->attrs = attr;
+    cfg->numAttrs = 1;
+}
+
+// whether every cluster of configuration i can be resident at once on the current
+// device (the kernel spins on the other clusters' flags), cached per device
+cudaError_t mc_fits(int i, bool drift, bool* fits) {
+    static int cache[64][kMCConfigs][2];   // 0 unknown, 1 fits, 2 does not
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) {
+        *fits = false;
+        return cudaSuccess;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    int& c = cache[dev][i][drift ? 1 : 0];
+    if (c == 0) {
+        const MCConfig& m = mc_table(i);
+        const void* fn = m.k[drift ? 1 : 0];
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute attr[1];
+        mc_launch_config(m, &cfg, attr, nullptr);
+        int active = 0;
+        e = cudaOccupancyMaxActiveClusters(&active, fn, &cfg);
+        if (e != cudaSuccess) return e;
+        c = active >= m.clusters ? 1 : 2;
+    }
+    *fits = c == 1;
+    return cudaSuccess;
+}
+
+// one multi-cluster solve: exchange buffer and flags from the stream-ordered pool
+// (private to this launch), flags cleared on the stream, then the kernel
+cudaError_t mc_forward(int i, const GSArgs<float>& a0, bool drift, const float* u0, const float* v0, float* u,
+                       float* v, float* trace, int every, cudaStream_t st) {
+    const MCConfig& m = mc_table(i);
+    const void* fn = m.k[drift ? 1 : 0];
+    const size_t xbytes = m.xfloats * sizeof(float), fbytes = m.flags * sizeof(uint32_t);
+    char* buf = nullptr;
+    cudaError_t e = pool_alloc((void**)&buf, xbytes + fbytes, st);
+    if (e != cudaSuccess) return e;
+    float* xb = reinterpret_cast<float*>(buf);
+    uint32_t* fl = reinterpret_cast<uint32_t*>(buf + xbytes);
+    e = cudaMemsetAsync(fl, 0, fbytes, st);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) {
+        GSArgs<float> a = a0;
+        void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every, &xb, &fl};
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute attr[1];
+        mc_launch_config(m, &cfg, attr, st);
+        e = cudaLaunchKernelExC(&cfg, fn, args);
+    }
+    cudaError_t e2 = pool_free(buf, st);
+    return e != cudaSuccess ? e : e2;
 }
 
 // register-resident adjoint kernel with wpc warps per CTA
@@ -673,7 +776,25 @@ cudaError_t gs_forward(const GSParams& p, const T* u0, const T* v0, T* u, T* v, 
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     int every = trace_every > 0 ? trace_every : 1;
     void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every};
-    if (sizeof(T) == 4 && cl == kRRCluster && (p.variant == 0 || p.variant == 3 || p.variant > 10)) {
+    if constexpr (std::is_same<T, float>::value) {
+        const bool drift = p.vx != 0.0 || p.vy != 0.0;
+        if (p.variant >= kMCVariant && p.variant < kMCVariant + kMCConfigs) {
+            const int i = p.variant - kMCVariant;
+            bool fits = false;
+            if (cl != kRRCluster || mc_table(i).n != p.n) return cudaErrorInvalidValue;
+            cudaError_t e = mc_fits(i, drift, &fits);
+            if (e != cudaSuccess) return e;
+            if (!fits) return cudaErrorInvalidConfiguration;
+            return mc_forward(i, a, drift, u0, v0, u, v, trace, every, st);
+        }
+        if (p.variant == 0 && cl == kRRCluster && p.n == mc_table(kMCDefault).n) {
+            bool fits = false;
+            cudaError_t e = mc_fits(kMCDefault, drift, &fits);
+            if (e != cudaSuccess) return e;
+            if (fits) return mc_forward(kMCDefault, a, drift, u0, v0, u, v, trace, every, st);
+        }
+    }
+    if (sizeof(T) == 4 && cl == kRRCluster && (p.variant == 0 || p.variant == 3 || (p.variant > 10 && p.variant < kMCVariant))) {
         size_t smem = 0;
         int wpc = p.variant > 10 ? p.variant - 10 : 0;
         const void* rk = rr_kernel(p.n, &wpc, p.vx != 0.0 || p.vy != 0.0, &smem);
@@ -695,12 +816,14 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     if (cl <= 0) return cudaErrorInvalidValue;
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad, &err};
-    if (sizeof(T) == 4 && cl == kRRCluster && (p.variant == 0 || p.variant == 3 || p.variant > 10)) {
+    // a multi-cluster forward variant pairs with the default adjoint
+    const int variant = p.variant >= kMCVariant ? 0 : p.variant;
+    if (sizeof(T) == 4 && cl == kRRCluster && (variant == 0 || variant == 3 || variant > 10)) {
         size_t smem = 0;
-        int wpc = p.variant > 10 ? p.variant - 10 : 0;
+        int wpc = variant > 10 ? variant - 10 : 0;
         const void* rk = rr_adj_kernel(p.n, &wpc, p.vx != 0.0 || p.vy != 0.0, &smem);
         if (rk) return launch_cluster<T>(rk, p.n, cl, smem, st, args, dim3(32 * wpc, 1, 1));
-        if (p.variant != 0) return cudaErrorInvalidValue;
+        if (variant != 0) return cudaErrorInvalidValue;
     }
     const dim3 blk = sizeof(T) == 4 ? x2_block(p.n, cl, 512) : cw_block(p.n, cl, 512);
     const void* ak = adj_kernel<T>(p.n);
@@ -722,7 +845,7 @@ cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMemb
         drift = drift || m.vx != 0.0 || m.vy != 0.0;
     }
     size_t smem = 0;
-    int wpc = p.variant > 10 ? p.variant - 10 : 0;
+    int wpc = p.variant > 10 && p.variant < kMCVariant ? p.variant - 10 : 0;   // one lattice per cluster
     const void* rk = rr_kernel(p.n, &wpc, drift, &smem);
     if (!rk) return cudaErrorInvalidValue;
     GSArgs<float>* d = nullptr;
@@ -754,6 +877,27 @@ cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMemb
     }
     cudaError_t e2 = pool_free(d, st);
     return e != cudaSuccess ? e : e2;
+}
+
+cudaError_t gs_auto_variant(int n, bool drift, int* variant) {
+    const int cl = gs_cluster_size(n, 4);
+    if (cl == kRRCluster && n == mc_table(kMCDefault).n) {
+        bool fits = false;
+        cudaError_t e = mc_fits(kMCDefault, drift, &fits);
+        if (e != cudaSuccess) return e;
+        if (fits) {
+            *variant = kMCVariant + kMCDefault;
+            return cudaSuccess;
+        }
+    }
+    size_t smem = 0;
+    int wpc = 0;
+    if (cl == kRRCluster && rr_kernel(n, &wpc, drift, &smem)) {
+        *variant = 10 + wpc;
+        return cudaSuccess;
+    }
+    *variant = cl > 0 && x2_block(n, cl, 512).x != 0 && fwd_kernel<float>(n) ? 2 : 1;
+    return cudaSuccess;
 }
 
 cudaError_t gs_batch_capacity(int n, int* clusters) {

@@ -220,6 +220,15 @@ int gpgmp_gs_batch_capacity(int32_t n, int32_t* lattices) {
     return GPGMP_OK;
 }
 
+int gpgmp_gs_auto_variant(int32_t n, int32_t drift, int32_t* variant) {
+    if (!variant) return set_error(GPGMP_ERR_INVALID, "NULL argument");
+    if (n <= 2) return set_error(GPGMP_ERR_INVALID, "n %d", n);
+    int v = 0;
+    CK(gs_auto_variant(n, drift != 0, &v));
+    *variant = v;
+    return GPGMP_OK;
+}
+
 int gpgmp_gs_status(int32_t* flags) {
     if (!flags) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     CK(cudaDeviceSynchronize());

@@ -26,6 +26,8 @@ cudaError_t gs_forward_batch_f32(const GSParams& p, int batch, const GSBatchMemb
 // how many lattices of side n a batched launch runs at the same time on this device
 // (16-CTA clusters that fit at once)
 cudaError_t gs_batch_capacity(int n, int* clusters);
+// the float32 family variant 0 resolves to for an n x n lattice on the current device
+cudaError_t gs_auto_variant(int n, bool drift, int* variant);
 
 // reads (and with clear, resets) the device word that the register-resident forward
 // kernel sets when one of its bounded waits gave up; synchronous

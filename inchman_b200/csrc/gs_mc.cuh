@@ -1,0 +1,282 @@
+// Register-resident float32 Gray-Scott forward kernel over C thread-block clusters.
+//
+// The single-cluster kernel (gs_rr.cuh) runs one lattice on 16 SMs; its step time is
+// the arithmetic of 16 rows per SM plus one neighbour hop.  Here the lattice's N rows
+// are cut into C bands of B = N / C rows, one band per 16-CTA cluster, so each SM
+// holds a few rows (one per warp) and the arithmetic per step shrinks C-fold.
+//
+// Clusters cannot exchange rows through distributed shared memory, so each cluster
+// also keeps G ghost rows on each side of its band (L = B + 2G rows per cluster, one
+// per warp, WPC = L / 16 warps per CTA) and runs exactly the single-cluster kernel's
+// ring inside the cluster: every step a warp waits for its two neighbours' rows,
+// computes its row and sends it to them.  The ring's two ends (the outermost ghost
+// rows) have no true neighbour, so a ghost row's value goes stale one row per step
+// from the outside in; after G steps every ghost row is stale while the band rows,
+// at least G rows from the ring's ends, are still exact.  At every state m * G the
+// clusters swap rows through global memory: the G first and G last band rows of each
+// cluster are written to an exchange buffer and flagged (one flag per lane), and the
+// warps that own the ghost rows wait for the neighbouring clusters' flags and take
+// the fresh rows before they send them on.  Every row of the band is therefore computed from exactly
+// the values the single-cluster kernel uses: the result is bit-identical to it.
+//
+// The exchange buffer is double-buffered by the parity of m.  A cluster writes the
+// block m + 2 buffer only after its ghost rows were refreshed at state (m + 1) G from
+// rows its neighbour computed after reading block m, so no buffer is overwritten
+// before it has been read.  A flag holds the m of the last block published into its
+// rows; the host clears the flags on the launching stream before every launch (a
+// captured graph replays that clear too).  Every wait is bounded; a wait that gives
+// up marks the CTA failed and its rows are written as NaN.
+//
+// All C clusters must be resident at once; the host checks that with
+// cudaOccupancyMaxActiveClusters (shared memory is padded so one CTA holds one SM)
+// and otherwise runs the single-cluster kernel.
+//
+// Included from gray_scott.cu after gs_rr.cuh.
+
+constexpr uint32_t kMCFlagWaitLimit = 1u << 22;
+
+template <int N, int C, int G, int WPC>
+struct MCShape {
+    static constexpr int B = N / C;                    // band rows per cluster
+    static constexpr int L = B + 2 * G;                // rows per cluster (one per warp)
+    static constexpr int H = N / 64;                   // column pairs per lane
+    static constexpr uint32_t kRow = 4u * N;           // bytes of one halo row of one field
+    static constexpr uint32_t kHalo = (uint32_t)WPC * 8u * kRow;
+    static constexpr uint32_t kUsed = kHalo + (uint32_t)WPC * 16u + 16u;
+    // at least 120 KB, so that no SM holds two CTAs (the steps are latency-bound: two
+    // rows' arithmetic on one SM would lengthen every step)
+    static constexpr uint32_t kSmem = kUsed > 120u * 1024u ? kUsed : 120u * 1024u;
+    // exchange buffer floats: [parity][cluster][side][g][field][N]
+    static constexpr size_t kXFloats = (size_t)2 * C * 2 * G * 2 * N;
+    static constexpr size_t kFlags = (size_t)C * 2 * G * 32;  // flags [cluster][side][g][lane]
+    static_assert(N % C == 0 && C >= 2, "bands");
+    static_assert(L == kRRCluster * WPC, "one row per warp");
+    static_assert(B >= 2 * G && G >= 1, "band rows at least G rows from the ring's ends");
+    static_assert(kSmem <= 227u * 1024u, "shared memory of a B200 CTA");
+    static_assert(64 * H == N, "lane layout");
+};
+
+__device__ __forceinline__ uint32_t mc_ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void mc_st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// one lane's 2H columns of a row in global memory, read through L2 (the exchange
+// buffer is rewritten by other SMs, so no line of it may come from this SM's L1)
+template <int H>
+__device__ __forceinline__ void mc_load_cg(const float* __restrict__ p, float2 (&x)[H]) {
+    static_assert(H % 4 == 0, "16-byte loads");
+#pragma unroll
+    for (int q = 0; q < H / 4; ++q) {
+        const float4 a = __ldcg(reinterpret_cast<const float4*>(p) + q);
+        const float4 b = __ldcg(reinterpret_cast<const float4*>(p + H) + q);
+        x[4 * q] = make_float2(a.x, b.x);
+        x[4 * q + 1] = make_float2(a.y, b.y);
+        x[4 * q + 2] = make_float2(a.z, b.z);
+        x[4 * q + 3] = make_float2(a.w, b.w);
+    }
+}
+
+template <int N, int C, int G, int WPC>
+struct MCCtx {
+    using S = MCShape<N, C, G, WPC>;
+    uint32_t sbase;
+    const unsigned char* smem;
+    int lane, w;
+    uint32_t up_rank, dn_rank;
+    int up_w, dn_w;
+    bool up_remote, dn_remote;
+    uint32_t tx;             // bytes the producers in other CTAs deliver per phase
+    volatile int* failed;
+    // exchange roles of this warp's row: source of a neighbour's ghost row, or ghost row
+    float* src_row;          // where this row goes at a swap, or nullptr
+    uint32_t* src_flag;
+    const float* ghost_row;  // where this row comes from at a swap, or nullptr
+    const uint32_t* ghost_flag;
+    size_t parity_stride;    // floats between the two parities of the exchange buffer
+    __device__ __forceinline__ uint32_t slot(int ww, int par, int side, int f) const {
+        return sbase + (uint32_t)(((ww * 2 + par) * 2 + side) * 2 + f) * S::kRow;
+    }
+    __device__ __forceinline__ uint32_t bar(int ww, int par) const { return sbase + S::kHalo + (uint32_t)(ww * 2 + par) * 8u; }
+};
+
+// the swap at state m * G of a warp's freshly computed row y (see the file comment)
+template <int N, int C, int G, int WPC>
+__device__ __forceinline__ void mc_swap(const MCCtx<N, C, G, WPC>& c, float2 (&yu)[N / 64], float2 (&yv)[N / 64],
+                                        int m) {
+    constexpr int H = N / 64;
+    const size_t poff = (size_t)(m & 1) * c.parity_stride;
+    const int col0 = c.lane * 2 * H;
+    const uint32_t want = (uint32_t)m;
+    // each lane publishes its own columns under its own flag (a release store orders
+    // the lane's row stores before it) and the lane of the same index reads them
+    if (c.src_row) {
+        rr_store<H>(c.src_row + poff + col0, yu);
+        rr_store<H>(c.src_row + poff + N + col0, yv);
+        mc_st_release(c.src_flag + c.lane, want);
+    }
+    if (c.ghost_row) {
+        if (!*c.failed) {
+            uint32_t it = 0;
+            while (mc_ld_acquire(c.ghost_flag + c.lane) < want) {
+                if (++it == kMCFlagWaitLimit) {
+                    *c.failed = 1;
+                    break;
+                }
+            }
+        }
+        __syncwarp();
+        mc_load_cg<H>(c.ghost_row + poff + col0, yu);
+        mc_load_cg<H>(c.ghost_row + poff + N + col0, yv);
+    }
+}
+
+// one step X -> Y of the warp's row (s: the step index of X; send: whether Y goes out)
+template <int N, int C, int G, int WPC, int DRIFT>
+__device__ __forceinline__ void mc_step(const MCCtx<N, C, G, WPC>& c, const GSCoef2& k, const float2 (&xu)[N / 64],
+                                        const float2 (&xv)[N / 64], float2 (&yu)[N / 64], float2 (&yv)[N / 64],
+                                        int s, bool send) {
+    constexpr int H = N / 64;
+    const int par = s & 1;
+    rr_wait(c.bar(c.w, par), (uint32_t)(s >> 1) & 1u, c.failed);
+    __syncwarp();
+    if (c.lane == 0) rr_arm(c.bar(c.w, par), c.tx);   // the phase of step s + 2
+    float2 au[H], av[H], bu[H], bv[H];
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 0) - c.sbase), c.lane, au);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 1) - c.sbase), c.lane, av);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 0) - c.sbase), c.lane, bu);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 1) - c.sbase), c.lane, bv);
+    rr_row<H, DRIFT>(k, au, xu, bu, av, xv, bv, yu, yv, c.lane);
+    if (send) {
+        if ((s + 1) % G == 0) mc_swap<N, C, G, WPC>(c, yu, yv, (s + 1) / G);
+        const int np = par ^ 1;
+        rr_send<H>(yu, yv, c.slot(c.up_w, np, 1, 0), c.slot(c.up_w, np, 1, 1), c.bar(c.up_w, np), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(yu, yv, c.slot(c.dn_w, np, 0, 0), c.slot(c.dn_w, np, 0, 1), c.bar(c.dn_w, np), c.dn_remote,
+                   c.dn_rank, c.lane);
+    }
+}
+
+template <int N, int C, int G, int WPC, int DRIFT>
+__global__ void __launch_bounds__(32 * WPC, 1)
+    k_gs_forward_mc(GSArgs<float> a, const float* __restrict__ u0, const float* __restrict__ v0,
+                    float* __restrict__ uo, float* __restrict__ vo, float* __restrict__ trace, int trace_every,
+                    float* __restrict__ xbuf, uint32_t* __restrict__ flags) {
+    using S = MCShape<N, C, G, WPC>;
+    constexpr int H = S::H, B = S::B;
+    constexpr int NN = N * N;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MCCtx<N, C, G, WPC> c;
+    c.smem = smem_raw;
+    c.sbase = smem_u32(smem_raw);
+    c.lane = threadIdx.x & 31;
+    c.w = threadIdx.x >> 5;
+    const uint32_t rank = rr_ctarank();
+    const int cl = (int)blockIdx.x / kRRCluster;
+    c.up_remote = c.w == 0;
+    c.dn_remote = c.w == WPC - 1;
+    c.up_rank = c.up_remote ? (rank + kRRCluster - 1) % kRRCluster : rank;
+    c.dn_rank = c.dn_remote ? (rank + 1) % kRRCluster : rank;
+    c.up_w = c.up_remote ? WPC - 1 : c.w - 1;
+    c.dn_w = c.dn_remote ? 0 : c.w + 1;
+    c.failed = reinterpret_cast<volatile int*>(smem_raw + S::kHalo + WPC * 16);
+    const int nremote = (int)c.up_remote + (int)c.dn_remote;
+    c.tx = (uint32_t)nremote * 2u * S::kRow;
+    // local row l of cluster cl is lattice row cl * B - G + l (periodic)
+    const int l = (int)rank * WPC + c.w;
+    const int row = (cl * B - G + l + N) % N;
+    const int col0 = c.lane * 2 * H;
+    // exchange roles: rows [G, 2G) feed the cluster above (side 0), rows [B, B + G) the
+    // cluster below (side 1); ghost rows [0, G) come from the cluster above's side 1,
+    // ghost rows [B + G, B + 2G) from the cluster below's side 0
+    auto xrow = [&](int cluster, int side, int g) {
+        return xbuf + ((((size_t)cluster * 2 + side) * G + g) * 2) * N;
+    };
+    auto xflag = [&](int cluster, int side, int g) { return flags + (((size_t)cluster * 2 + side) * G + g) * 32; };
+    c.parity_stride = (size_t)C * 2 * G * 2 * N;
+    c.src_row = nullptr;
+    c.src_flag = nullptr;
+    c.ghost_row = nullptr;
+    c.ghost_flag = nullptr;
+    if (l >= G && l < 2 * G) {
+        c.src_row = xrow(cl, 0, l - G);
+        c.src_flag = xflag(cl, 0, l - G);
+    } else if (l >= B && l < B + G) {
+        c.src_row = xrow(cl, 1, l - B);
+        c.src_flag = xflag(cl, 1, l - B);
+    } else if (l < G) {
+        const int up = (cl + C - 1) % C;
+        c.ghost_row = xrow(up, 1, l);
+        c.ghost_flag = xflag(up, 1, l);
+    } else if (l >= B + G) {
+        const int dn = (cl + 1) % C;
+        c.ghost_row = xrow(dn, 0, l - B - G);
+        c.ghost_flag = xflag(dn, 0, l - B - G);
+    }
+    const bool band = l >= G && l < G + B;
+    const GSCoef2 k(a);
+
+    if (c.lane == 0) {
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 0) - c.sbase)), 1 + 32 * (2 - nremote));
+        mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 1) - c.sbase)), 1 + 32 * (2 - nremote));
+        fence_mbar_init();
+    }
+    if (threadIdx.x == 0) *c.failed = 0;
+    float2 xu[H], xv[H], yu[H], yv[H];
+    rr_load<H>(u0 + (size_t)row * N + col0, xu);
+    rr_load<H>(v0 + (size_t)row * N + col0, xv);
+    __syncthreads();
+    cluster_arrive();     // every CTA's mbarriers exist before anyone sends
+    cluster_wait();
+    const int steps = a.steps;
+    const int every = trace_every > 0 ? trace_every : 1;
+    if (steps > 0) {
+        if (c.lane == 0) {
+            rr_arm(c.bar(c.w, 0), c.tx);
+            rr_arm(c.bar(c.w, 1), c.tx);
+        }
+        rr_send<H>(xu, xv, c.slot(c.up_w, 0, 1, 0), c.slot(c.up_w, 0, 1, 1), c.bar(c.up_w, 0), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(xu, xv, c.slot(c.dn_w, 0, 0, 0), c.slot(c.dn_w, 0, 0, 1), c.bar(c.dn_w, 0), c.dn_remote,
+                   c.dn_rank, c.lane);
+    }
+    auto put_trace = [&](int s, const float2 (&pu)[H], const float2 (&pv)[H]) {
+        if (trace != nullptr && band && s % every == 0) {
+            float* du = trace + (size_t)(2 * (s / every)) * NN;
+            rr_store<H>(du + (size_t)row * N + col0, pu);
+            rr_store<H>(du + NN + (size_t)row * N + col0, pv);
+        }
+    };
+    int s = 0;
+    for (; s + 2 <= steps; s += 2) {      // two steps per iteration: X -> Y -> X without copies
+        put_trace(s, xu, xv);
+        mc_step<N, C, G, WPC, DRIFT>(c, k, xu, xv, yu, yv, s, true);
+        put_trace(s + 1, yu, yv);
+        mc_step<N, C, G, WPC, DRIFT>(c, k, yu, yv, xu, xv, s + 1, s + 2 < steps);
+    }
+    const bool odd = s < steps;
+    if (odd) {
+        put_trace(s, xu, xv);
+        mc_step<N, C, G, WPC, DRIFT>(c, k, xu, xv, yu, yv, s, false);
+    }
+    __syncthreads();
+    cluster_arrive();     // no CTA leaves while a neighbour may still address its shared memory
+    cluster_wait();
+    const bool bad = *c.failed != 0;
+    if (bad && threadIdx.x == 0) atomicOr(&g_gs_fwd_err, 1);
+    if (band) {
+        const float nan = __int_as_float(0x7fc00000);
+        float2 pu[H], pv[H];
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            pu[j] = bad ? make_float2(nan, nan) : (odd ? yu[j] : xu[j]);
+            pv[j] = bad ? make_float2(nan, nan) : (odd ? yv[j] : xv[j]);
+        }
+        rr_store<H>(uo + (size_t)row * N + col0, pu);
+        rr_store<H>(vo + (size_t)row * N + col0, pv);
+    }
+}

@@ -40,6 +40,7 @@ _SIGS = {
     "gpgmp_gs_status": (C.c_int, [C.POINTER(C.c_int32)]),
     "gpgmp_gs_forward_batch_f32": (C.c_int, [C.POINTER(GSParams), C.c_int32, C.c_void_p] + [C.c_void_p] * 5),
     "gpgmp_gs_batch_capacity": (C.c_int, [C.c_int32, C.POINTER(C.c_int32)]),
+    "gpgmp_gs_auto_variant": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
 }
 _lib.SIGNATURES.update(_SIGS)
 
@@ -145,6 +146,19 @@ def batch_capacity(n: int) -> int:
     c = C.c_int32(0)
     _lib.check(_fn("gpgmp_gs_batch_capacity")(n, C.byref(c)), "gpgmp_gs_batch_capacity")
     return int(c.value)
+
+
+# multi-cluster float32 forward families: variant -> (16-CTA clusters, ghost rows per band side)
+MULTI_CLUSTER = {40: (2, 8), 41: (4, 8), 42: (4, 16), 43: (8, 8), 44: (8, 16), 45: (4, 32), 46: (2, 32)}
+
+
+def auto_variant(n: int, drift: bool = False) -> int:
+    """The float32 kernel family that variant 0 resolves to for an n x n lattice on
+    this GPU (42: four 16-CTA clusters; 10 + w: one cluster, w warps per CTA; 2: the
+    shared-memory column walk; 1: one cell per iteration)."""
+    v = C.c_int32(0)
+    _lib.check(_fn("gpgmp_gs_auto_variant")(n, int(drift), C.byref(v)), "gpgmp_gs_auto_variant")
+    return int(v.value)
 
 
 def status() -> int:

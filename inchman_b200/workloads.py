@@ -399,7 +399,9 @@ def scan_sort(args, rank, world):
     scanned values/s; the sorts are reported beside it in keys/s.
 
     Roofline (scan): 8 B per value (read, write); (sort) 16 B per key and pass (read
-    key and value, write key and value)."""
+    key and value, write key and value).  Library comparators, timed the same way on
+    the same inputs: torch.cumsum (int32) beside the scan, torch.sort(stable=True)
+    (int32 keys with int64 indices) beside each sort."""
     import torch
     from . import individual as ind
     dev = "cuda"
@@ -424,6 +426,10 @@ def scan_sort(args, rank, world):
 
     t_scan = timed(lambda: ind._call("gpgmp_exclusive_scan_u32", ind._ptr(x), ind._ptr(out), n, ind._ptr(scr),
                                      scr.numel(), ind._stream()))
+    # library comparator: torch.cumsum on the same int32 values (inclusive, int32 out)
+    lib_out = torch.empty_like(x)
+    t_cumsum = timed(lambda: torch.cumsum(x, 0, dtype=torch.int32, out=lib_out))
+    del lib_out
     peak, peak_kind = _peaks()
     ns = 1 << 24
     sorts = {}
@@ -435,14 +441,18 @@ def scan_sort(args, rank, world):
         t = timed(lambda: ind._call("gpgmp_sort_pairs_u32", ind._ptr(k), ind._ptr(v), ind._ptr(ko), ind._ptr(vo), ns,
                                     bits, ind._ptr(sscr), sscr.numel(), ind._stream()))
         ach = 16.0 * passes * ns / t / 1e9
+        # library comparator on the same keys: torch.sort(stable=True) (int32 keys, int64
+        # indices as the values: 12 B per key moved each pass instead of 8)
+        t_lib = timed(lambda: torch.sort(k, stable=True))
         sorts[f"keys_{bits}bit"] = {"pairs": ns, "passes": passes, "ms_per_sort": t * 1e3, "keys_per_s": ns / t,
                                     "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                                                 "frac": ach / peak, "peak_kind": peak_kind}}
+                                                 "frac": ach / peak, "peak_kind": peak_kind},
+                                    "torch_sort_stable_ms": t_lib * 1e3}
         del k, v, ko, vo, sscr
     ach = 8.0 * n / t_scan / 1e9
     return _base(args, world, n / t_scan, "values/s", "scan_2^27_u32_sort_2^24_pairs",
                  {"scan_values": n, "sort_pairs": ns, "l2": "inputs larger than L2 (scan)"}, t_scan * 1e3,
-                 {"dtype": "u32", "sorts": sorts,
+                 {"dtype": "u32", "sorts": sorts, "torch_cumsum_int32_ms": t_cumsum * 1e3,
                   # per timed scan: one scan kernel; per sort: histogram + one kernel per pass
                   "gpu_launches": args.steps * (1 + (1 + 2) + (1 + 4)),
                   "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,

@@ -271,11 +271,18 @@ typedef struct gpgmp_gs_params {
     double  F, k, Du, Dv, vx, vy, dt;
     int32_t checkpoint_every;   /* <= 0: 100 */
     int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
-    int32_t variant;            /* kernel family (float32): 0 automatic = register-resident where
-                                   the lattice allows (n 64, 128, 256 on a 16-CTA cluster), else the
-                                   shared-memory column walk; 1 one cell per iteration; 2 shared-memory
-                                   column walk; 3 register-resident; 10 + w register-resident with w
-                                   warps per CTA.  float64 always uses 0 / 1 (column walk / per cell). */
+    int32_t variant;            /* kernel family (float32): 0 automatic = for n = 256 the
+                                   multi-cluster kernel 42 where the device holds its four clusters at
+                                   once, else register-resident where the lattice allows (n 64, 128,
+                                   256 on a 16-CTA cluster), else the shared-memory column walk;
+                                   1 one cell per iteration; 2 shared-memory column walk;
+                                   3 register-resident; 10 + w register-resident with w warps per
+                                   CTA; 40 + i multi-cluster (n = 256; clusters, ghost rows):
+                                   i = 0 (2, 8), 1 (4, 8), 2 (4, 16), 3 (8, 8), 4 (8, 16),
+                                   5 (4, 32), 6 (2, 32), a CUDA error where the device cannot hold
+                                   all its clusters at once.  Every float32 family gives the same
+                                   bits.  float64 always uses 0 / 1 (column walk / per cell).  The
+                                   adjoint and the batched forward treat 40 + i as 0. */
 } gpgmp_gs_params;
 
 /* bytes of the checkpoint buffer and of the adjoint's work buffer */
@@ -302,6 +309,9 @@ int gpgmp_gs_forward_batch_f32(const gpgmp_gs_params* p, int32_t batch, const do
 /* how many lattices of side n gpgmp_gs_forward_batch_f32 runs at the same time on the
  * current device (its 16-CTA clusters that are resident at once) */
 int gpgmp_gs_batch_capacity(int32_t n, int32_t* lattices);
+/* the float32 kernel family (gpgmp_gs_params.variant) that variant 0 resolves to for an
+ * n x n lattice, with (drift != 0) or without drift, on the current device */
+int gpgmp_gs_auto_variant(int32_t n, int32_t drift, int32_t* variant);
 /* Status of the forward kernels on the current device: *flags != 0 if a bounded wait
  * inside a register-resident forward solve gave up since the last call (that solve's
  * output is NaN).  Synchronises the device and clears the flags.  No counterpart in

@@ -1,0 +1,111 @@
+"""GPU parity of the multi-cluster float32 Gray-Scott forward kernel.
+
+The multi-cluster kernel spreads one 256 x 256 lattice over 2, 4 or 8 thread-block
+clusters with G ghost rows per band side, swapped through global memory every G
+steps.  Each band row sees exactly the values of the single-cluster kernel, so every
+configuration must give the same bits: final state and every stored checkpoint, at
+step counts around the swap period (G - 1, G, G + 1, 2G + 1), with and without drift,
+and bit for bit against the oracle's float32 restatement over 1000 steps."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _variants():
+    from inchman_b200.gray_scott import MULTI_CLUSTER
+    return sorted(MULTI_CLUSTER)
+
+
+def _cfg(**kw):
+    from inchman_b200.gray_scott import GrayScottConfig
+    return GrayScottConfig(**kw)
+
+
+def _run(cfg, variant, tu, tv, every, steps):
+    import torch
+    from inchman_b200 import gray_scott as gs
+    n = cfg.n
+    nck = max(1, -(-steps // every))
+    ck = torch.full((nck, 2, n, n), float("nan"), device="cuda")
+    u, v = gs.forward(tu, tv, cfg.params(variant=variant, checkpoint_every=every), checkpoints=ck if steps else None)
+    torch.cuda.synchronize()
+    return u, v, ck
+
+
+def _fits(variant):
+    """Whether the device holds all clusters of the variant at once (else the library
+    refuses the launch with an error; it never starts a kernel that could wait on a
+    cluster that is not running)."""
+    import torch
+    from inchman_b200 import _lib
+    cfg = _cfg(n=256, steps=1)
+    t = torch.zeros((256, 256), device="cuda")
+    try:
+        _run(cfg, variant, t, t, 1, 1)
+    except _lib.GpgmpError:
+        return False
+    return True
+
+
+@pytest.mark.parametrize("steps,drift,every", [(0, False, 1), (1, True, 1), (7, False, 3), (8, True, 8),
+                                               (9, False, 2), (16, True, 5), (17, False, 1), (33, True, 4),
+                                               (31, False, 3), (32, True, 1), (65, False, 9), (301, True, 7), (1000, False, 100)])
+def test_multicluster_forward_bit_identical_to_single_cluster(gpgmp, steps, drift, every):
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=256, steps=steps, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0)
+    u0, v0 = cfg.initial_state(np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    ru, rv, rck = _run(cfg, 3, tu, tv, every, steps)
+    ran = 0
+    for var in _variants():
+        if not _fits(var):
+            continue
+        u, v, ck = _run(cfg, var, tu, tv, every, steps)
+        assert torch.equal(u, ru) and torch.equal(v, rv), (var, int((u != ru).sum()), int((v != rv).sum()))
+        if steps:
+            assert torch.equal(ck, rck), var
+        ran += 1
+    assert ran >= 1, "no multi-cluster configuration fits this device"
+    assert gs.status() == 0
+
+
+def test_multicluster_forward_bit_exact_against_oracle(gpgmp):
+    """The automatic 4-cluster configuration (16 ghost rows), 1000 steps with drift, bit
+    for bit against the oracle's float32 restatement of the kernels' operation order."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=256, steps=1000, vx=0.05, vy=-0.03, variant=42)
+    if not _fits(42):
+        pytest.skip("4 clusters of 16 CTAs are not co-resident on this device")
+    u0, v0 = cfg.initial_state(np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    u, v = gs.forward(tu, tv, cfg.params())
+    torch.cuda.synchronize()
+    gu, gv = u.cpu().numpy(), v.cpu().numpy()
+    ou, ov = u0.astype(np.float32).copy(), v0.astype(np.float32).copy()
+    oracle.orc().orc_gs_forward_f32(cfg.n, cfg.steps, cfg.F, cfg.k, cfg.Du, cfg.Dv, cfg.vx, cfg.vy, cfg.dt,
+                                    oracle.ptr(ou), oracle.ptr(ov))
+    assert gs.status() == 0
+    assert np.array_equal(gu.view(np.uint32), ou.view(np.uint32)), int((gu != ou).sum())
+    assert np.array_equal(gv.view(np.uint32), ov.view(np.uint32)), int((gv != ov).sum())
+
+
+def test_automatic_choice_is_the_multicluster_kernel(gpgmp):
+    """On a B200 variant 0 resolves to four clusters for 256 x 256 (the device holds
+    them at once) and runs it: same bits as naming variant 42, with and without drift."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    for drift in (False, True):
+        assert gs.auto_variant(256, drift) == 42
+        cfg = _cfg(n=256, steps=50, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0)
+        u0, v0 = cfg.initial_state(np.float32)
+        tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+        a = _run(cfg, 0, tu, tv, 7, 50)
+        b = _run(cfg, 42, tu, tv, 7, 50)
+        assert all(torch.equal(x, y) for x, y in zip(a, b))
+    assert gs.auto_variant(128) == 14   # one cluster, 4 warps per CTA
+    assert gs.status() == 0
