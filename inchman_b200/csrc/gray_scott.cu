@@ -550,14 +550,16 @@ const void* rr_kernel(int n, int* wpc, bool drift, size_t* smem) {
 // lattice over `clusters` 16-CTA clusters with `ghost` ghost rows per band side.
 struct MCConfig {
     int n, clusters, ghost, wpc;
-    const void* k[2];   // without / with drift
+    const void* k[2][2];   // [forward / adjoint][without / with drift]
     uint32_t smem;
     size_t xfloats, flags;
 };
 template <int N, int C, int G, int W>
 MCConfig mc_config() {
     using S = MCShape<N, C, G, W>;
-    return {N, C, G, W, {(const void*)k_gs_forward_mc<N, C, G, W, 0>, (const void*)k_gs_forward_mc<N, C, G, W, 1>},
+    return {N, C, G, W,
+            {{(const void*)k_gs_forward_mc<N, C, G, W, 0>, (const void*)k_gs_forward_mc<N, C, G, W, 1>},
+             {(const void*)k_gs_adjoint_mc<N, C, G, W, 0>, (const void*)k_gs_adjoint_mc<N, C, G, W, 1>}},
             S::kSmem, S::kXFloats, S::kFlags};
 }
 constexpr int kMCVariant = 40;
@@ -573,7 +575,10 @@ const MCConfig& mc_table(int i) {
     return t[i];
 }
 
-void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, cudaStream_t st) {
+// launch configuration of a multi-cluster kernel; cooperative: all CTAs resident at
+// once (the clusters wait on one another's flags), asked of the launch itself
+void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, cudaStream_t st,
+                      bool cooperative) {
     *cfg = {};
     cfg->gridDim = dim3(kRRCluster * m.clusters, 1, 1);
     cfg->blockDim = dim3(32 * m.wpc, 1, 1);
@@ -583,14 +588,16 @@ void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttr
     attr[0].val.clusterDim.x = kRRCluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeCooperative;
+    attr[1].val.cooperative = 1;
     cfg->attrs = attr;
-    cfg->numAttrs = 1;
+    cfg->numAttrs = cooperative ? 2 : 1;
 }
 
 // whether every cluster of configuration i can be resident at once on the current
 // device (the kernel spins on the other clusters' flags), cached per device
-cudaError_t mc_fits(int i, bool drift, bool* fits) {
-    static int cache[64][kMCConfigs][2];   // 0 unknown, 1 fits, 2 does not
+cudaError_t mc_fits(int i, bool drift, bool* fits, int kind = 0) {
+    static int cache[64][kMCConfigs][2][2];   // [dev][config][forward / adjoint][drift]: 0 unknown, 1 fits, 2 not
     static std::mutex mu;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -600,16 +607,16 @@ cudaError_t mc_fits(int i, bool drift, bool* fits) {
         return cudaSuccess;
     }
     std::lock_guard<std::mutex> lock(mu);
-    int& c = cache[dev][i][drift ? 1 : 0];
+    int& c = cache[dev][i][kind][drift ? 1 : 0];
     if (c == 0) {
         const MCConfig& m = mc_table(i);
-        const void* fn = m.k[drift ? 1 : 0];
+        const void* fn = m.k[kind][drift ? 1 : 0];
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
         cudaLaunchConfig_t cfg;
-        cudaLaunchAttribute attr[1];
-        mc_launch_config(m, &cfg, attr, nullptr);
+        cudaLaunchAttribute attr[2];
+        mc_launch_config(m, &cfg, attr, nullptr, false);
         int active = 0;
         e = cudaOccupancyMaxActiveClusters(&active, fn, &cfg);
         if (e != cudaSuccess) return e;
@@ -619,12 +626,12 @@ cudaError_t mc_fits(int i, bool drift, bool* fits) {
     return cudaSuccess;
 }
 
-// one multi-cluster solve: exchange buffer and flags from the stream-ordered pool
-// (private to this launch), flags cleared on the stream, then the kernel
-cudaError_t mc_forward(int i, const GSArgs<float>& a0, bool drift, const float* u0, const float* v0, float* u,
-                       float* v, float* trace, int every, cudaStream_t st) {
+// one multi-cluster launch (kind 0 forward, 1 adjoint segment): exchange buffer and
+// flags from the stream-ordered pool (private to this launch), flags cleared on the
+// stream, then the kernel with `args` followed by the buffer and flag pointers
+cudaError_t mc_run(int i, int kind, bool drift, void** args, int nargs, cudaStream_t st) {
     const MCConfig& m = mc_table(i);
-    const void* fn = m.k[drift ? 1 : 0];
+    const void* fn = m.k[kind][drift ? 1 : 0];
     const size_t xbytes = m.xfloats * sizeof(float), fbytes = m.flags * sizeof(uint32_t);
     char* buf = nullptr;
     cudaError_t e = pool_alloc((void**)&buf, xbytes + fbytes, st);
@@ -635,15 +642,24 @@ cudaError_t mc_forward(int i, const GSArgs<float>& a0, bool drift, const float* 
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) {
-        GSArgs<float> a = a0;
-        void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every, &xb, &fl};
+        void* all[16];
+        for (int q = 0; q < nargs; ++q) all[q] = args[q];
+        all[nargs] = &xb;
+        all[nargs + 1] = &fl;
         cudaLaunchConfig_t cfg;
-        cudaLaunchAttribute attr[1];
-        mc_launch_config(m, &cfg, attr, st);
-        e = cudaLaunchKernelExC(&cfg, fn, args);
+        cudaLaunchAttribute attr[2];
+        mc_launch_config(m, &cfg, attr, st, true);
+        e = cudaLaunchKernelExC(&cfg, fn, all);
     }
     cudaError_t e2 = pool_free(buf, st);
     return e != cudaSuccess ? e : e2;
+}
+
+cudaError_t mc_forward(int i, const GSArgs<float>& a0, bool drift, const float* u0, const float* v0, float* u,
+                       float* v, float* trace, int every, cudaStream_t st) {
+    GSArgs<float> a = a0;
+    void* args[] = {&a, (void*)&u0, (void*)&v0, &u, &v, &trace, &every};
+    return mc_run(i, 0, drift, args, 7, st);
 }
 
 // register-resident adjoint kernel with wpc warps per CTA
@@ -816,7 +832,23 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     if (cl <= 0) return cudaErrorInvalidValue;
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad, &err};
-    // a multi-cluster forward variant pairs with the default adjoint
+    if constexpr (std::is_same<T, float>::value) {
+        // the multi-cluster adjoint, with a multi-cluster variant only: in the gradient
+        // it runs beside the segment recomputation on the side stream, and two 64-SM
+        // kernels at once made the backward pass slower (18.1 ms against 15.4 ms with
+        // the single-cluster adjoint for 256^2, 10,000 steps), so variant 0 keeps the
+        // single-cluster adjoint
+        const bool drift = p.vx != 0.0 || p.vy != 0.0;
+        int i = -1;
+        if (p.variant >= kMCVariant && p.variant < kMCVariant + kMCConfigs) i = p.variant - kMCVariant;
+        if (i >= 0 && cl == kRRCluster && mc_table(i).n == p.n) {
+            bool fits = false;
+            cudaError_t e = mc_fits(i, drift, &fits, 1);
+            if (e != cudaSuccess) return e;
+            if (fits) return mc_run(i, 1, drift, args, 9, st);
+            if (p.variant != 0) return cudaErrorInvalidConfiguration;
+        }
+    }
     const int variant = p.variant >= kMCVariant ? 0 : p.variant;
     if (sizeof(T) == 4 && cl == kRRCluster && (variant == 0 || variant == 3 || variant > 10)) {
         size_t smem = 0;

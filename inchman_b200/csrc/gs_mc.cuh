@@ -161,16 +161,13 @@ __device__ __forceinline__ void mc_step(const MCCtx<N, C, G, WPC>& c, const GSCo
     }
 }
 
-template <int N, int C, int G, int WPC, int DRIFT>
-__global__ void __launch_bounds__(32 * WPC, 1)
-    k_gs_forward_mc(GSArgs<float> a, const float* __restrict__ u0, const float* __restrict__ v0,
-                    float* __restrict__ uo, float* __restrict__ vo, float* __restrict__ trace, int trace_every,
-                    float* __restrict__ xbuf, uint32_t* __restrict__ flags) {
+// the ring neighbours, exchange roles and mbarriers of a warp's row (forward and
+// adjoint alike); *row: the warp's lattice row, *band: whether it is a band row
+template <int N, int C, int G, int WPC>
+__device__ __forceinline__ void mc_setup(MCCtx<N, C, G, WPC>& c, unsigned char* smem_raw, float* xbuf,
+                                         uint32_t* flags, int* row, bool* band) {
     using S = MCShape<N, C, G, WPC>;
-    constexpr int H = S::H, B = S::B;
-    constexpr int NN = N * N;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    MCCtx<N, C, G, WPC> c;
+    constexpr int B = S::B;
     c.smem = smem_raw;
     c.sbase = smem_u32(smem_raw);
     c.lane = threadIdx.x & 31;
@@ -188,8 +185,8 @@ __global__ void __launch_bounds__(32 * WPC, 1)
     c.tx = (uint32_t)nremote * 2u * S::kRow;
     // local row l of cluster cl is lattice row cl * B - G + l (periodic)
     const int l = (int)rank * WPC + c.w;
-    const int row = (cl * B - G + l + N) % N;
-    const int col0 = c.lane * 2 * H;
+    *row = (cl * B - G + l + N) % N;
+    *band = l >= G && l < G + B;
     // exchange roles: rows [G, 2G) feed the cluster above (side 0), rows [B, B + G) the
     // cluster below (side 1); ghost rows [0, G) come from the cluster above's side 1,
     // ghost rows [B + G, B + 2G) from the cluster below's side 0
@@ -217,15 +214,29 @@ __global__ void __launch_bounds__(32 * WPC, 1)
         c.ghost_row = xrow(dn, 0, l - B - G);
         c.ghost_flag = xflag(dn, 0, l - B - G);
     }
-    const bool band = l >= G && l < G + B;
-    const GSCoef2 k(a);
-
     if (c.lane == 0) {
         mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 0) - c.sbase)), 1 + 32 * (2 - nremote));
         mbar_init(reinterpret_cast<uint64_t*>(smem_raw + (c.bar(c.w, 1) - c.sbase)), 1 + 32 * (2 - nremote));
         fence_mbar_init();
     }
     if (threadIdx.x == 0) *c.failed = 0;
+}
+
+template <int N, int C, int G, int WPC, int DRIFT>
+__global__ void __launch_bounds__(32 * WPC, 1)
+    k_gs_forward_mc(GSArgs<float> a, const float* __restrict__ u0, const float* __restrict__ v0,
+                    float* __restrict__ uo, float* __restrict__ vo, float* __restrict__ trace, int trace_every,
+                    float* __restrict__ xbuf, uint32_t* __restrict__ flags) {
+    using S = MCShape<N, C, G, WPC>;
+    constexpr int H = S::H;
+    constexpr int NN = N * N;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MCCtx<N, C, G, WPC> c;
+    int row;
+    bool band;
+    mc_setup<N, C, G, WPC>(c, smem_raw, xbuf, flags, &row, &band);
+    const int col0 = c.lane * 2 * H;
+    const GSCoef2 k(a);
     float2 xu[H], xv[H], yu[H], yv[H];
     rr_load<H>(u0 + (size_t)row * N + col0, xu);
     rr_load<H>(v0 + (size_t)row * N + col0, xv);
@@ -279,4 +290,133 @@ __global__ void __launch_bounds__(32 * WPC, 1)
         rr_store<H>(uo + (size_t)row * N + col0, pu);
         rr_store<H>(vo + (size_t)row * N + col0, pv);
     }
+}
+
+// ---- multi-cluster adjoint -------------------------------------------------------
+// The transposed steps of a segment, last to first, over the same bands and ghost
+// rows as the multi-cluster forward: the adjoint fields (lambda_u, lambda_v) of a
+// warp's row stay in registers and are exchanged and swapped exactly like the forward
+// rows (a ghost row's lambda goes stale from the ring's ends inwards just as a state
+// row does).  The adjoint update needs the forward state only at the cell itself, so
+// each warp reads its own row of the stored state from global memory, two steps
+// ahead, into registers.  The parameter-gradient partial sums of ghost rows are
+// dropped: every lattice cell is a band row of exactly one cluster.  The adjoint
+// fields are bit-identical to the single-cluster adjoint's; the gradient sums differ
+// from its only in the order of the float partial sums.
+
+template <int N>
+__device__ __forceinline__ void mc_adj_state(const float* __restrict__ states, int len, int q, int row, int col0,
+                                             float2 (&su)[N / 64], float2 (&sv)[N / 64]) {
+    constexpr int H = N / 64;
+    constexpr size_t NN = (size_t)N * N;
+    if (q >= len) return;
+    const int j = len - 1 - q;   // adjoint step q uses stored state len - 1 - q
+    rr_load<H>(states + (size_t)(2 * j) * NN + (size_t)row * N + col0, su);
+    rr_load<H>(states + (size_t)(2 * j + 1) * NN + (size_t)row * N + col0, sv);
+}
+
+template <int N, int C, int G, int WPC, int DRIFT>
+__device__ __forceinline__ void mc_adj_step(const MCCtx<N, C, G, WPC>& c, const GSCoef2& k,
+                                            const float2 (&xa)[N / 64], const float2 (&xb)[N / 64],
+                                            float2 (&ya)[N / 64], float2 (&yb)[N / 64], const float2 (&su)[N / 64],
+                                            const float2 (&sv)[N / 64], int s, bool send, float2 t[6]) {
+    constexpr int H = N / 64;
+    const int par = s & 1;
+    rr_wait(c.bar(c.w, par), (uint32_t)(s >> 1) & 1u, c.failed);
+    __syncwarp();
+    if (c.lane == 0) rr_arm(c.bar(c.w, par), c.tx);
+    float2 ha[H], hb[H], la[H], lb[H];
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 0) - c.sbase), c.lane, ha);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 0, 1) - c.sbase), c.lane, hb);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 0) - c.sbase), c.lane, la);
+    rr_read_halo<H>(c.smem + (c.slot(c.w, par, 1, 1) - c.sbase), c.lane, lb);
+    rr_adj_row<H, DRIFT>(k, ha, xa, la, hb, xb, lb, su, sv, ya, yb, t, c.lane);
+    if (send) {
+        if ((s + 1) % G == 0) mc_swap<N, C, G, WPC>(c, ya, yb, (s + 1) / G);
+        const int np = par ^ 1;
+        rr_send<H>(ya, yb, c.slot(c.up_w, np, 1, 0), c.slot(c.up_w, np, 1, 1), c.bar(c.up_w, np), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(ya, yb, c.slot(c.dn_w, np, 0, 0), c.slot(c.dn_w, np, 0, 1), c.bar(c.dn_w, np), c.dn_remote,
+                   c.dn_rank, c.lane);
+    }
+}
+
+template <int N, int C, int G, int WPC, int DRIFT>
+__global__ void __launch_bounds__(32 * WPC, 1)
+    k_gs_adjoint_mc(GSArgs<float> a, const float* __restrict__ states, int len, const float* __restrict__ lu_in,
+                    const float* __restrict__ lv_in, float* __restrict__ lu_out, float* __restrict__ lv_out,
+                    double* __restrict__ grad, int* __restrict__ err, float* __restrict__ xbuf,
+                    uint32_t* __restrict__ flags) {
+    constexpr int H = N / 64;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[6][32];
+    MCCtx<N, C, G, WPC> c;
+    int row;
+    bool band;
+    mc_setup<N, C, G, WPC>(c, smem_raw, xbuf, flags, &row, &band);
+    const int col0 = c.lane * 2 * H;
+    const GSCoef2 k(a);
+    float2 xa[H], xb[H], ya[H], yb[H];
+    rr_load<H>(lu_in + (size_t)row * N + col0, xa);
+    rr_load<H>(lv_in + (size_t)row * N + col0, xb);
+    // the forward state of the row for the even and the odd step of an iteration
+    float2 eu[H], ev[H], ou[H], ov[H];
+    mc_adj_state<N>(states, len, 0, row, col0, eu, ev);
+    mc_adj_state<N>(states, len, 1, row, col0, ou, ov);
+    __syncthreads();
+    cluster_arrive();     // every CTA's mbarriers exist before anyone sends
+    cluster_wait();
+    if (len > 0) {
+        if (c.lane == 0) {
+            rr_arm(c.bar(c.w, 0), c.tx);
+            rr_arm(c.bar(c.w, 1), c.tx);
+        }
+        rr_send<H>(xa, xb, c.slot(c.up_w, 0, 1, 0), c.slot(c.up_w, 0, 1, 1), c.bar(c.up_w, 0), c.up_remote,
+                   c.up_rank, c.lane);
+        rr_send<H>(xa, xb, c.slot(c.dn_w, 0, 0, 0), c.slot(c.dn_w, 0, 0, 1), c.bar(c.dn_w, 0), c.dn_remote,
+                   c.dn_rank, c.lane);
+    }
+    // gradient partial sums: float over the two steps of an iteration, then double;
+    // ghost rows' sums are dropped
+    double g[6] = {0, 0, 0, 0, 0, 0};
+    auto flush = [&](float2 (&t)[6]) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            if (band) g[q] += (double)t[q].x + (double)t[q].y;
+            t[q] = f2(0.f);
+        }
+    };
+    float2 t[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
+    int s = 0;
+    for (; s + 2 <= len; s += 2) {
+        mc_adj_step<N, C, G, WPC, DRIFT>(c, k, xa, xb, ya, yb, eu, ev, s, true, t);
+        mc_adj_state<N>(states, len, s + 2, row, col0, eu, ev);
+        mc_adj_step<N, C, G, WPC, DRIFT>(c, k, ya, yb, xa, xb, ou, ov, s + 1, s + 2 < len, t);
+        mc_adj_state<N>(states, len, s + 3, row, col0, ou, ov);
+        flush(t);
+    }
+    const bool odd = s < len;
+    if (odd) {
+        mc_adj_step<N, C, G, WPC, DRIFT>(c, k, xa, xb, ya, yb, eu, ev, s, false, t);
+        flush(t);
+    }
+    g[4] = -g[4];      // gs_adj_update2s accumulates the drift sums negated
+    g[5] = -g[5];
+    __syncthreads();
+    cluster_arrive();     // no CTA leaves while a neighbour may still address its shared memory
+    cluster_wait();
+    const bool bad = *c.failed != 0;
+    if (bad && threadIdx.x == 0) atomicOr(err, 1);
+    if (band) {
+        const float nan = __int_as_float(0x7fc00000);
+        float2 pa[H], pb[H];
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            pa[j] = bad ? make_float2(nan, nan) : (odd ? ya[j] : xa[j]);
+            pb[j] = bad ? make_float2(nan, nan) : (odd ? yb[j] : xb[j]);
+        }
+        rr_store<H>(lu_out + (size_t)row * N + col0, pa);
+        rr_store<H>(lv_out + (size_t)row * N + col0, pb);
+    }
+    grad_reduce(g, (double)a.dt, grad, red, (int)threadIdx.x, (int)blockDim.x);
 }

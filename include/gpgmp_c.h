@@ -282,7 +282,9 @@ typedef struct gpgmp_gs_params {
                                    5 (4, 32), 6 (2, 32), a CUDA error where the device cannot hold
                                    all its clusters at once.  Every float32 family gives the same
                                    bits.  float64 always uses 0 / 1 (column walk / per cell).  The
-                                   adjoint and the batched forward treat 40 + i as 0. */
+                                   adjoint runs the multi-cluster adjoint under 40 + i (the same
+                                   lambda bits) and the single-cluster one under 0; the batched
+                                   forward treats 40 + i as 0. */
 } gpgmp_gs_params;
 
 /* bytes of the checkpoint buffer and of the adjoint's work buffer */

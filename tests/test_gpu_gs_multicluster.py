@@ -109,3 +109,43 @@ def test_automatic_choice_is_the_multicluster_kernel(gpgmp):
         assert all(torch.equal(x, y) for x, y in zip(a, b))
     assert gs.auto_variant(128) == 14   # one cluster, 4 warps per CTA
     assert gs.status() == 0
+
+
+@pytest.mark.parametrize("steps,drift,every", [(1, False, 100), (17, True, 5), (250, False, 100), (301, True, 40)])
+def test_multicluster_adjoint_matches_single_cluster(gpgmp, steps, drift, every):
+    """The multi-cluster adjoint (with the multi-cluster recomputation of the segments)
+    gives the same bits of lambda at the initial state as the single-cluster adjoint,
+    and the same parameter gradient up to the order of its float partial sums (one row
+    per lane instead of two): within 1e-4 of the largest component, far below the
+    float32 gradient's own error against float64 and far above what a ghost row counted
+    or a band row dropped would leave (about 1/256 of a component)."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=256, steps=steps, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0, checkpoint_every=every)
+    u0, v0 = cfg.initial_state(np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(steps)
+    lu = torch.rand((256, 256), device="cuda", generator=g) - 0.5
+    lv = torch.rand((256, 256), device="cuda", generator=g) - 0.5
+
+    def grad(variant):
+        p = cfg.params(variant=variant)
+        nck = -(-steps // every)
+        ck = torch.empty((nck, 2, 256, 256), device="cuda")
+        gs.forward(tu, tv, p, checkpoints=ck)
+        out = gs.adjoint(p, ck, lu, lv)
+        torch.cuda.synchronize()
+        return out
+
+    ru, rv, rg = grad(3)
+    ran = 0
+    for var in _variants():
+        if not _fits(var):
+            continue
+        mu, mv, mg = grad(var)
+        assert torch.equal(mu, ru) and torch.equal(mv, rv), (var, int((mu != ru).sum()), int((mv != rv).sum()))
+        scale = float(rg.abs().max())
+        assert float((mg - rg).abs().max()) <= 1e-4 * scale, (var, (mg - rg).tolist(), rg.tolist())
+        ran += 1
+    assert ran >= 1
+    assert gs.status() == 0
