@@ -46,14 +46,19 @@ GSParams to_params(const gpgmp_gs_params* p) {
     return g;
 }
 
-int ck_every(const gpgmp_gs_params* p) { return p->checkpoint_every > 0 ? p->checkpoint_every : 100; }
+// the automatic interval: 100 steps in float32; 50 in float64, whose 50-state segment
+// (50 MB at 256^2) the adjoint reads back while it is still in L2 (the same memory:
+// ceil(steps / c) + 2c states either way at 10,000 steps)
+int ck_every(const gpgmp_gs_params* p, int elem_bytes) {
+    return p->checkpoint_every > 0 ? p->checkpoint_every : (elem_bytes == 8 ? 50 : 100);
+}
 
 template <typename T>
 int forward(const gpgmp_gs_params* p, const T* u0, const T* v0, T* u, T* v, T* ckpt, void* stream) {
     int rc = check(p, sizeof(T));
     if (rc) return rc;
     GSParams g = to_params(p);
-    CK(gs_forward<T>(g, u0, v0, u, v, ckpt, ck_every(p), (cudaStream_t)stream));
+    CK(gs_forward<T>(g, u0, v0, u, v, ckpt, ck_every(p, (int)sizeof(T)), (cudaStream_t)stream));
     return GPGMP_OK;
 }
 
@@ -97,7 +102,7 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
     if (rc) return rc;
     if (!ckpt || !lu || !lv || !gu || !gv || !grad6 || !work) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
-    const int c = ck_every(p);
+    const int c = ck_every(p, (int)sizeof(T));
     const size_t nn = (size_t)p->n * p->n;
     T* segb[2] = {(T*)work, (T*)work + (size_t)2 * c * nn};   // c states, 2 nn each
     T* fin[2] = {segb[1] + (size_t)2 * c * nn, segb[1] + (size_t)2 * c * nn + 2 * nn};   // recomputed end states
@@ -164,7 +169,7 @@ extern "C" {
 int gpgmp_gs_buffer_sizes(const gpgmp_gs_params* p, int32_t elem_bytes, size_t* ck_bytes, size_t* work_bytes) {
     if (!p || !ck_bytes || !work_bytes) return set_error(GPGMP_ERR_INVALID, "NULL argument");
     if (elem_bytes != 4 && elem_bytes != 8) return set_error(GPGMP_ERR_INVALID, "elem_bytes %d", elem_bytes);
-    const int c = ck_every(p);
+    const int c = ck_every(p, elem_bytes);
     const size_t nn = (size_t)p->n * p->n;
     const size_t nseg = (size_t)((p->steps + c - 1) / c);
     *ck_bytes = std::max<size_t>(1, nseg) * 2 * nn * elem_bytes;

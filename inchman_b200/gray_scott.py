@@ -195,10 +195,11 @@ def _make_autograd():
     import torch
 
     class GrayScott(torch.autograd.Function):
-        """(u0, v0, theta) -> (u_N, v_N); theta = (F, k, Du, Dv, vx, vy)."""
+        """(u0, v0, theta) -> (u_N, v_N); theta = (F, k, Du, Dv, vx, vy); checkpoint_every
+        <= 0: the library's automatic interval (100 steps in float32, 50 in float64)."""
 
         @staticmethod
-        def forward(ctx, u0, v0, theta, steps: int, dt: float, checkpoint_every: int = 100):
+        def forward(ctx, u0, v0, theta, steps: int, dt: float, checkpoint_every: int = 0):
             th = theta.detach().double().cpu().tolist()
             n = u0.shape[-1]
             p = GSParams(n=n, steps=steps, F=th[0], k=th[1], Du=th[2], Dv=th[3], vx=th[4], vy=th[5], dt=dt,
