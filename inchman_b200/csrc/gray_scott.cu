@@ -833,11 +833,10 @@ cudaError_t gs_adjoint_segment(const GSParams& p, const T* states, int len, cons
     GSArgs<T> a{p.n, p.steps, (T)p.F, (T)p.k, (T)p.Du, (T)p.Dv, (T)p.vx, (T)p.vy, (T)p.dt};
     void* args[] = {&a, (void*)&states, &len, (void*)&lu_in, (void*)&lv_in, &lu_out, &lv_out, &grad, &err};
     if constexpr (std::is_same<T, float>::value) {
-        // the multi-cluster adjoint, with a multi-cluster variant only: in the gradient
-        // it runs beside the segment recomputation on the side stream, and two 64-SM
-        // kernels at once made the backward pass slower (18.1 ms against 15.4 ms with
-        // the single-cluster adjoint for 256^2, 10,000 steps), so variant 0 keeps the
-        // single-cluster adjoint
+        // the multi-cluster adjoint, with a multi-cluster variant only (the gradient
+        // pipeline names it under the automatic choice, with the single-cluster forward
+        // recomputing the segments beside it: two 64-SM kernels at once made the
+        // backward slower, 18.1 ms against 15.4 ms)
         const bool drift = p.vx != 0.0 || p.vy != 0.0;
         int i = -1;
         if (p.variant >= kMCVariant && p.variant < kMCVariant + kMCConfigs) i = p.variant - kMCVariant;

@@ -283,8 +283,10 @@ typedef struct gpgmp_gs_params {
                                    all its clusters at once.  Every float32 family gives the same
                                    bits.  float64 always uses 0 / 1 (column walk / per cell).  The
                                    adjoint runs the multi-cluster adjoint under 40 + i (the same
-                                   lambda bits) and the single-cluster one under 0; the batched
-                                   forward treats 40 + i as 0. */
+                                   lambda bits); under 0, where the forward is multi-cluster, it
+                                   recomputes the segments with the single-cluster forward and runs
+                                   the multi-cluster adjoint beside it.  The batched forward treats
+                                   40 + i as 0. */
 } gpgmp_gs_params;
 
 /* bytes of the checkpoint buffer and of the adjoint's work buffer */
