@@ -575,10 +575,12 @@ const MCConfig& mc_table(int i) {
     return t[i];
 }
 
-// launch configuration of a multi-cluster kernel; cooperative: all CTAs resident at
-// once (the clusters wait on one another's flags), asked of the launch itself
-void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, cudaStream_t st,
-                      bool cooperative) {
+// launch configuration of a multi-cluster kernel.  The clusters wait on one another's
+// flags, so all of them must be resident at once: mc_fits checks that the device holds
+// them (the launch itself is not cooperative, which the profiler refuses for cluster
+// launches), and every wait is bounded, so a cluster that is not running yet costs a
+// NaN result and an error status, never a hang
+void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, cudaStream_t st) {
     *cfg = {};
     cfg->gridDim = dim3(kRRCluster * m.clusters, 1, 1);
     cfg->blockDim = dim3(32 * m.wpc, 1, 1);
@@ -588,10 +590,8 @@ void mc_launch_config(const MCConfig& m, cudaLaunchConfig_t* cfg, cudaLaunchAttr
     attr[0].val.clusterDim.x = kRRCluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    attr[1].id = cudaLaunchAttributeCooperative;
-    attr[1].val.cooperative = 1;
     cfg->attrs = attr;
-    cfg->numAttrs = cooperative ? 2 : 1;
+    cfg->numAttrs = 1;
 }
 
 // whether every cluster of configuration i can be resident at once on the current
@@ -615,8 +615,8 @@ cudaError_t mc_fits(int i, bool drift, bool* fits, int kind = 0) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
         cudaLaunchConfig_t cfg;
-        cudaLaunchAttribute attr[2];
-        mc_launch_config(m, &cfg, attr, nullptr, false);
+        cudaLaunchAttribute attr[1];
+        mc_launch_config(m, &cfg, attr, nullptr);
         int active = 0;
         e = cudaOccupancyMaxActiveClusters(&active, fn, &cfg);
         if (e != cudaSuccess) return e;
@@ -647,8 +647,8 @@ cudaError_t mc_run(int i, int kind, bool drift, void** args, int nargs, cudaStre
         all[nargs] = &xb;
         all[nargs + 1] = &fl;
         cudaLaunchConfig_t cfg;
-        cudaLaunchAttribute attr[2];
-        mc_launch_config(m, &cfg, attr, st, true);
+        cudaLaunchAttribute attr[1];
+        mc_launch_config(m, &cfg, attr, st);
         e = cudaLaunchKernelExC(&cfg, fn, all);
     }
     cudaError_t e2 = pool_free(buf, st);
