@@ -320,7 +320,7 @@ def bench_gray_scott(args, rank, world):
     ut64, vt64 = ut.double(), vt.double()
 
     def grad64_once():
-        u, v = GS.apply(u064, v064, th, steps, cfg.dt, 0)    # automatic interval: 50 steps
+        u, v = GS.apply(u064, v064, th, steps, cfg.dt, 0)    # automatic interval: 25 steps
         loss = ((u - ut64) ** 2 + (v - vt64) ** 2).sum()
         loss.backward()
         return loss
@@ -365,7 +365,7 @@ def bench_gray_scott(args, rank, world):
         "adjoint_forward_ratio_f64": t_grad64 / t_fwd64,
         "gradient_ms": t_grad * 1e3,
         "gradient_ms_f64": t_grad64 * 1e3, "forward_ms_f64": t_fwd64 * 1e3,
-        "checkpoint_every": {"f32": 100, "f64": 50},
+        "checkpoint_every": {"f32": 100, "f64": 25},
         "batched_fd_solves": batched,
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": 2 * n * n * 4},

@@ -46,11 +46,13 @@ GSParams to_params(const gpgmp_gs_params* p) {
     return g;
 }
 
-// the automatic interval: 100 steps in float32; 50 in float64, whose 50-state segment
-// (50 MB at 256^2) the adjoint reads back while it is still in L2 (the same memory:
-// ceil(steps / c) + 2c states either way at 10,000 steps)
+// the automatic interval: 100 steps in float32 (shorter segments add launches to a
+// latency-bound adjoint: 3.05 / 3.30 / 3.79 x the forward at 100 / 50 / 25 steps);
+// 25 in float64, whose two 25-state segment buffers (50 MB at 256^2) stay in L2 while
+// the adjoint reads them back (3.11 / 3.28 / 3.70 at 25 / 50 / 100 steps, the 50-step
+// buffers at the edge of L2 and 3.78 in some runs)
 int ck_every(const gpgmp_gs_params* p, int elem_bytes) {
-    return p->checkpoint_every > 0 ? p->checkpoint_every : (elem_bytes == 8 ? 50 : 100);
+    return p->checkpoint_every > 0 ? p->checkpoint_every : (elem_bytes == 8 ? 25 : 100);
 }
 
 template <typename T>

@@ -196,7 +196,7 @@ def _make_autograd():
 
     class GrayScott(torch.autograd.Function):
         """(u0, v0, theta) -> (u_N, v_N); theta = (F, k, Du, Dv, vx, vy); checkpoint_every
-        <= 0: the library's automatic interval (100 steps in float32, 50 in float64)."""
+        <= 0: the library's automatic interval (100 steps in float32, 25 in float64)."""
 
         @staticmethod
         def forward(ctx, u0, v0, theta, steps: int, dt: float, checkpoint_every: int = 0):

@@ -269,7 +269,7 @@ typedef struct gpgmp_gs_params {
     int32_t n;                  /* lattice side; a multiple of the cluster size */
     int32_t steps;
     double  F, k, Du, Dv, vx, vy, dt;
-    int32_t checkpoint_every;   /* <= 0: 100 in float32, 50 in float64 */
+    int32_t checkpoint_every;   /* <= 0: 100 in float32, 25 in float64 */
     int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
     int32_t variant;            /* kernel family (float32): 0 automatic = for n = 256 the
                                    multi-cluster kernel 42 where the device holds its four clusters at
