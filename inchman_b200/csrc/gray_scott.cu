@@ -552,7 +552,7 @@ struct MCConfig {
     int n, clusters, ghost, wpc;
     const void* k[2][2];   // [forward / adjoint][without / with drift]
     uint32_t smem;
-    size_t xfloats, flags;
+    size_t xwords;   // exchange buffer, 64-bit words
 };
 template <int N, int C, int G, int W>
 MCConfig mc_config() {
@@ -560,13 +560,13 @@ MCConfig mc_config() {
     return {N, C, G, W,
             {{(const void*)k_gs_forward_mc<N, C, G, W, 0>, (const void*)k_gs_forward_mc<N, C, G, W, 1>},
              {(const void*)k_gs_adjoint_mc<N, C, G, W, 0>, (const void*)k_gs_adjoint_mc<N, C, G, W, 1>}},
-            S::kSmem, S::kXFloats, S::kFlags};
+            S::kSmem, S::kXWords};
 }
 constexpr int kMCVariant = 40;
 constexpr int kMCConfigs = 7;
-// the automatic choice for n = 256: 4 clusters, 16 ghost rows (0.63 us per step
-// against 0.74 for the single-cluster kernel; (4, 8) and (4, 32) within 1 %)
-constexpr int kMCDefault = 2;
+// the automatic choice for n = 256: 4 clusters, 8 ghost rows (0.587 us per step;
+// (4, 16) 0.594, (4, 32) 0.611, the single-cluster kernel 0.74)
+constexpr int kMCDefault = 1;
 const MCConfig& mc_table(int i) {
     static const MCConfig t[kMCConfigs] = {mc_config<256, 2, 8, 9>(),   mc_config<256, 4, 8, 5>(),
                                            mc_config<256, 4, 16, 6>(),  mc_config<256, 8, 8, 3>(),
@@ -576,7 +576,7 @@ const MCConfig& mc_table(int i) {
 }
 
 // launch configuration of a multi-cluster kernel.  The clusters wait on one another's
-// flags, so all of them must be resident at once: mc_fits checks that the device holds
+// rows, so all of them must be resident at once: mc_fits checks that the device holds
 // them (the launch itself is not cooperative, which the profiler refuses for cluster
 // launches), and every wait is bounded, so a cluster that is not running yet costs a
 // NaN result and an error status, never a hang
@@ -626,32 +626,29 @@ cudaError_t mc_fits(int i, bool drift, bool* fits, int kind = 0) {
     return cudaSuccess;
 }
 
-// one multi-cluster launch (kind 0 forward, 1 adjoint segment): exchange buffer and
-// flags from the stream-ordered pool (private to this launch), flags cleared on the
-// stream, then the kernel with `args` followed by the buffer and flag pointers
+// one multi-cluster launch (kind 0 forward, 1 adjoint segment): exchange buffer from
+// the stream-ordered pool (private to this launch), cleared on the stream, then the
+// kernel with `args` followed by the buffer pointer
 cudaError_t mc_run(int i, int kind, bool drift, void** args, int nargs, cudaStream_t st) {
     const MCConfig& m = mc_table(i);
     const void* fn = m.k[kind][drift ? 1 : 0];
-    const size_t xbytes = m.xfloats * sizeof(float), fbytes = m.flags * sizeof(uint32_t);
-    char* buf = nullptr;
-    cudaError_t e = pool_alloc((void**)&buf, xbytes + fbytes, st);
+    const size_t xbytes = m.xwords * sizeof(uint64_t);
+    uint64_t* xb = nullptr;
+    cudaError_t e = pool_alloc((void**)&xb, xbytes, st);
     if (e != cudaSuccess) return e;
-    float* xb = reinterpret_cast<float*>(buf);
-    uint32_t* fl = reinterpret_cast<uint32_t*>(buf + xbytes);
-    e = cudaMemsetAsync(fl, 0, fbytes, st);
+    e = cudaMemsetAsync(xb, 0, xbytes, st);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) {
         void* all[16];
         for (int q = 0; q < nargs; ++q) all[q] = args[q];
         all[nargs] = &xb;
-        all[nargs + 1] = &fl;
         cudaLaunchConfig_t cfg;
         cudaLaunchAttribute attr[1];
         mc_launch_config(m, &cfg, attr, st);
         e = cudaLaunchKernelExC(&cfg, fn, all);
     }
-    cudaError_t e2 = pool_free(buf, st);
+    cudaError_t e2 = pool_free(xb, st);
     return e != cudaSuccess ? e : e2;
 }
 

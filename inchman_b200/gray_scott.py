@@ -154,7 +154,7 @@ MULTI_CLUSTER = {40: (2, 8), 41: (4, 8), 42: (4, 16), 43: (8, 8), 44: (8, 16), 4
 
 def auto_variant(n: int, drift: bool = False) -> int:
     """The float32 kernel family that variant 0 resolves to for an n x n lattice on
-    this GPU (42: four 16-CTA clusters; 10 + w: one cluster, w warps per CTA; 2: the
+    this GPU (41: four 16-CTA clusters, 8 ghost rows; 10 + w: one cluster, w warps per CTA; 2: the
     shared-memory column walk; 1: one cell per iteration)."""
     v = C.c_int32(0)
     _lib.check(_fn("gpgmp_gs_auto_variant")(n, int(drift), C.byref(v)), "gpgmp_gs_auto_variant")

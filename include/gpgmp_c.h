@@ -272,7 +272,7 @@ typedef struct gpgmp_gs_params {
     int32_t checkpoint_every;   /* <= 0: 100 in float32, 25 in float64 */
     int32_t cluster;            /* CTAs per thread-block cluster, 0 = automatic */
     int32_t variant;            /* kernel family (float32): 0 automatic = for n = 256 the
-                                   multi-cluster kernel 42 where the device holds its four clusters at
+                                   multi-cluster kernel 41 where the device holds its four clusters at
                                    once, else register-resident where the lattice allows (n 64, 128,
                                    256 on a 16-CTA cluster), else the shared-memory column walk;
                                    1 one cell per iteration; 2 shared-memory column walk;

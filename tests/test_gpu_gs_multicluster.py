@@ -74,12 +74,12 @@ def test_multicluster_forward_bit_identical_to_single_cluster(gpgmp, steps, drif
 
 
 def test_multicluster_forward_bit_exact_against_oracle(gpgmp):
-    """The automatic 4-cluster configuration (16 ghost rows), 1000 steps with drift, bit
+    """The automatic 4-cluster configuration (8 ghost rows), 1000 steps with drift, bit
     for bit against the oracle's float32 restatement of the kernels' operation order."""
     import torch
     from inchman_b200 import gray_scott as gs
-    cfg = _cfg(n=256, steps=1000, vx=0.05, vy=-0.03, variant=42)
-    if not _fits(42):
+    cfg = _cfg(n=256, steps=1000, vx=0.05, vy=-0.03, variant=41)
+    if not _fits(41):
         pytest.skip("4 clusters of 16 CTAs are not co-resident on this device")
     u0, v0 = cfg.initial_state(np.float32)
     tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
@@ -96,16 +96,16 @@ def test_multicluster_forward_bit_exact_against_oracle(gpgmp):
 
 def test_automatic_choice_is_the_multicluster_kernel(gpgmp):
     """On a B200 variant 0 resolves to four clusters for 256 x 256 (the device holds
-    them at once) and runs it: same bits as naming variant 42, with and without drift."""
+    them at once) and runs it: same bits as naming variant 41, with and without drift."""
     import torch
     from inchman_b200 import gray_scott as gs
     for drift in (False, True):
-        assert gs.auto_variant(256, drift) == 42
+        assert gs.auto_variant(256, drift) == 41
         cfg = _cfg(n=256, steps=50, vx=0.05 if drift else 0.0, vy=-0.03 if drift else 0.0)
         u0, v0 = cfg.initial_state(np.float32)
         tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
         a = _run(cfg, 0, tu, tv, 7, 50)
-        b = _run(cfg, 42, tu, tv, 7, 50)
+        b = _run(cfg, 41, tu, tv, 7, 50)
         assert all(torch.equal(x, y) for x, y in zip(a, b))
     assert gs.auto_variant(128) == 14   # one cluster, 4 warps per CTA
     assert gs.status() == 0
