@@ -123,16 +123,19 @@ int adjoint(const gpgmp_gs_params* p, const T* ckpt, const T* lu, const T* lv, T
     }
     GSParams g = to_params(p);
     // float32 under the automatic choice, where the forward is the multi-cluster kernel:
-    // the segments are recomputed by the single-cluster forward (16 SMs) and the
-    // adjoint runs on four clusters (64 SMs), so both fit on the chip at once (backward
-    // 12.0 ms against 15.2 ms with the multi-cluster recomputation and the single-cluster
-    // adjoint, 256^2, 10,000 steps); every pairing gives the same bits of lambda
+    // the segments are recomputed on two clusters (32 SMs, variant 40) and the adjoint
+    // runs on four (64 SMs), so both fit on the chip at once (backward 10.6 ms, against
+    // 12.0 ms with the single-cluster recomputation, 15.2 ms with the multi-cluster
+    // recomputation and the single-cluster adjoint, 256^2, 10,000 steps); every pairing
+    // gives the same bits of lambda.  Where four clusters are resident at once two are;
+    // the adjoint never waits on the recomputation beside it, so a recomputation that
+    // finds only part of the chip free waits (bounded) for the adjoint's SMs, no longer
     GSParams gr = g, ga = g;
     if (sizeof(T) == 4 && g.variant == 0) {
         int v = 0;
         CK(gs_auto_variant(p->n, p->vx != 0.0 || p->vy != 0.0, &v));
         if (v >= 40) {
-            gr.variant = 3;
+            gr.variant = 40;
             ga.variant = v;
         }
     }

@@ -284,8 +284,8 @@ typedef struct gpgmp_gs_params {
                                    bits.  float64 always uses 0 / 1 (column walk / per cell).  The
                                    adjoint runs the multi-cluster adjoint under 40 + i (the same
                                    lambda bits); under 0, where the forward is multi-cluster, it
-                                   recomputes the segments with the single-cluster forward and runs
-                                   the multi-cluster adjoint beside it.  The batched forward treats
+                                   recomputes the segments on two clusters (40) and runs the
+                                   four-cluster adjoint beside it.  The batched forward treats
                                    40 + i as 0. */
 } gpgmp_gs_params;
 
