@@ -149,3 +149,43 @@ def test_multicluster_adjoint_matches_single_cluster(gpgmp, steps, drift, every)
         ran += 1
     assert ran >= 1
     assert gs.status() == 0
+
+
+def test_multicluster_forwards_on_two_streams_and_in_a_graph(gpgmp):
+    """Each multi-cluster launch takes its own exchange buffer from the stream-ordered
+    pool and clears it on its stream: two solves on two streams at once, and two
+    replays of a captured graph, give the bits of a solve on its own."""
+    import torch
+    from inchman_b200 import gray_scott as gs
+    cfg = _cfg(n=256, steps=200, vx=0.05, vy=-0.03)
+    if not _fits(41):
+        pytest.skip("4 clusters of 16 CTAs are not co-resident on this device")
+    p = cfg.params(variant=41)
+    u0, v0 = cfg.initial_state(np.float32)
+    tu, tv = torch.tensor(u0, device="cuda"), torch.tensor(v0, device="cuda")
+    ru, rv = gs.forward(tu, tv, p)
+    torch.cuda.synchronize()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    with torch.cuda.stream(s1):
+        a = gs.forward(tu, tv, p)
+    with torch.cuda.stream(s2):
+        b = gs.forward(tu, tv, p)
+    torch.cuda.synchronize()
+    for u, v in (a, b):
+        assert torch.equal(u, ru) and torch.equal(v, rv)
+    # graph capture: the launch, its pool allocation and the buffer clear are replayed
+    s3 = torch.cuda.Stream()
+    s3.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s3):
+        gs.forward(tu, tv, p)              # warm up on the capturing stream
+    torch.cuda.current_stream().wait_stream(s3)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        gu, gv = gs.forward(tu, tv, p)
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(gu, ru) and torch.equal(gv, rv)
+    del g
+    assert gs.status() == 0
