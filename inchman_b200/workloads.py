@@ -391,6 +391,23 @@ def _peaks():
     return load_peaks()
 
 
+def _profile_figures(name):
+    """`key: value` lines at the top of a profile summary (measured DRAM traffic per
+    launch, from its ncu capture)."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles", name)
+    out = {}
+    if os.path.exists(path):
+        for ln in open(path):
+            k, sep, v = ln.partition(":")
+            if sep and k.endswith("_bytes_per_launch"):
+                try:
+                    out[k.strip()] = float(v)
+                except ValueError:
+                    pass
+    return out
+
+
 def scan_sort(args, rank, world):
     """The individual-particle primitives on their own, through the C ABI: exclusive
     scan of 2^27 uint32 values (512 MB in, 512 MB out: larger than L2, so no flush is
@@ -431,6 +448,7 @@ def scan_sort(args, rank, world):
     t_cumsum = timed(lambda: torch.cumsum(x, 0, dtype=torch.int32, out=lib_out))
     del lib_out
     peak, peak_kind = _peaks()
+    figs = _profile_figures("scan_sort_2p27_2p24.md")
     ns = 1 << 24
     sorts = {}
     for bits, passes in ((20, 2), (32, 4)):
@@ -444,9 +462,14 @@ def scan_sort(args, rank, world):
         # library comparator on the same keys: torch.sort(stable=True) (int32 keys, int64
         # indices as the values: 12 B per key moved each pass instead of 8)
         t_lib = timed(lambda: torch.sort(k, stable=True))
+        # the library's digit width: 10 bits where that saves a pass, else 8
+        digit = 10 if 16 < bits <= 30 and (bits + 9) // 10 < (bits + 7) // 8 else 8
+        pass_traffic = figs.get(f"sort{digit}_pass_traffic_bytes_per_launch")
         sorts[f"keys_{bits}bit"] = {"pairs": ns, "passes": passes, "ms_per_sort": t * 1e3, "keys_per_s": ns / t,
                                     "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                                                 "frac": ach / peak, "peak_kind": peak_kind},
+                                                 "frac": ach / peak, "peak_kind": peak_kind,
+                                                 "traffic_per_pass": pass_traffic,
+                                                 "algorithmic_bytes_per_pass": 16 * ns},
                                     "torch_sort_stable_ms": t_lib * 1e3}
         del k, v, ko, vo, sscr
     ach = 8.0 * n / t_scan / 1e9
@@ -456,7 +479,8 @@ def scan_sort(args, rank, world):
                   # per timed scan: one scan kernel; per sort: histogram + one kernel per pass
                   "gpu_launches": args.steps * (1 + (1 + 2) + (1 + 4)),
                   "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                               "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_scan": 8 * n}})
+                               "peak_kind": peak_kind, "traffic": figs.get("scan_traffic_bytes_per_launch"),
+                               "algorithmic_bytes_per_scan": 8 * n}})
 
 
 def run(args, rank, world):
