@@ -221,3 +221,34 @@ def test_particle_step_edge_cases(gpgmp, case):
     if case in ("all_a", "no_reaction", "empty", "single"):
         assert int(count.sum()) == len(gx)
     assert np.array_equal(start, (np.cumsum(count) - count).astype(np.uint32))
+
+
+@pytest.mark.parametrize("bits", [20, 32])
+def test_sort_at_2p28_pairs_size_independent_properties(gpgmp, bits):
+    """2^28 pairs (about 7 GB on the device, 70,000 tiles, counts far above 16 bits in
+    the look-back words): too large for the oracle, so the size-independent properties
+    of a stable sort, checked on the device -- keys in order, equal keys in input order
+    (the values are the input indices), every output pair taken from its input index,
+    and the values a permutation."""
+    import torch
+    from inchman_b200 import individual as ind
+    n = 1 << 28
+    g = torch.Generator(device="cuda").manual_seed(bits)
+    keys = torch.randint(0, 1 << 31, (n,), dtype=torch.int64, device="cuda", generator=g)
+    if bits < 32:
+        keys &= (1 << bits) - 1
+    else:
+        keys = keys * 2 + (keys & 1)      # use the top bit too
+    keys = keys.to(torch.uint32).view(torch.int32) if hasattr(torch, "uint32") else keys.to(torch.int32)
+    vals = torch.arange(n, dtype=torch.int32, device="cuda")
+    ko, vo, scratch = ind.sort_pairs_u32(keys, vals, bits)
+    torch.cuda.synchronize()
+    assert ind.scratch_status(scratch, 1, n, bits) == 0
+    k64 = ko.to(torch.int64) & 0xFFFFFFFF
+    assert bool((k64[1:] >= k64[:-1]).all())
+    same = k64[1:] == k64[:-1]
+    assert bool((vo[1:][same] > vo[:-1][same]).all())
+    assert torch.equal(ko, keys[vo.long()])
+    seen = torch.zeros(n, dtype=torch.int32, device="cuda")
+    seen.index_put_((vo.long(),), torch.ones(n, dtype=torch.int32, device="cuda"), accumulate=True)
+    assert bool((seen == 1).all())
