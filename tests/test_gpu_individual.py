@@ -252,3 +252,24 @@ def test_sort_at_2p28_pairs_size_independent_properties(gpgmp, bits):
     seen = torch.zeros(n, dtype=torch.int32, device="cuda")
     seen.index_put_((vo.long(),), torch.ones(n, dtype=torch.int32, device="cuda"), accumulate=True)
     assert bool((seen == 1).all())
+
+
+def test_scan_at_2p29_values_size_independent_properties(gpgmp):
+    """2^29 values (4 GB in and out, 32,768 tiles, sums that wrap modulo 2^32): the
+    defining property of the exclusive scan checked on the device, in chunks --
+    out[0] = 0 and out[i + 1] - out[i] = in[i] modulo 2^32 -- and no look-back timeout."""
+    import torch
+    from inchman_b200 import individual as ind
+    n = 1 << 29
+    g = torch.Generator(device="cuda").manual_seed(29)
+    x = torch.randint(-(1 << 31), 1 << 31, (n,), dtype=torch.int64, device="cuda", generator=g).to(torch.int32)
+    scratch = ind.scan_scratch(n)
+    out = ind.exclusive_scan_u32(x, scratch)
+    torch.cuda.synchronize()
+    assert ind.scratch_status(scratch, 0, n) == 0
+    assert int(out[0]) == 0
+    step = 1 << 26
+    for a in range(0, n - 1, step):
+        b = min(a + step, n - 1)
+        d = (out[a + 1:b + 1].to(torch.int64) - out[a:b].to(torch.int64)) & 0xFFFFFFFF
+        assert torch.equal(d, x[a:b].to(torch.int64) & 0xFFFFFFFF), a
